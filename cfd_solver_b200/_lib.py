@@ -1,0 +1,140 @@
+"""ctypes binding of libcfd_b200.so (the C ABI declared in include/cfd_b200.h).
+
+There is no CPU fallback: if the shared library is missing or no CUDA device
+is present, the calls below raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libcfd_b200.so"
+
+OK = 0
+ERRORS = {-1: "CFD_E_ARG", -2: "CFD_E_CUDA", -3: "CFD_E_OOM", -4: "CFD_E_DIVERGED",
+          -5: "CFD_E_MAXITER", -6: "CFD_E_BREAKDOWN", -7: "CFD_E_NOTCONV"}
+PROFILE_OGRID, PROFILE_CAVITY = 0, 1
+
+# exported symbols (kept in sync with include/cfd_b200.h; tests check both)
+SYMBOLS = ("cfd_params_default", "cfd_last_error", "cfd_device_count", "cfd_case_create",
+           "cfd_case_step", "cfd_case_solve_to", "cfd_case_get_fields", "cfd_case_destroy",
+           "cfd_batch_create", "cfd_batch_step", "cfd_batch_stats", "cfd_batch_get_plane",
+           "cfd_batch_destroy", "cfd_case_bytes", "cfd_batch_profile", "cfd_batch_kernel_times",
+           "cfd_batch_sync")
+
+_D = ctypes.c_double
+_PD = ctypes.POINTER(ctypes.c_double)
+
+
+class CfdGrid(ctypes.Structure):
+    _fields_ = [("n0", ctypes.c_int), ("n1", ctypes.c_int), ("dxi0", _D), ("dxi1", _D),
+                ("p_grid", _D), ("a_grid", _D), ("ar", _D),
+                ("x", _PD), ("y", _PD), ("xix", _PD), ("xiy", _PD), ("etx", _PD), ("ety", _PD),
+                ("alph", _PD), ("beta", _PD), ("gam", _PD), ("jac", _PD),
+                ("xnix", _PD), ("xniy", _PD), ("xnox", _PD), ("xnoy", _PD)]
+
+
+class CfdParams(ctypes.Structure):
+    _fields_ = [("Re", _D), ("Ri", _D), ("Pr", _D), ("F", _D), ("alpha_deg", _D), ("dt", _D),
+                ("tol_mom", _D), ("atol_mom", _D), ("tol_p", _D), ("atol_p", _D),
+                ("maxit_mom", ctypes.c_int), ("maxit_p", ctypes.c_int), ("profile", ctypes.c_int),
+                ("fix_T_annw", ctypes.c_int), ("fix_circ_de", ctypes.c_int),
+                ("warm_start", ctypes.c_int), ("omega_p", _D), ("lid_u", _D)]
+
+
+class CfdStepStats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int), ("status", ctypes.c_int), ("it_mom", ctypes.c_int * 5),
+                ("it_p", ctypes.c_int), ("dmax", _D), ("cl", _D), ("cd", _D), ("cm", _D),
+                ("nu", _D), ("circ", _D), ("cl_pr", _D), ("cd_pr", _D), ("cl_vor", _D),
+                ("cd_vor", _D), ("q_l1", _D), ("q_l2", _D), ("q_max", _D), ("dT_l1", _D),
+                ("dT_max", _D), ("p_res_rel", _D), ("mass_res_rel", _D)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "it_mom"}
+        d["it_mom"] = list(self.it_mom)
+        return d
+
+
+class CfdError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    """Load the solver library (raises if it is missing: the product has no CPU path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(os.environ.get("CFD_B200_LIB", LIB_PATH))
+    if not path.exists():
+        raise CfdError(f"{path} not built: run `make -C cfd_solver_b200/csrc` "
+                       "(or __graft_entry__.build()); there is no CPU fallback")
+    L = ctypes.CDLL(str(path))
+    vp = ctypes.c_void_p
+    L.cfd_params_default.argtypes = [ctypes.POINTER(CfdParams)]
+    L.cfd_params_default.restype = None
+    L.cfd_last_error.restype = ctypes.c_char_p
+    L.cfd_device_count.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    L.cfd_case_create.argtypes = [ctypes.POINTER(CfdGrid), ctypes.POINTER(CfdParams), ctypes.POINTER(vp)]
+    L.cfd_case_step.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CfdStepStats)]
+    L.cfd_case_solve_to.argtypes = [vp, _D, ctypes.c_int, ctypes.POINTER(CfdStepStats)]
+    L.cfd_case_get_fields.argtypes = [vp] + [_PD] * 6
+    L.cfd_case_destroy.argtypes = [vp]
+    L.cfd_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(CfdGrid), ctypes.POINTER(CfdParams),
+                                   ctypes.POINTER(vp)]
+    L.cfd_batch_step.argtypes = [vp, ctypes.c_int]
+    L.cfd_batch_stats.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CfdStepStats)]
+    L.cfd_batch_get_plane.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, _PD]
+    L.cfd_batch_destroy.argtypes = [vp]
+    L.cfd_case_bytes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.cfd_case_bytes.restype = ctypes.c_size_t
+    L.cfd_batch_profile.argtypes = [vp, ctypes.c_int]
+    L.cfd_batch_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p), _PD,
+                                         ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+    L.cfd_batch_sync.argtypes = [vp]
+    for name in SYMBOLS:
+        if name not in ("cfd_params_default", "cfd_last_error", "cfd_case_bytes"):
+            getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def check(rc: int, what: str = ""):
+    if rc != OK:
+        msg = lib().cfd_last_error().decode(errors="replace")
+        raise CfdError(f"{what}: {ERRORS.get(rc, rc)}: {msg}")
+
+
+def default_params(**overrides) -> CfdParams:
+    p = CfdParams()
+    lib().cfd_params_default(ctypes.byref(p))
+    alias = {"alpha": "alpha_deg"}
+    for k, v in overrides.items():
+        k = alias.get(k, k)
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def make_grid(g) -> tuple[CfdGrid, list]:
+    """CfdGrid view of a cfd_solver_b200.grid.Grid; returns (struct, keep-alive arrays)."""
+    keep = []
+
+    def ptr(a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        return a.ctypes.data_as(_PD)
+
+    s = CfdGrid(n0=g.n0, n1=g.n1, dxi0=g.dxi0, dxi1=g.dxi1, p_grid=g.p_grid, a_grid=g.a_grid, ar=g.ar,
+                x=ptr(g.x), y=ptr(g.y), xix=ptr(g.xix), xiy=ptr(g.xiy), etx=ptr(g.etx),
+                ety=ptr(g.ety), alph=ptr(g.alph), beta=ptr(g.beta), gam=ptr(g.gam),
+                jac=ptr(g.jac), xnix=ptr(g.xnix), xniy=ptr(g.xniy), xnox=ptr(g.xnox),
+                xnoy=ptr(g.xnoy))
+    return s, keep

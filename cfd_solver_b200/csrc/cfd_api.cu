@@ -1,0 +1,822 @@
+// cfd_api.cu -- host runtime and C ABI (include/cfd_b200.h).
+//
+// A batch owns one FP64 arena (NPLANES planes per case), one FP32 arena (the
+// multigrid hierarchy), a device case table, the tile tables of every level
+// and one CUDA stream. One time step of every case in the batch is a fixed
+// sequence of launches (the step of PSolver.cpp:1058-1983); the inner solves
+// iterate on the device and the host only reads a 4-byte "cases still
+// iterating" counter to decide when to stop launching.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cfd_b200.h"
+#include "cfd_common.cuh"
+#include "cfd_kernels.cuh"
+#include "cfd_reduce.cuh"
+
+using namespace cfd;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(e_ == cudaErrorMemoryAllocation ? CFD_E_OOM : CFD_E_CUDA,         \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));              \
+    } while (0)
+
+long long rup(long long x, long long a) { return (x + a - 1) / a * a; }
+
+enum KernelId {
+    K_ASSEMBLE_P, K_RHS, K_JAC, K_UPBC, K_FACE_Q, K_BICG_P, K_SPMV, K_BICG_S, K_BICG_X,
+    K_MG_SMOOTH, K_MG_RESID, K_MG_RESTRICT, K_MG_PROLONG, K_MG_COARSE, K_MG_GALERKIN,
+    K_CORRECT, K_BC, K_DIAG, K_SI, NKERNEL
+};
+const char* kKernelNames[NKERNEL] = {
+    "k_assemble_p", "k_rhs", "k_jac", "k_upbc", "k_face_q", "k_bicg_p", "k_spmv", "k_bicg_s",
+    "k_bicg_x", "k_mg_smooth", "k_mg_resid", "k_mg_restrict", "k_mg_prolong", "k_mg_coarse",
+    "k_mg_galerkin", "k_correct", "k_bc", "k_diag", "k_si"};
+
+struct LevelGeom {
+    int W, n1, ld, ilo, ihi;
+    long long ps;
+};
+
+// multigrid hierarchy of a case: coarsen by 2 while the level stays even-sized
+std::vector<LevelGeom> build_levels(int W, int n1, int periodic) {
+    std::vector<LevelGeom> L;
+    int w = W, n = n1;
+    for (int l = 0; l < MAXLEV; l++) {
+        LevelGeom g;
+        g.W = w;
+        g.n1 = n;
+        g.ld = (int)rup(w + 2 * H, 32);
+        g.ps = rup(32 + (long long)n * g.ld, 32);
+        g.ilo = periodic ? 0 : 1;
+        g.ihi = periodic ? w - 1 : w - 2;
+        L.push_back(g);
+        if ((long long)(g.ihi - g.ilo + 1) * (n - 2) <= 64) break;
+        bool can;
+        int wc, nc;
+        if (periodic) {
+            can = (w % 2 == 0) && (w / 2 >= 4);
+            wc = w / 2;
+        } else {
+            can = ((w - 1) % 2 == 0) && ((w - 1) / 2 + 1 >= 5);
+            wc = (w - 1) / 2 + 1;
+        }
+        can = can && ((n - 1) % 2 == 0) && ((n - 1) / 2 + 1 >= 4);
+        nc = (n - 1) / 2 + 1;
+        if (!can) break;
+        w = wc;
+        n = nc;
+    }
+    return L;
+}
+
+struct CaseGeom {
+    int W, ld, ilo, ihi, periodic;
+    long long ps;
+    std::vector<LevelGeom> lev;
+    long long bytes64() const { return (long long)NPLANES * ps + 16; }
+    long long words32() const {
+        long long s = 0;
+        for (auto& g : lev) s += (long long)NMG * g.ps + 32;
+        return s;
+    }
+};
+
+CaseGeom case_geom(int n0, int n1, int profile) {
+    CaseGeom g;
+    g.periodic = profile == CFD_PROFILE_OGRID;
+    g.W = g.periodic ? n0 - 1 : n0;
+    g.ld = (int)rup(g.W + 2 * H, 16);
+    g.ps = rup(16 + (long long)n1 * g.ld, 16);
+    g.ilo = g.periodic ? 0 : 1;
+    g.ihi = g.periodic ? g.W - 1 : n0 - 2;
+    g.lev = build_levels(g.W, n1, g.periodic);
+    return g;
+}
+
+struct Launch {
+    int id;
+    cudaEvent_t e0, e1;
+};
+
+}  // namespace
+
+struct cfd_batch {
+    int n = 0;
+    std::vector<CaseDev> hc;
+    std::vector<cfd_params> prm;
+    std::vector<CaseGeom> geom;
+    std::vector<double> q_l2_first;
+    CaseDev* dc = nullptr;
+    double* f64 = nullptr;
+    float* f32 = nullptr;
+    long long n64 = 0, n32 = 0;
+    double* scal = nullptr;
+    int* iscal = nullptr;
+    double* partial = nullptr;
+    unsigned int* counter = nullptr;
+    int* flags = nullptr;  // [0] active (pressure), [1] mactive (momentum)
+    int* h_flags = nullptr;
+    Tile* dtiles = nullptr;
+    int* dcc = nullptr;
+    BatchDev bd{};
+    int nlev_max = 0;
+    int ncol[MAXLEV] = {};
+    int maxit_mom = 100, maxit_p = 200;
+    int coarse_sweeps = 30;
+    int max_W = 0;
+    int cur = 0;
+    long long steps_done = 0;
+    cudaStream_t st = nullptr;
+    int dev = 0;
+    // profiling
+    bool prof = false;
+    std::vector<Launch> pending;
+    std::vector<cudaEvent_t> pool;
+    double kt_ms[NKERNEL] = {};
+    long long kt_n[NKERNEL] = {};
+    // host staging
+    std::vector<double> hscal;
+    std::vector<int> hiscal;
+};
+
+namespace {
+
+cudaEvent_t get_event(cfd_batch* b) {
+    if (!b->pool.empty()) {
+        cudaEvent_t e = b->pool.back();
+        b->pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct Prof {
+    cfd_batch* b;
+    int id;
+    cudaEvent_t e0{}, e1{};
+    Prof(cfd_batch* b_, int id_) : b(b_), id(id_) {
+        if (b->prof) {
+            e0 = get_event(b);
+            e1 = get_event(b);
+            cudaEventRecord(e0, b->st);
+        }
+    }
+    ~Prof() {
+        if (b->prof) {
+            cudaEventRecord(e1, b->st);
+            b->pending.push_back({id, e0, e1});
+        }
+    }
+};
+
+int flush_profile(cfd_batch* b) {
+    if (b->pending.empty()) return CFD_OK;
+    CK(cudaStreamSynchronize(b->st));
+    for (auto& l : b->pending) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, l.e0, l.e1);
+        b->kt_ms[l.id] += ms;
+        b->kt_n[l.id] += 1;
+        b->pool.push_back(l.e0);
+        b->pool.push_back(l.e1);
+    }
+    b->pending.clear();
+    return CFD_OK;
+}
+
+int read_flag(cfd_batch* b, int idx, int* out) {
+    CK(cudaMemcpyAsync(b->h_flags + idx, b->flags + idx, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    *out = b->h_flags[idx];
+    return CFD_OK;
+}
+
+// host copy of one padded plane: [j][i] with n0 columns (the seam column of the
+// O-grid is the halo copy of column 0)
+void pad_plane(const CaseDev& c, const double* src, std::vector<double>& dst) {
+    dst.assign((size_t)c.ps, 0.0);
+    double* o = dst.data() + 16;  // column 0 of row 0
+    for (int j = 0; j < c.n1; j++) {
+        double* row = o + (long long)j * c.ld;
+        const double* s = src + (size_t)j * c.n0;
+        if (c.periodic) {
+            for (int i = 0; i < c.W; i++) row[i] = s[i];
+            row[-2] = s[c.W - 2];
+            row[-1] = s[c.W - 1];
+            row[c.W] = s[0];
+            row[c.W + 1] = s[1];
+        } else {
+            for (int i = 0; i < c.n0; i++) row[i] = s[i];
+        }
+    }
+}
+
+void unpad_plane(const CaseDev& c, const double* padded, double* out) {
+    const double* o = padded + 16;
+    for (int j = 0; j < c.n1; j++) {
+        const double* row = o + (long long)j * c.ld;
+        double* d = out + (size_t)j * c.n0;
+        if (c.periodic) {
+            for (int i = 0; i < c.W; i++) d[i] = row[i];
+            d[c.n0 - 1] = row[c.W];
+        } else {
+            for (int i = 0; i < c.n0; i++) d[i] = row[i];
+        }
+    }
+}
+
+int check_params(const cfd_grid* g, const cfd_params* p) {
+    if (!g || !p) return fail(CFD_E_ARG, "null grid or params");
+    if (p->profile != CFD_PROFILE_OGRID && p->profile != CFD_PROFILE_CAVITY)
+        return fail(CFD_E_ARG, "unknown profile");
+    if (g->n0 < 8 || g->n1 < 6) return fail(CFD_E_ARG, "grid too small (need n0 >= 8, n1 >= 6)");
+    if (g->n0 > 8192 || g->n1 > 8192) return fail(CFD_E_ARG, "grid too large (n0, n1 <= 8192)");
+    if (!(g->dxi0 > 0) || !(g->dxi1 > 0)) return fail(CFD_E_ARG, "non-positive grid spacing");
+    if (!g->x || !g->y || !g->xix || !g->xiy || !g->etx || !g->ety || !g->alph || !g->beta ||
+        !g->gam || !g->jac || !g->xnix || !g->xniy || !g->xnox || !g->xnoy)
+        return fail(CFD_E_ARG, "missing grid plane");
+    if (!(p->dt > 0) || !(p->Re > 0) || !(p->Pr > 0)) return fail(CFD_E_ARG, "dt, Re, Pr must be > 0");
+    if (p->maxit_mom < 2 || p->maxit_p < 1) return fail(CFD_E_ARG, "iteration caps too small");
+    const size_t N = (size_t)g->n0 * g->n1;
+    for (size_t k = 0; k < N; k++) {
+        if (!(g->alph[k] > 0) || !(g->gam[k] > 0) || !std::isfinite(g->beta[k]) || !std::isfinite(g->jac[k]))
+            return fail(CFD_E_ARG, "grid metrics invalid (alpha, gamma must be > 0)");
+    }
+    return CFD_OK;
+}
+
+// initial state of PSolver.cpp:614-748 (O-grid) or the cavity's
+void initial_state(const cfd_grid* g, const cfd_params* p, const CaseDev& c, std::vector<double>* st) {
+    // st: u, v, T, up, vp, p (n1*n0, [j][i])
+    const int n0 = g->n0, n1 = g->n1;
+    const size_t N = (size_t)n0 * n1;
+    for (int m = 0; m < 6; m++) st[m].assign(N, 0.0);
+    if (p->profile == CFD_PROFILE_CAVITY) {
+        for (int i = 1; i < n0 - 1; i++) {
+            st[0][(size_t)(n1 - 1) * n0 + i] = p->lid_u;
+            st[3][(size_t)(n1 - 1) * n0 + i] = p->lid_u;
+        }
+        for (int i = 0; i < n0; i++) st[2][i] = 1.0;
+        return;
+    }
+    for (size_t k = 0; k < N; k++) {
+        st[0][k] = c.uinf; st[1][k] = c.vinf; st[3][k] = c.uinf; st[4][k] = c.vinf;
+    }
+    for (int i = 0; i < n0; i++) {
+        st[0][i] = -c.speed_amp * g->y[i];
+        st[1][i] = c.speed_amp * g->x[i];
+        st[3][i] = st[0][i];
+        st[4][i] = st[1][i];
+        st[2][i] = 1.0;
+    }
+    const int j = n1 - 1;
+    for (int i = 0; i < n0 - 1; i++) {
+        const size_t k = (size_t)j * n0 + i;
+        const double vnn = st[0][k] * g->xnox[i] + st[1][k] * g->xnoy[i];
+        if (vnn >= 0) {
+            st[0][k] = c.uinf; st[1][k] = c.vinf; st[2][k] = 0.0;
+            st[3][k] = st[0][k]; st[4][k] = st[1][k];
+        } else {
+            const size_t kb = k - n0;
+            st[0][k] = st[0][kb]; st[1][k] = st[1][kb]; st[2][k] = st[2][kb];
+            if (i == 0) {
+                const size_t s = (size_t)j * n0 + n0 - 1;
+                st[0][s] = st[0][k]; st[1][s] = st[1][k]; st[2][s] = st[2][k];
+            }
+        }
+    }
+}
+
+void make_tiles(int ilo, int ihi, int n1, int cid, std::vector<Tile>& out) {
+    int k = 0;
+    for (int j0 = 1; j0 <= n1 - 2; j0 += TY)
+        for (int i0 = (ilo / TX) * TX; i0 <= ihi; i0 += TX) out.push_back({cid, i0, j0, k++});
+}
+
+// --------------------------------------------------------------------------
+// one time step of every case in the batch
+int run_vcycle(cfd_batch* b) {
+    BatchDev& bd = b->bd;
+    for (int l = 0; l < b->nlev_max; l++) {
+        if (bd.nccases[l] > 0) {
+            Prof pr(b, K_MG_COARSE);
+            k_mg_coarse<<<bd.nccases[l], 1024, 0, b->st>>>(bd, l, b->coarse_sweeps);
+        }
+        if (bd.nmtiles[l] > 0) {
+            for (int col = 0; col < b->ncol[l]; col++) {
+                Prof pr(b, K_MG_SMOOTH);
+                k_mg_smooth<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l, col);
+            }
+            {
+                Prof pr(b, K_MG_RESID);
+                k_mg_resid<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l);
+            }
+            {
+                Prof pr(b, K_MG_RESTRICT);
+                k_mg_restrict<<<bd.natiles[l + 1], NT, 0, b->st>>>(bd, l);
+            }
+        }
+    }
+    for (int l = b->nlev_max - 2; l >= 0; l--) {
+        if (bd.nmtiles[l] == 0) continue;
+        {
+            Prof pr(b, K_MG_PROLONG);
+            k_mg_prolong<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l);
+        }
+        for (int col = b->ncol[l] - 1; col >= 0; col--) {
+            Prof pr(b, K_MG_SMOOTH);
+            k_mg_smooth<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l, col);
+        }
+    }
+    return CFD_OK;
+}
+
+int one_step(cfd_batch* b) {
+    BatchDev& bd = b->bd;
+    bd.cur = b->cur;
+    const int nf = bd.nftiles;
+    CK(cudaMemsetAsync(b->flags, 0, 2 * sizeof(int), b->st));
+    {
+        Prof pr(b, K_RHS);
+        k_rhs<<<nf, NT, 0, b->st>>>(bd);
+    }
+    // momentum / energy solves: sweeps in pairs until every (case, field) stopped
+    const int npairs = std::max(1, b->maxit_mom / 2);
+    for (int pair = 0; pair < npairs; pair++) {
+        {
+            Prof pr(b, K_JAC);
+            k_jac<<<nf, NT, 0, b->st>>>(bd, 1, pair == 0, 0);
+        }
+        {
+            Prof pr(b, K_JAC);
+            k_jac<<<nf, NT, 0, b->st>>>(bd, 0, 0, 1);
+        }
+        int m = 0;
+        int rc = read_flag(b, 1, &m);
+        if (rc) return rc;
+        if (m <= 0) break;
+    }
+    {
+        Prof pr(b, K_UPBC);
+        k_upbc<<<b->n, BC_THREADS, 0, b->st>>>(bd);
+    }
+    {
+        Prof pr(b, K_FACE_Q);
+        k_face_q<<<nf, NT, 0, b->st>>>(bd);
+    }
+    for (int it = 0; it < b->maxit_p; it++) {
+        int a = 0;
+        int rc = read_flag(b, 0, &a);
+        if (rc) return rc;
+        if (a <= 0) break;
+        { Prof pr(b, K_BICG_P); k_bicg_p<<<nf, NT, 0, b->st>>>(bd); }
+        run_vcycle(b);
+        { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 0); }
+        { Prof pr(b, K_BICG_S); k_bicg_s<<<nf, NT, 0, b->st>>>(bd); }
+        run_vcycle(b);
+        { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 1); }
+        { Prof pr(b, K_BICG_X); k_bicg_x<<<nf, NT, 0, b->st>>>(bd, b->maxit_p); }
+    }
+    {
+        Prof pr(b, K_CORRECT);
+        k_correct<<<nf, NT, 0, b->st>>>(bd);
+    }
+    {
+        Prof pr(b, K_BC);
+        k_bc<<<b->n, BC_THREADS, 2 * (b->max_W + 1) * sizeof(double), b->st>>>(bd);
+    }
+    {
+        Prof pr(b, K_DIAG);
+        k_diag<<<nf, NT, 0, b->st>>>(bd);
+    }
+    CK(cudaGetLastError());
+    b->cur ^= 1;
+    b->steps_done++;
+    if (b->prof) return flush_profile(b);
+    return CFD_OK;
+}
+
+int fetch_scalars(cfd_batch* b) {
+    b->hscal.resize((size_t)b->n * NSCAL);
+    b->hiscal.resize((size_t)b->n * NISCAL);
+    CK(cudaMemcpyAsync(b->hscal.data(), b->scal, b->hscal.size() * sizeof(double), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(b->hiscal.data(), b->iscal, b->hiscal.size() * sizeof(int), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    for (int c = 0; c < b->n; c++) {
+        if (b->q_l2_first[c] < 0 && b->steps_done > 0) b->q_l2_first[c] = b->hscal[(size_t)c * NSCAL + S_QL2];
+    }
+    return CFD_OK;
+}
+
+void fill_stats(cfd_batch* b, int c, cfd_step_stats* s) {
+    const double* sc = b->hscal.data() + (size_t)c * NSCAL;
+    const int* is = b->hiscal.data() + (size_t)c * NISCAL;
+    memset(s, 0, sizeof(*s));
+    s->status = is[I_STATUS] | is[I_PSTATUS];
+    for (int f = 0; f < NFIELD; f++) s->it_mom[f] = is[I_MIT0 + f];
+    s->it_p = is[I_PIT];
+    s->dmax = sc[S_DMAX];
+    s->cl = sc[S_CL]; s->cd = sc[S_CD]; s->cm = sc[S_CM]; s->nu = sc[S_NU]; s->circ = sc[S_CIRC];
+    s->cl_pr = sc[S_CLP]; s->cd_pr = sc[S_CDP]; s->cl_vor = sc[S_CLV]; s->cd_vor = sc[S_CDV];
+    s->q_l1 = sc[S_QL1]; s->q_l2 = sc[S_QL2]; s->q_max = sc[S_QMAX];
+    s->dT_l1 = sc[S_DTL1]; s->dT_max = sc[S_DTMAX];
+    s->p_res_rel = sc[S_NB1] > 0 ? sc[S_RL1] / sc[S_NB1] : 0.0;
+    const double q0 = b->q_l2_first[c];
+    s->mass_res_rel = q0 > 0 ? sc[S_QL2] / q0 : (sc[S_QL2] == 0 ? 0.0 : 1.0);
+}
+
+int plane_id(const char* name, int cur) {
+    struct { const char* n; int id; } t[] = {
+        {"x", P_X}, {"y", P_Y}, {"xix", P_XIX}, {"xiy", P_XIY}, {"etx", P_ETX}, {"ety", P_ETY},
+        {"alph", P_ALPH}, {"beta", P_BETA}, {"gam", P_GAM}, {"jac", P_JAC},
+        {"ap", P_AP}, {"ae", P_AE}, {"aw", P_AW}, {"an", P_AN}, {"as", P_AS}, {"ane", P_ANE},
+        {"anw", P_ANW}, {"ase", P_ASE}, {"asw", P_ASW},
+        {"u", P_U}, {"v", P_V}, {"p", P_P}, {"T", P_T0 + cur}, {"up", P_UP0 + cur}, {"vp", P_VP0 + cur},
+        {"us", P_US}, {"vs", P_VS}, {"qu", P_RU}, {"qv", P_RV}, {"qt", P_RT}, {"qup", P_RUP},
+        {"qvp", P_RVP}, {"q", P_Q}, {"pcor", P_PCOR}, {"vort", P_VORT}, {"si", P_SI}, {"dil", P_DIL}};
+    for (auto& e : t)
+        if (strcmp(e.n, name) == 0) return e.id;
+    return -1;
+}
+
+}  // namespace
+
+// ==========================================================================
+extern "C" {
+
+void cfd_params_default(cfd_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->Re = 1000.0; p->Ri = 0.0; p->Pr = 0.71; p->F = 0.0; p->alpha_deg = 82.0; p->dt = 0.01e-2;
+    p->tol_mom = 0.75e-2; p->atol_mom = 0.0; p->tol_p = 0.75e-2; p->atol_p = 0.0;
+    p->maxit_mom = 100; p->maxit_p = 200;
+    p->profile = CFD_PROFILE_OGRID;
+    p->fix_T_annw = 0; p->fix_circ_de = 0; p->warm_start = 1;
+    p->omega_p = 1.0; p->lid_u = 1.0;
+}
+
+const char* cfd_last_error(void) { return g_err.c_str(); }
+
+int cfd_device_count(int* count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (count) *count = (e == cudaSuccess) ? n : 0;
+    if (e != cudaSuccess) return fail(CFD_E_CUDA, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    return CFD_OK;
+}
+
+size_t cfd_case_bytes(int n0, int n1, int profile) {
+    if (n0 < 8 || n1 < 6) return 0;
+    CaseGeom g = case_geom(n0, n1, profile);
+    long long ntiles = (long long)((n1 - 2 + TY - 1) / TY) * ((g.W + TX - 1) / TX + 1);
+    return (size_t)(g.bytes64() * 8 + g.words32() * 4 + ntiles * (PSTRIDE * 8 + sizeof(Tile) * 3) +
+                    sizeof(CaseDev) + (NSCAL * 8 + NISCAL * 4));
+}
+
+int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params, cfd_batch** out) {
+    if (!out || ncases <= 0 || !grids || !params) return fail(CFD_E_ARG, "bad batch arguments");
+    *out = nullptr;
+    for (int c = 0; c < ncases; c++) {
+        int rc = check_params(&grids[c], &params[c]);
+        if (rc) return fail(rc, "case " + std::to_string(c) + ": " + g_err);
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(CFD_E_CUDA, "no CUDA device available (this library has no CPU path)");
+    cfd_batch* b = new cfd_batch();
+    b->n = ncases;
+    cudaGetDevice(&b->dev);
+    auto cleanup = [&](int rc) { cfd_batch_destroy(b); return rc; };
+    if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(CFD_E_CUDA, "stream creation failed"));
+
+    // ---- geometry, offsets, tiles
+    long long off64 = 0, off32 = 0;
+    std::vector<Tile> ftiles;
+    std::vector<std::vector<Tile>> at(MAXLEV), mt(MAXLEV);
+    std::vector<std::vector<int>> cc(MAXLEV);
+    b->hc.resize(ncases);
+    b->prm.assign(params, params + ncases);
+    b->q_l2_first.assign(ncases, -1.0);
+    b->maxit_mom = 0;
+    b->maxit_p = 0;
+    for (int c = 0; c < ncases; c++) {
+        const cfd_grid& g = grids[c];
+        const cfd_params& p = params[c];
+        CaseGeom G = case_geom(g.n0, g.n1, p.profile);
+        b->geom.push_back(G);
+        CaseDev& d = b->hc[c];
+        memset(&d, 0, sizeof(d));
+        d.W = G.W; d.n0 = g.n0; d.n1 = g.n1; d.ld = G.ld;
+        d.periodic = G.periodic; d.ilo = G.ilo; d.ihi = G.ihi; d.profile = p.profile;
+        d.base = off64 + 16 - H;
+        d.ps = G.ps;
+        off64 += G.bytes64() - 16 + 16;
+        off64 = rup(off64, 16);
+        d.fix_T_annw = p.fix_T_annw; d.fix_circ_de = p.fix_circ_de; d.warm_up = p.warm_start;
+        d.d0 = g.dxi0; d.d1 = g.dxi1; d.dt = p.dt; d.Re = p.Re; d.Pr = p.Pr; d.Ri = p.Ri; d.F = p.F;
+        d.Pi = acos(-1.0);
+        const double thetamax = d.Pi / 12.0;
+        d.speed_amp = thetamax * 2.0 * d.Pi * p.F;
+        d.accn_amp = 2.0 * d.Pi * p.F * d.speed_amp;
+        d.uinf = sin(p.alpha_deg * d.Pi / 180.0);
+        d.vinf = cos(p.alpha_deg * d.Pi / 180.0);
+        d.sa = sin(p.alpha_deg * d.Pi / 180.0);
+        d.ca = cos(p.alpha_deg * d.Pi / 180.0);
+        d.ar = g.ar; d.omega_p = p.omega_p; d.lid_u = p.lid_u;
+        d.tol_mom = p.tol_mom; d.atol_mom = p.atol_mom; d.tol_p = p.tol_p; d.atol_p = p.atol_p;
+        d.tile_begin = (int)ftiles.size();
+        make_tiles(G.ilo, G.ihi, g.n1, c, ftiles);
+        d.tile_count = (int)ftiles.size() - d.tile_begin;
+        d.nlev = (int)G.lev.size();
+        for (int l = 0; l < d.nlev; l++) {
+            const LevelGeom& lg = G.lev[l];
+            LevelDev& L = d.lev[l];
+            L.W = lg.W; L.n1 = lg.n1; L.ld = lg.ld; L.ilo = lg.ilo; L.ihi = lg.ihi; L.nlo = lg.ilo;
+            L.base = off32 + 32 - H;
+            L.ps = lg.ps;
+            off32 += (long long)NMG * lg.ps + 32;
+            off32 = rup(off32, 32);
+            L.tile_begin = (int)at[l].size();
+            make_tiles(lg.ilo, lg.ihi, lg.n1, c, at[l]);
+            L.tile_count = (int)at[l].size() - L.tile_begin;
+            if (l < d.nlev - 1) make_tiles(lg.ilo, lg.ihi, lg.n1, c, mt[l]);
+            else cc[l].push_back(c);
+            b->ncol[l] = std::max(b->ncol[l], (G.periodic && (lg.W & 1)) ? 6 : 4);
+        }
+        b->nlev_max = std::max(b->nlev_max, d.nlev);
+        b->max_W = std::max(b->max_W, d.W);
+        b->maxit_mom = std::max(b->maxit_mom, p.maxit_mom);
+        b->maxit_p = std::max(b->maxit_p, p.maxit_p);
+    }
+    if (b->max_W > 4096) return cleanup(fail(CFD_E_ARG, "grid width above 4096 columns"));
+    b->n64 = off64 + 16;
+    b->n32 = off32 + 32;
+
+    // ---- device allocations
+    size_t ntl = ftiles.size();
+    for (int l = 0; l < MAXLEV; l++) ntl += at[l].size() + mt[l].size();
+    size_t ncc = 0;
+    for (int l = 0; l < MAXLEV; l++) ncc += cc[l].size();
+#define ALLOC(ptr, bytes)                                                         \
+    do {                                                                          \
+        cudaError_t e_ = cudaMalloc((void**)&(ptr), (bytes));                     \
+        if (e_ != cudaSuccess)                                                    \
+            return cleanup(fail(CFD_E_OOM, std::string("cudaMalloc ") + #ptr + ": " + cudaGetErrorString(e_))); \
+    } while (0)
+    ALLOC(b->f64, (size_t)b->n64 * sizeof(double));
+    ALLOC(b->f32, (size_t)b->n32 * sizeof(float));
+    ALLOC(b->dc, sizeof(CaseDev) * ncases);
+    ALLOC(b->scal, sizeof(double) * NSCAL * ncases);
+    ALLOC(b->iscal, sizeof(int) * NISCAL * ncases);
+    ALLOC(b->partial, sizeof(double) * PSTRIDE * std::max<size_t>(ftiles.size(), 1));
+    ALLOC(b->counter, sizeof(unsigned) * ncases);
+    ALLOC(b->flags, sizeof(int) * 4);
+    ALLOC(b->dtiles, sizeof(Tile) * std::max<size_t>(ntl, 1));
+    ALLOC(b->dcc, sizeof(int) * std::max<size_t>(ncc, 1));
+#undef ALLOC
+    if (cudaHostAlloc((void**)&b->h_flags, sizeof(int) * 4, cudaHostAllocDefault) != cudaSuccess)
+        return cleanup(fail(CFD_E_CUDA, "pinned allocation failed"));
+    cudaMemsetAsync(b->f64, 0, (size_t)b->n64 * sizeof(double), b->st);
+    cudaMemsetAsync(b->f32, 0, (size_t)b->n32 * sizeof(float), b->st);
+    cudaMemsetAsync(b->scal, 0, sizeof(double) * NSCAL * ncases, b->st);
+    cudaMemsetAsync(b->iscal, 0, sizeof(int) * NISCAL * ncases, b->st);
+    cudaMemsetAsync(b->counter, 0, sizeof(unsigned) * ncases, b->st);
+    CK(cudaStreamSynchronize(b->st));
+    {
+        const size_t smem = 2 * (size_t)(b->max_W + 1) * sizeof(double);
+        if (smem > 48 * 1024)
+            CK(cudaFuncSetAttribute(k_bc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+
+    // ---- tile tables
+    std::vector<Tile> all(ftiles);
+    std::vector<int> allcc;
+    size_t pos_at[MAXLEV], pos_mt[MAXLEV], pos_cc[MAXLEV];
+    for (int l = 0; l < MAXLEV; l++) {
+        pos_at[l] = all.size();
+        all.insert(all.end(), at[l].begin(), at[l].end());
+        pos_mt[l] = all.size();
+        all.insert(all.end(), mt[l].begin(), mt[l].end());
+        pos_cc[l] = allcc.size();
+        allcc.insert(allcc.end(), cc[l].begin(), cc[l].end());
+    }
+    CK(cudaMemcpy(b->dtiles, all.data(), sizeof(Tile) * all.size(), cudaMemcpyHostToDevice));
+    if (!allcc.empty())
+        CK(cudaMemcpy(b->dcc, allcc.data(), sizeof(int) * allcc.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->dc, b->hc.data(), sizeof(CaseDev) * ncases, cudaMemcpyHostToDevice));
+
+    BatchDev& bd = b->bd;
+    bd.cases = b->dc; bd.ncases = ncases; bd.f64 = b->f64; bd.f32 = b->f32;
+    bd.scal = b->scal; bd.iscal = b->iscal; bd.partial = b->partial; bd.counter = b->counter;
+    bd.active = b->flags; bd.mactive = b->flags + 1;
+    bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
+    for (int l = 0; l < MAXLEV; l++) {
+        bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
+        bd.mtiles[l] = b->dtiles + pos_mt[l]; bd.nmtiles[l] = (int)mt[l].size();
+        bd.ccases[l] = b->dcc + pos_cc[l]; bd.nccases[l] = (int)cc[l].size();
+    }
+
+    // ---- upload grid + initial state (padded planes with halos)
+    std::vector<double> pad;
+    for (int c = 0; c < ncases; c++) {
+        const cfd_grid& g = grids[c];
+        const CaseDev& d = b->hc[c];
+        const double* gp[10] = {g.x, g.y, g.xix, g.xiy, g.etx, g.ety, g.alph, g.beta, g.gam, g.jac};
+        const int gid[10] = {P_X, P_Y, P_XIX, P_XIY, P_ETX, P_ETY, P_ALPH, P_BETA, P_GAM, P_JAC};
+        for (int m = 0; m < 10; m++) {
+            pad_plane(d, gp[m], pad);
+            CK(cudaMemcpy(b->f64 + d.base + H - 16 + (long long)gid[m] * d.ps, pad.data(),
+                          sizeof(double) * d.ps, cudaMemcpyHostToDevice));
+        }
+        // normals as rows 0..3 of P_VEC
+        std::vector<double> vec((size_t)g.n0 * g.n1, 0.0);
+        const double* nv[4] = {g.xnix, g.xniy, g.xnox, g.xnoy};
+        for (int r = 0; r < 4 && r < g.n1; r++)
+            for (int i = 0; i < g.n0; i++) vec[(size_t)r * g.n0 + i] = nv[r][i];
+        pad_plane(d, vec.data(), pad);
+        CK(cudaMemcpy(b->f64 + d.base + H - 16 + (long long)P_VEC * d.ps, pad.data(), sizeof(double) * d.ps,
+                      cudaMemcpyHostToDevice));
+        std::vector<double> st[6];
+        initial_state(&g, &params[c], d, st);
+        const int sid[6] = {P_U, P_V, P_T0, P_UP0, P_VP0, P_P};
+        for (int m = 0; m < 6; m++) {
+            pad_plane(d, st[m].data(), pad);
+            CK(cudaMemcpy(b->f64 + d.base + H - 16 + (long long)sid[m] * d.ps, pad.data(),
+                          sizeof(double) * d.ps, cudaMemcpyHostToDevice));
+        }
+    }
+    // ---- set-up kernels: pressure stencil, multigrid hierarchy
+    b->cur = 0;
+    bd.cur = 0;
+    {
+        Prof pr(b, K_ASSEMBLE_P);
+        k_assemble_p<<<bd.nftiles, NT, 0, b->st>>>(bd);
+    }
+    for (int l = 0; l + 1 < b->nlev_max; l++) {
+        if (bd.natiles[l + 1] == 0) continue;
+        Prof pr(b, K_MG_GALERKIN);
+        k_mg_galerkin<<<bd.natiles[l + 1], NT, 0, b->st>>>(bd, l);
+    }
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(b->st) != cudaSuccess)
+        return cleanup(fail(CFD_E_CUDA, "set-up kernels failed"));
+    flush_profile(b);
+    *out = b;
+    return CFD_OK;
+}
+
+int cfd_batch_step(cfd_batch* b, int nsteps) {
+    if (!b || nsteps < 0) return fail(CFD_E_ARG, "bad arguments");
+    for (int s = 0; s < nsteps; s++) {
+        int rc = one_step(b);
+        if (rc) return rc;
+        if (s == 0 && b->steps_done == 1) {
+            rc = fetch_scalars(b);
+            if (rc) return rc;
+        }
+    }
+    CK(cudaStreamSynchronize(b->st));
+    return CFD_OK;
+}
+
+int cfd_batch_stats(cfd_batch* b, int case_index, cfd_step_stats* out) {
+    if (!b || !out || case_index < 0 || case_index >= b->n) return fail(CFD_E_ARG, "bad arguments");
+    int rc = fetch_scalars(b);
+    if (rc) return rc;
+    fill_stats(b, case_index, out);
+    return CFD_OK;
+}
+
+int cfd_batch_get_plane(cfd_batch* b, int case_index, const char* name, double* out) {
+    if (!b || !name || !out || case_index < 0 || case_index >= b->n) return fail(CFD_E_ARG, "bad arguments");
+    const CaseDev& d = b->hc[case_index];
+    const int id = plane_id(name, b->cur);
+    if (id < 0) return fail(CFD_E_ARG, std::string("unknown plane ") + name);
+    if (id == P_SI) {
+        b->bd.cur = b->cur;
+        Prof pr(b, K_SI);
+        k_si<<<b->n, BC_THREADS, 0, b->st>>>(b->bd);
+    }
+    std::vector<double> pad((size_t)d.ps);
+    CK(cudaMemcpyAsync(pad.data(), b->f64 + d.base + H - 16 + (long long)id * d.ps, sizeof(double) * d.ps,
+                       cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    unpad_plane(d, pad.data(), out);
+    return CFD_OK;
+}
+
+int cfd_batch_destroy(cfd_batch* b) {
+    if (!b) return CFD_OK;
+    if (b->st) cudaStreamSynchronize(b->st);
+    for (auto& l : b->pending) { cudaEventDestroy(l.e0); cudaEventDestroy(l.e1); }
+    for (auto e : b->pool) cudaEventDestroy(e);
+    cudaFree(b->f64); cudaFree(b->f32); cudaFree(b->dc); cudaFree(b->scal); cudaFree(b->iscal);
+    cudaFree(b->partial); cudaFree(b->counter); cudaFree(b->flags); cudaFree(b->dtiles); cudaFree(b->dcc);
+    if (b->h_flags) cudaFreeHost(b->h_flags);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+    return CFD_OK;
+}
+
+int cfd_batch_profile(cfd_batch* b, int enable) {
+    if (!b) return fail(CFD_E_ARG, "null batch");
+    int rc = flush_profile(b);
+    b->prof = enable != 0;
+    for (int k = 0; k < NKERNEL; k++) { b->kt_ms[k] = 0; b->kt_n[k] = 0; }
+    return rc;
+}
+
+int cfd_batch_kernel_times(cfd_batch* b, const char** names, double* total_ms, long long* launches, int cap) {
+    if (!b) return fail(CFD_E_ARG, "null batch");
+    flush_profile(b);
+    for (int k = 0; k < NKERNEL && k < cap; k++) {
+        if (names) names[k] = kKernelNames[k];
+        if (total_ms) total_ms[k] = b->kt_ms[k];
+        if (launches) launches[k] = b->kt_n[k];
+    }
+    return NKERNEL;
+}
+
+int cfd_batch_sync(cfd_batch* b) {
+    if (!b) return fail(CFD_E_ARG, "null batch");
+    CK(cudaStreamSynchronize(b->st));
+    return CFD_OK;
+}
+
+// ---- single case
+int cfd_case_create(const cfd_grid* g, const cfd_params* prm, cfd_case** out) {
+    return cfd_batch_create(1, g, prm, out);
+}
+
+int cfd_case_step(cfd_case* c, int nsteps, cfd_step_stats* last) {
+    int rc = cfd_batch_step(c, nsteps);
+    if (rc) return rc;
+    if (last) {
+        rc = cfd_batch_stats(c, 0, last);
+        if (rc) return rc;
+        last->steps = nsteps;
+        if (last->status & ST_NAN) return fail(CFD_E_DIVERGED, "NaN in the solution");
+    }
+    return CFD_OK;
+}
+
+int cfd_case_solve_to(cfd_case* c, double mass_tol, int max_steps, cfd_step_stats* last) {
+    if (!c || max_steps < 0) return fail(CFD_E_ARG, "bad arguments");
+    cfd_step_stats s{};
+    int done = 0;
+    const int chunk = 10;
+    while (done < max_steps) {
+        const int n = std::min(chunk, max_steps - done);
+        int rc = cfd_batch_step(c, n);
+        if (rc) return rc;
+        done += n;
+        rc = cfd_batch_stats(c, 0, &s);
+        if (rc) return rc;
+        if (s.status & ST_NAN) {
+            s.steps = done;
+            if (last) *last = s;
+            return fail(CFD_E_DIVERGED, "NaN in the solution");
+        }
+        if (s.mass_res_rel <= mass_tol) break;
+    }
+    s.steps = done;
+    if (last) *last = s;
+    if (s.mass_res_rel > mass_tol) return fail(CFD_E_NOTCONV, "max_steps reached before mass_tol");
+    return CFD_OK;
+}
+
+int cfd_case_get_fields(cfd_case* c, double* u, double* v, double* T, double* p, double* si, double* vort) {
+    if (!c) return fail(CFD_E_ARG, "null case");
+    struct { const char* n; double* o; } f[] = {{"u", u}, {"v", v}, {"T", T}, {"p", p}, {"si", si}, {"vort", vort}};
+    for (auto& e : f) {
+        if (!e.o) continue;
+        int rc = cfd_batch_get_plane(c, 0, e.n, e.o);
+        if (rc) return rc;
+    }
+    return CFD_OK;
+}
+
+int cfd_case_destroy(cfd_case* c) { return cfd_batch_destroy(c); }
+
+}  // extern "C"

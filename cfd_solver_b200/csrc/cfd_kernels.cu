@@ -1,0 +1,1145 @@
+// cfd_kernels.cu -- sm_100a kernels of one projection time step, batched over a case table.
+//
+// Reference mapping (mhsuhail00/CFD_Solver, PSolver.cpp):
+//   k_assemble_p     pressure 9-point stencil            PSolver.cpp:944-1040
+//   k_rhs            contravariant velocities,           PSolver.cpp:1063-1069
+//                    convection + predictor RHS          PSolver.cpp:1075-1237
+//   k_jac            the five gauss() systems            PSolver.cpp:1241-1350, 2280-2446
+//                    (u/v/T coefficients assembled in     PSolver.cpp:752-940
+//                     registers from alpha, beta, gamma)
+//   k_upbc           up/vp far-field condition           PSolver.cpp:1356-1382
+//   k_face_q         face velocities -> continuity q     PSolver.cpp:1390-1449
+//   k_bicg_* / k_mg_*  pressure correction (replaces      PSolver.cpp:1453-1466, 2067-2278
+//                    sip9p): BiCGStab on the stored 9-point stencil, preconditioned by a
+//                    Galerkin multigrid V-cycle with multicolour Gauss-Seidel smoothing
+//   k_correct        pcor BCs + velocity / p correction  PSolver.cpp:1471-1542
+//   k_bc             far-field / wall BCs, circulation,  PSolver.cpp:1549-1783
+//                    boundary pressure, wall integrals   PSolver.cpp:1901-1983
+//   k_diag           dilatation, vorticity, dmax         PSolver.cpp:1807-1853
+//   k_si             stream function (output only)       PSolver.cpp:1789-1801
+#include "cfd_common.cuh"
+#include "cfd_reduce.cuh"
+#include "cfd_kernels.cuh"
+
+namespace cfd {
+
+#define AT(ptr, ii, jj) (ptr)[(long long)(jj) * ld + (ii)]
+
+__device__ __forceinline__ bool near_wall(const CaseDev& c, int i, int j) {
+    if (j == 1 || j == c.n1 - 2) return true;
+    return c.profile == CAVITY && (i == 1 || i == c.n0 - 2);
+}
+
+// ---------------------------------------------------------------------------
+// pressure stencil assembly (PSolver.cpp:944-1040), also the set-up of MG level 0
+__global__ void __launch_bounds__(NT) k_assemble_p(BatchDev b) {
+    const Tile t = b.ftiles[blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
+    const int ld = c.ld, W = c.W, per = c.periodic;
+    const double d0 = c.d0, d1 = c.d1;
+    const double* X = plane(b, c, P_XIX);
+    const double* Y = plane(b, c, P_XIY);
+    const double* E = plane(b, c, P_ETX);
+    const double* G = plane(b, c, P_ETY);
+    const long long k = (long long)j * ld + i, kE = k + 1, kW = k - 1, kN = k + ld, kS = k - ld;
+    double aae = (X[k] / (2.0 * d0 * d0)) * (X[k] + X[kE]);
+    double bbe = (E[k] / (8.0 * d0 * d1)) * (X[kN] - X[kS]);
+    double cce = (Y[k] / (2.0 * d0 * d0)) * (Y[k] + Y[kE]);
+    double dde = (G[k] / (8.0 * d0 * d1)) * (Y[kN] - Y[kS]);
+    const double ae = aae + bbe + cce + dde;
+    double aaw = (X[k] / (2.0 * d0 * d0)) * (X[k] + X[kW]);
+    double bbw = (E[k] / (8.0 * d0 * d1)) * (X[kS] - X[kN]);
+    double ccw = (Y[k] / (2.0 * d0 * d0)) * (Y[k] + Y[kW]);
+    double ddw = (G[k] / (8.0 * d0 * d1)) * (Y[kS] - Y[kN]);
+    const double aw = aaw + bbw + ccw + ddw;
+    double aan = (X[k] / (8.0 * d0 * d1)) * (E[kE] - E[kW]);
+    double bbn = (E[k] / (2.0 * d1 * d1)) * (E[k] + E[kN]);
+    double ccn = (Y[k] / (8.0 * d0 * d1)) * (G[kE] - G[kW]);
+    double ddn = (G[k] / (2.0 * d1 * d1)) * (G[k] + G[kN]);
+    const double an = aan + bbn + ccn + ddn;
+    double aas = (X[k] / (8.0 * d0 * d1)) * (E[kW] - E[kE]);
+    double bbs = (E[k] / (2.0 * d1 * d1)) * (E[k] + E[kS]);
+    double ccs = (Y[k] / (8.0 * d0 * d1)) * (G[kW] - G[kE]);
+    double dds = (G[k] / (2.0 * d1 * d1)) * (G[k] + G[kS]);
+    const double as = aas + bbs + ccs + dds;
+    double aane = (X[k] / (8.0 * d0 * d1)) * (E[k] + E[kE]);
+    double bbne = (E[k] / (8.0 * d0 * d1)) * (X[k] + X[kN]);
+    double ccne = (Y[k] / (8.0 * d0 * d1)) * (G[k] + G[kE]);
+    double ddne = (G[k] / (8.0 * d0 * d1)) * (Y[k] + Y[kN]);
+    const double ane = aane + bbne + ccne + ddne;
+    double aasw = (X[k] / (8.0 * d0 * d1)) * (E[k] + E[kW]);
+    double bbsw = (E[k] / (8.0 * d0 * d1)) * (X[k] + X[kS]);
+    double ccsw = (Y[k] / (8.0 * d0 * d1)) * (G[k] + G[kW]);
+    double ddsw = (G[k] / (8.0 * d0 * d1)) * (Y[k] + Y[kS]);
+    const double asw = aasw + bbsw + ccsw + ddsw;
+    double aanw = -(X[k] / (8.0 * d0 * d1)) * (E[k] + E[kW]);
+    double bbnw = -(E[k] / (8.0 * d0 * d1)) * (X[k] + X[kN]);
+    double ccnw = -(Y[k] / (8.0 * d0 * d1)) * (G[k] + G[kW]);
+    double ddnw = -(G[k] / (8.0 * d0 * d1)) * (Y[k] + Y[kN]);
+    const double anw = aanw + bbnw + ccnw + ddnw;
+    double aase = -(X[k] / (8.0 * d0 * d1)) * (E[k] + E[kE]);
+    double bbse = -(E[k] / (8.0 * d0 * d1)) * (X[k] + X[kS]);
+    double ccse = -(Y[k] / (8.0 * d0 * d1)) * (G[k] + G[kE]);
+    double ddse = -(G[k] / (8.0 * d0 * d1)) * (Y[k] + Y[kS]);
+    const double ase = aase + bbse + ccse + ddse;
+    const double pxi = 1.0 / (2. * d0 * d0);
+    const double pet = 1.0 / (2. * d1 * d1);
+    double aap = -X[k] * (2. * X[k] + X[kW] + X[kE]);
+    double bbp = -E[k] * (2. * E[k] + E[kS] + E[kN]);
+    double ccp = -Y[k] * (2. * Y[k] + Y[kW] + Y[kE]);
+    double ddp = -G[k] * (2. * G[k] + G[kS] + G[kN]);
+    const double ap = aap * pxi + bbp * pet + ccp * pxi + ddp * pet;
+    const double vals[9] = {ap, ae, aw, an, as, ane, anw, ase, asw};
+    const LevelDev& L0 = c.lev[0];
+    const int ld0 = L0.ld;
+#pragma unroll
+    for (int m = 0; m < 9; m++) {
+        store_mirrored(plane(b, c, P_AP + m), ld, i, j, W, per, vals[m]);
+        store_mirrored(mplane(b, L0, M_AP + m), ld0, i, j, W, per, (float)vals[m]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// u/v/T operator coefficients, PSolver.cpp:765-849, computed in registers
+struct Coef25 {
+    double p, e, w, n, s, ne, nw, se, sw;
+    double ee, ww, nn, ss, nnee, nnww, ssee, ssww, nne, nnw, sse, ssw, nee, nww, see, sww;
+};
+
+__device__ __forceinline__ void build_coefs(const CaseDev& c, double al, double be, double ga,
+                                            bool nearw, int j, Coef25& A, Coef25& T) {
+    const double d0 = c.d0, d1 = c.d1, dt = c.dt, Re = c.Re, Pr = c.Pr;
+    if (nearw) {
+        A.e = A.w = -dt * (al / (d0 * d0)) / Re;
+        A.n = A.s = -dt * (ga / (d1 * d1)) / Re;
+        A.ne = A.sw = dt * be / (2.0 * d0 * d1 * Re);
+        A.nw = A.se = -dt * be / (2.0 * d0 * d1 * Re);
+        A.p = 1 + dt * 2.0 * (al / (d0 * d0) + ga / (d1 * d1)) / Re;
+        T.e = T.w = -dt * (al / (d0 * d0)) / (Re * Pr);
+        T.n = T.s = -dt * (ga / (d1 * d1)) / (Re * Pr);
+        T.ne = T.sw = dt * (be / (2.0 * d0 * d1)) / (Re * Pr);
+        T.nw = T.se = -dt * (be / (2.0 * d0 * d1)) / (Re * Pr);
+        T.p = 1 + dt * 2.0 * (al / (d0 * d0) + ga / (d1 * d1)) / (Re * Pr);
+        if (c.profile == OGRID) {
+            // wall-row couplings are folded into the right-hand side (PSolver.cpp:851-882)
+            if (j == 1) { A.s = A.se = A.sw = 0.0; T.s = T.se = T.sw = 0.0; }
+            if (j == c.n1 - 2) { A.n = A.ne = A.nw = 0.0; T.n = T.ne = T.nw = 0.0; }
+        }
+        A.ee = A.ww = A.nn = A.ss = A.nnee = A.nnww = A.ssee = A.ssww = 0.0;
+        A.nne = A.nnw = A.sse = A.ssw = A.nee = A.nww = A.see = A.sww = 0.0;
+        T.ee = T.ww = T.nn = T.ss = T.nnee = T.nnww = T.ssee = T.ssww = 0.0;
+        T.nne = T.nnw = T.sse = T.ssw = T.nee = T.nww = T.see = T.sww = 0.0;
+    } else {
+        A.e = A.w = (-dt) * ((4.0 * al) / (3.0 * d0 * d0)) / Re;
+        A.n = A.s = (-dt) * ((4.0 * ga) / (3.0 * d1 * d1)) / Re;
+        A.ne = A.sw = (-dt) * (-8.0 * be / (9.0 * d0 * d1)) / Re;
+        A.nw = A.se = (-dt) * (8.0 * be / (9.0 * d0 * d1)) / Re;
+        A.nn = A.ss = (-dt) * (-ga / (12.0 * d1 * d1)) / Re;
+        A.ee = A.ww = (-dt) * (-al / (12.0 * d0 * d0)) / Re;
+        A.nnee = A.ssww = (-dt) * (-be / (72.0 * d0 * d1)) / Re;
+        A.nnww = A.ssee = (-dt) * (be / (72.0 * d0 * d1)) / Re;
+        A.nne = A.ssw = A.nee = A.sww = (-dt) * (be / (9.0 * d0 * d1)) / Re;
+        A.nnw = A.sse = A.nww = A.see = (-dt) * (-be / (9.0 * d0 * d1)) / Re;
+        A.p = 1 + dt * (5.0 * al / (2.0 * d0 * d0) + 5.0 * ga / (2.0 * d1 * d1)) / Re;
+        T.e = A.e / Pr; T.w = A.w / Pr; T.n = A.n / Pr; T.s = A.s / Pr;
+        T.ne = A.ne / Pr; T.nw = A.nw / Pr; T.se = A.se / Pr; T.sw = A.sw / Pr;
+        T.nn = A.nn / Pr; T.ss = A.ss / Pr; T.ee = A.ee / Pr; T.ww = A.ww / Pr;
+        T.nnee = A.nnee / Pr; T.nnww = A.nnww / Pr; T.ssee = A.ssee / Pr; T.ssww = A.ssww / Pr;
+        T.nne = A.nne / Pr; T.nnw = A.nnw / Pr; T.sse = A.sse / Pr; T.ssw = A.ssw / Pr;
+        T.nee = A.nee / Pr; T.nww = A.nww / Pr; T.see = A.see / Pr; T.sww = A.sww / Pr;
+        T.p = 1 + dt * (5.0 * al / (2.0 * d0 * d0) + 5.0 * ga / (2.0 * d1 * d1)) / (Re * Pr);
+        // the reference's T solve passes atnw in the annw slot (PSolver.cpp:1290)
+        if (!c.fix_T_annw) T.nnw = T.nw;
+    }
+}
+
+// sum of the off-centre couplings, in the order of gauss() (PSolver.cpp:2408-2425)
+__device__ __forceinline__ double offsum(const double* F, long long k, int ld, const Coef25& a, bool nearw) {
+    double s = a.e * F[k + 1] + a.n * F[k + ld] + a.s * F[k - ld] + a.w * F[k - 1] +
+               a.nw * F[k + ld - 1] + a.ne * F[k + ld + 1] + a.sw * F[k - ld - 1] + a.se * F[k - ld + 1];
+    if (!nearw) {
+        const long long l2 = 2LL * ld;
+        s += a.ee * F[k + 2] + a.ww * F[k - 2] + a.nnee * F[k + l2 + 2] + a.nee * F[k + ld + 2] +
+             a.see * F[k - ld + 2] + a.ssee * F[k - l2 + 2] + a.nne * F[k + l2 + 1] +
+             a.sse * F[k - l2 + 1] + a.nnw * F[k + l2 - 1] + a.ssw * F[k - l2 - 1] +
+             a.nnww * F[k + l2 - 2] + a.nww * F[k + ld - 2] + a.sww * F[k - ld - 2] +
+             a.ssww * F[k - l2 - 2] + a.nn * F[k + l2] + a.ss * F[k - l2];
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// contravariant velocities + convection + the five right-hand sides
+// (PSolver.cpp:1063-1237); also seeds the five solves' iterates
+__global__ void __launch_bounds__(NT) k_rhs(BatchDev b) {
+    const Tile t = b.ftiles[blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    if (t.k == 0 && threadIdx.x == 0) {
+        int* is = b.iscal + (long long)t.c * NISCAL;
+        for (int f = 0; f < NFIELD; f++) { is[I_MDONE0 + f] = 0; is[I_MIT0 + f] = 0; }
+        atomicAdd(b.mactive, NFIELD);
+    }
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
+    const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
+    const int cur = b.cur, nxt = cur ^ 1;
+    const bool cav = c.profile == CAVITY;
+    const double d0 = c.d0, d1 = c.d1, dt = c.dt, Re = c.Re, Pr = c.Pr, Ri = c.Ri;
+    const double* U = plane(b, c, P_U);
+    const double* V = plane(b, c, P_V);
+    const double* T = plane(b, c, P_T0 + cur);
+    const double* UP = plane(b, c, P_UP0 + cur);
+    const double* VP = plane(b, c, P_VP0 + cur);
+    const double* P = plane(b, c, P_P);
+    const double* XIX = plane(b, c, P_XIX);
+    const double* XIY = plane(b, c, P_XIY);
+    const double* ETX = plane(b, c, P_ETX);
+    const double* ETY = plane(b, c, P_ETY);
+    const long long k = (long long)j * ld + i;
+    const double al = plane(b, c, P_ALPH)[k], ga = plane(b, c, P_GAM)[k];
+    const double ux = XIX[k] * U[k] + XIY[k] * V[k];
+    const double ue = ETX[k] * U[k] + ETY[k] * V[k];
+    const bool near_j = (j == 1 || j == n1 - 2);
+    const bool near_i = cav && (i == 1 || i == n0 - 2);
+    const double* Fs[3] = {U, V, T};
+    double conv[3];
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+        const double* F = Fs[m];
+        double pec1, pec2;
+        if (m <= 1) {
+            pec1 = ux * Re * d0 / al;
+            pec2 = ue * Re * d1 / ga;
+        } else {
+            pec1 = ux * Re * Pr * d0 / al;
+            pec2 = ue * Re * Pr * d1 / ga;
+        }
+        const double fc = F[k], fe = F[k + 1], fw = F[k - 1];
+        double du_xi, du_et;
+        if (near_i) {
+            du_xi = 0.5 * (fe - fw) / d0;
+        } else {
+            const double fee = F[k + 2], fww = F[k - 2];
+            if (near_j || (pec1 <= 2 && pec1 > -2)) {
+                double xpp = 8.0 * (fe - fw);
+                double xnn = fee - fww;
+                du_xi = (1.0 / 12.0) * (xpp - xnn) / d0;
+            } else {
+                double ak1 = ux * (-fee + 8 * fe - 8 * fw + fww) / (12.0 * d0);
+                double ak2 = fabs(ux) * (fee - 4 * fe + 6 * fc - 4 * fw + fww) / (4.0 * d0);
+                ak1 = ak1 + ak2;
+                du_xi = ak1 / ux;
+            }
+        }
+        const double fn = F[k + ld], fs = F[k - ld];
+        if (near_j) {
+            du_et = 0.5 * (fn - fs) / d1;
+        } else {
+            const double fnn = F[k + 2LL * ld], fss = F[k - 2LL * ld];
+            if (near_i || (pec2 <= 2 && pec2 > -2)) {
+                double ypp = 8.0 * (fn - fs);
+                double ynn = fnn - fss;
+                du_et = (1.0 / 12.0) * (ypp - ynn) / d1;
+            } else {
+                double ak3 = ue * (-fnn + 8 * fn - 8 * fs + fss) / (12.0 * d1);
+                double ak4 = fabs(ue) * (fnn - 4 * fn + 6 * fc - 4 * fs + fss) / (4.0 * d1);
+                ak3 = ak3 + ak4;
+                du_et = ak3 / ue;
+            }
+        }
+        conv[m] = ux * du_xi + ue * du_et;
+    }
+    const double dp_dxi = (P[k + 1] - P[k - 1]) / (2.0 * d0);
+    const double dp_de = (P[k + ld] - P[k - ld]) / (2.0 * d1);
+    const double dp_dx = XIX[k] * dp_dxi + ETX[k] * dp_de;
+    const double dp_dy = XIY[k] * dp_dxi + ETY[k] * dp_de;
+    double qu = dt * (-conv[0] - dp_dx) + U[k];
+    double qv = dt * (-conv[1] - dp_dy + Ri * T[k]) + V[k];
+    double qt = -dt * conv[2] + T[k];
+    double qup = qu + dt * dp_dx;
+    double qvp = qv + dt * dp_dy;
+    if (!cav && near_j) {
+        // folded wall-row couplings (PSolver.cpp:1195-1227)
+        const double be = plane(b, c, P_BETA)[k];
+        const double bs = -dt * (ga / (d1 * d1)) / Re;
+        const double bpos = dt * be / (2.0 * d0 * d1 * Re);
+        const double bneg = -dt * be / (2.0 * d0 * d1 * Re);
+        const double ts = -dt * (ga / (d1 * d1)) / (Re * Pr);
+        const double tpos = dt * (be / (2.0 * d0 * d1)) / (Re * Pr);
+        const double tneg = -dt * (be / (2.0 * d0 * d1)) / (Re * Pr);
+        long long s0, s1, s2;
+        double c1, c2, t1, t2;
+        if (j == 1) {  // bus, buse (= ause), busw (= ausw)
+            s0 = k - ld; s1 = k - ld + 1; s2 = k - ld - 1;
+            c1 = bneg; c2 = bpos; t1 = tneg; t2 = tpos;
+        } else {       // bun, bune (= aune), bunw (= aunw)
+            s0 = k + ld; s1 = k + ld + 1; s2 = k + ld - 1;
+            c1 = bpos; c2 = bneg; t1 = tpos; t2 = tneg;
+        }
+        double sumu = bs * U[s0] + c1 * U[s1] + c2 * U[s2];
+        qu = qu - sumu;
+        double sumv = bs * V[s0] + c1 * V[s1] + c2 * V[s2];
+        qv = qv - sumv;
+        double sumt = ts * T[s0] + t1 * T[s1] + t2 * T[s2];
+        qt = qt - sumt;
+        sumu = bs * UP[s0] + c1 * UP[s1] + c2 * UP[s2];
+        qup = qup - sumu;
+        sumv = bs * VP[s0] + c1 * VP[s1] + c2 * VP[s2];
+        qvp = qvp - sumv;
+    }
+    plane(b, c, P_RU)[k] = qu;
+    plane(b, c, P_RV)[k] = qv;
+    plane(b, c, P_RT)[k] = qt;
+    plane(b, c, P_RUP)[k] = qup;
+    plane(b, c, P_RVP)[k] = qvp;
+
+    // seed the iterates (PSolver.cpp:1241-1337): u*, v*, T from the current
+    // fields; up/vp from the previous solution (warm start) or zero
+    double* A[NFIELD] = {plane(b, c, P_US), plane(b, c, P_VS), plane(b, c, P_T0 + nxt),
+                         plane(b, c, P_UP0 + nxt), plane(b, c, P_VP0 + nxt)};
+    double* B[NFIELD] = {plane(b, c, P_BU), plane(b, c, P_BV), plane(b, c, P_BT),
+                         plane(b, c, P_BUP), plane(b, c, P_BVP)};
+    const bool warm = c.warm_up != 0;
+    store_mirrored(A[F_U], ld, i, j, W, per, U[k]);
+    store_mirrored(A[F_V], ld, i, j, W, per, V[k]);
+    store_mirrored(A[F_T], ld, i, j, W, per, T[k]);
+    store_mirrored(A[F_UP], ld, i, j, W, per, warm ? UP[k] : 0.0);
+    store_mirrored(A[F_VP], ld, i, j, W, per, warm ? VP[k] : 0.0);
+    // boundary values the stencils read (both iterate buffers)
+    auto put_bnd = [&](int bi, int bj) {
+        const long long kb = (long long)bj * ld + bi;
+        double vals[NFIELD] = {U[kb], V[kb], T[kb], UP[kb], VP[kb]};
+        if (!cav && bj == n1 - 1) {  // the up/vp solves see zero on the far-field row
+            vals[F_UP] = 0.0;
+            vals[F_VP] = 0.0;
+        }
+#pragma unroll
+        for (int f = 0; f < NFIELD; f++) {
+            store_mirrored(A[f], ld, bi, bj, W, per, vals[f]);
+            store_mirrored(B[f], ld, bi, bj, W, per, vals[f]);
+        }
+    };
+    if (j == 1) put_bnd(i, 0);
+    if (j == n1 - 2) put_bnd(i, n1 - 1);
+    if (cav) {
+        if (i == 1) {
+            put_bnd(0, j);
+            if (j == 1) put_bnd(0, 0);
+            if (j == n1 - 2) put_bnd(0, n1 - 1);
+        }
+        if (i == n0 - 2) {
+            put_bnd(n0 - 1, j);
+            if (j == 1) put_bnd(n0 - 1, 0);
+            if (j == n1 - 2) put_bnd(n0 - 1, n1 - 1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// one Jacobi sweep of the five momentum / energy systems (replaces gauss(),
+// PSolver.cpp:2280-2446). Iterates ping-pong between buffer A (the solution)
+// and the scratch B; sweeps come in pairs so the solution ends in A. The stop
+// rule is the reference's: relative L1 residual before a sweep below tol_mom
+// (or the absolute floor atol_mom) ends the solve after that sweep.
+__global__ void __launch_bounds__(NT) k_jac(BatchDev b, int to_scratch, int first, int decide) {
+    const Tile t = b.ftiles[blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    const int* isc = b.iscal + (long long)t.c * NISCAL;
+    int mask = 0;
+#pragma unroll
+    for (int f = 0; f < NFIELD; f++) mask |= (isc[I_MDONE0 + f] == 0) << f;
+    if (mask == 0) return;  // uniform over the case's CTAs
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    const int ld = c.ld;
+    double r[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
+        const long long k = (long long)j * ld + i;
+        const bool nearw = near_wall(c, i, j);
+        Coef25 A, TT;
+        build_coefs(c, plane(b, c, P_ALPH)[k], plane(b, c, P_BETA)[k], plane(b, c, P_GAM)[k],
+                    nearw, j, A, TT);
+        const int nxt = b.cur ^ 1;
+        const int pa[NFIELD] = {P_US, P_VS, P_T0 + nxt, P_UP0 + nxt, P_VP0 + nxt};
+        const int pb[NFIELD] = {P_BU, P_BV, P_BT, P_BUP, P_BVP};
+        const int pr[NFIELD] = {P_RU, P_RV, P_RT, P_RUP, P_RVP};
+#pragma unroll
+        for (int f = 0; f < NFIELD; f++) {
+            if (!(mask & (1 << f))) continue;
+            const double* src = plane(b, c, to_scratch ? pa[f] : pb[f]);
+            double* dst = plane(b, c, to_scratch ? pb[f] : pa[f]);
+            const Coef25& a = (f == F_T) ? TT : A;
+            const double s = offsum(src, k, ld, a, nearw);
+            const double rhs = plane(b, c, pr[f])[k];
+            const double res = rhs - a.p * src[k] - s;
+            store_mirrored(dst, ld, i, j, c.W, c.periodic, (rhs - s) / a.p);
+            r[f] = fabs(res);
+        }
+    }
+    if (case_reduce<NFIELD, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, r) &&
+        threadIdx.x == 0) {
+        double* sc = b.scal + (long long)t.c * NSCAL;
+        int* is = b.iscal + (long long)t.c * NISCAL;
+        for (int f = 0; f < NFIELD; f++) {
+            if (!(mask & (1 << f))) continue;
+            if (first) sc[S_MR0 + f] = (r[f] != 0.0) ? r[f] : 1.0;
+            sc[S_MR + f] = r[f];
+            is[I_MIT0 + f] += 1;
+            if (decide) {
+                bool done = (r[f] / sc[S_MR0 + f] < c.tol_mom) || (r[f] <= c.atol_mom);
+                if (!isfinite(r[f])) { is[I_STATUS] |= ST_NAN; done = true; }
+                if (done) { is[I_MDONE0 + f] = 1; atomicSub(b.mactive, 1); }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// up/vp far-field condition (PSolver.cpp:1356-1382), one CTA per O-grid case
+__global__ void __launch_bounds__(BC_THREADS) k_upbc(BatchDev b) {
+    const CaseDev& c = b.cases[blockIdx.x];
+    if (c.profile != OGRID) return;
+    const int ld = c.ld, j = c.n1 - 1, nxt = b.cur ^ 1;
+    double* UP = plane(b, c, P_UP0 + nxt);
+    double* VP = plane(b, c, P_VP0 + nxt);
+    const double* U = plane(b, c, P_U);
+    const double* V = plane(b, c, P_V);
+    const double* VEC = plane(b, c, P_VEC);
+    for (int i = threadIdx.x; i < c.W; i += blockDim.x) {
+        const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
+        const long long k = (long long)j * ld + i;
+        double a, bb;
+        if (vnn >= 0) {
+            a = U[k];
+            bb = V[k];
+        } else {
+            a = (5.0 * UP[k - ld] - 4.0 * UP[k - 2LL * ld] + UP[k - 3LL * ld]) / 2.0;
+            bb = (5.0 * VP[k - ld] - 4.0 * VP[k - 2LL * ld] + VP[k - 3LL * ld]) / 2.0;
+        }
+        store_mirrored(UP, ld, i, j, c.W, 1, a);
+        store_mirrored(VP, ld, i, j, c.W, 1, bb);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// face velocities -> continuity source q (PSolver.cpp:1390-1449) with the
+// mass-residual reductions; seeds the BiCGStab vectors (pcor starts at 0)
+__global__ void __launch_bounds__(NT) k_face_q(BatchDev b) {
+    const Tile t = b.ftiles[blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    const int ld = c.ld;
+    double red[3] = {0.0, 0.0, 0.0};
+    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
+        const int nxt = b.cur ^ 1;
+        const double d0 = c.d0, d1 = c.d1, dt = c.dt;
+        const double* P = plane(b, c, P_P);
+        const double* U = plane(b, c, P_UP0 + nxt);
+        const double* V = plane(b, c, P_VP0 + nxt);
+        const double* X = plane(b, c, P_XIX);
+        const double* Y = plane(b, c, P_XIY);
+        const double* E = plane(b, c, P_ETX);
+        const double* G = plane(b, c, P_ETY);
+        const long long k = (long long)j * ld + i, kE = k + 1, kW = k - 1, kN = k + ld, kS = k - ld;
+        double dpdxi_ip = (P[kE] - P[k]) / d0;
+        double dpde_ip = (P[kN + 1] + P[kN] - P[kS] - P[kS + 1]) / (4.0 * d1);
+        double dpdxi_in = (P[k] - P[kW]) / d0;
+        double dpde_in = (P[kN] + P[kN - 1] - P[kS] - P[kS - 1]) / (4.0 * d1);
+        double dpdxi_jp = (P[kN + 1] - P[kN - 1] + P[kE] - P[kW]) / (4.0 * d0);
+        double dpde_jp = (P[kN] - P[k]) / d1;
+        double dpdxi_jn = (P[kE] - P[kW] + P[kS + 1] - P[kS - 1]) / (4.0 * d0);
+        double dpde_jn = (P[k] - P[kS]) / d1;
+        double us_ip = 0.5 * (U[k] + U[kE]) - 0.5 * dt * ((X[k] + X[kE]) * dpdxi_ip + (E[k] + E[kE]) * dpde_ip);
+        double us_in = 0.5 * (U[k] + U[kW]) - 0.5 * dt * ((X[k] + X[kW]) * dpdxi_in + (E[k] + E[kW]) * dpde_in);
+        double us_jp = 0.5 * (U[k] + U[kN]) - 0.5 * dt * ((X[k] + X[kN]) * dpdxi_jp + (E[k] + E[kN]) * dpde_jp);
+        double us_jn = 0.5 * (U[k] + U[kS]) - 0.5 * dt * ((X[k] + X[kS]) * dpdxi_jn + (E[k] + E[kS]) * dpde_jn);
+        double vs_ip = 0.5 * (V[k] + V[kE]) - 0.5 * dt * ((Y[k] + Y[kE]) * dpdxi_ip + (G[k] + G[kE]) * dpde_ip);
+        double vs_in = 0.5 * (V[k] + V[kW]) - 0.5 * dt * ((Y[k] + Y[kW]) * dpdxi_in + (G[k] + G[kW]) * dpde_in);
+        double vs_jp = 0.5 * (V[k] + V[kN]) - 0.5 * dt * ((Y[k] + Y[kN]) * dpdxi_jp + (G[k] + G[kN]) * dpde_jp);
+        double vs_jn = 0.5 * (V[k] + V[kS]) - 0.5 * dt * ((Y[k] + Y[kS]) * dpdxi_jn + (G[k] + G[kS]) * dpde_jn);
+        double dusdxi = (us_ip - us_in) / d0;
+        double dusde = (us_jp - us_jn) / d1;
+        double dvsdxi = (vs_ip - vs_in) / d0;
+        double dvsde = (vs_jp - vs_jn) / d1;
+        double qq = (X[k] * dusdxi) + (E[k] * dusde) + (Y[k] * dvsdxi) + (G[k] * dvsde);
+        const double q = qq / dt;
+        plane(b, c, P_Q)[k] = q;
+        plane(b, c, P_KR)[k] = q;
+        plane(b, c, P_KRH)[k] = q;
+        plane(b, c, P_KP)[k] = 0.0;
+        plane(b, c, P_KV)[k] = 0.0;
+        store_mirrored(plane(b, c, P_PCOR), ld, i, j, c.W, c.periodic, 0.0);
+        red[0] = fabs(q);
+        red[1] = q * q;
+        red[2] = fabs(q);
+    }
+    if (case_reduce<3, 0x4u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) &&
+        threadIdx.x == 0) {
+        double* sc = b.scal + (long long)t.c * NSCAL;
+        int* is = b.iscal + (long long)t.c * NISCAL;
+        sc[S_QL1] = red[0];
+        sc[S_QL2] = sqrt(red[1]);
+        sc[S_QMAX] = red[2];
+        sc[S_RHO] = red[1];
+        sc[S_ALPHA] = 1.0;
+        sc[S_OMEGA] = 1.0;
+        sc[S_BETA] = 0.0;
+        sc[S_NB1] = red[0];
+        sc[S_RL1] = red[0];
+        is[I_PIT] = 0;
+        is[I_PSTATUS] = 0;
+        if (red[0] == 0.0 || !isfinite(red[0])) {
+            is[I_PDONE] = 1;
+            if (!isfinite(red[0])) is[I_STATUS] |= ST_NAN;
+        } else {
+            is[I_PDONE] = 0;
+            atomicAdd(b.active, 1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// BiCGStab, right-preconditioned, FP64 vectors; per-case scalars live on the device
+__global__ void __launch_bounds__(NT) k_bicg_p(BatchDev b) {
+    const Tile t = b.ftiles[blockIdx.x];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
+    const double* sc = b.scal + (long long)t.c * NSCAL;
+    const double beta = sc[S_BETA], omega = sc[S_OMEGA];
+    const long long k = (long long)j * c.ld + i;
+    double* Pv = plane(b, c, P_KP);
+    const double p = plane(b, c, P_KR)[k] + beta * (Pv[k] - omega * plane(b, c, P_KV)[k]);
+    Pv[k] = p;
+    const LevelDev& L = c.lev[0];
+    const long long k0 = (long long)j * L.ld + i;
+    mplane(b, L, M_B)[k0] = (float)p;
+    store_mirrored(mplane(b, L, M_X), L.ld, i, j, L.W, c.periodic, 0.0f);
+}
+
+// y = A * x with x = (double) MG level-0 iterate; mode 0: p_hat, v, (r_hat, v) -> alpha
+//                                                 mode 1: s_hat, t, (t, s), (t, t) -> omega
+__global__ void __launch_bounds__(NT) k_spmv(BatchDev b, int mode) {
+    const Tile t = b.ftiles[blockIdx.x];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    double red[2] = {0.0, 0.0};
+    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
+        const int ld = c.ld;
+        const LevelDev& L = c.lev[0];
+        const int l0 = L.ld;
+        const float* X = mplane(b, L, M_X);
+        const long long k = (long long)j * ld + i, q = (long long)j * l0 + i;
+        const double xc = (double)X[q];
+        const double y = plane(b, c, P_AP)[k] * xc + plane(b, c, P_AE)[k] * (double)X[q + 1] +
+                         plane(b, c, P_AW)[k] * (double)X[q - 1] + plane(b, c, P_AN)[k] * (double)X[q + l0] +
+                         plane(b, c, P_AS)[k] * (double)X[q - l0] + plane(b, c, P_ANE)[k] * (double)X[q + l0 + 1] +
+                         plane(b, c, P_ANW)[k] * (double)X[q + l0 - 1] + plane(b, c, P_ASE)[k] * (double)X[q - l0 + 1] +
+                         plane(b, c, P_ASW)[k] * (double)X[q - l0 - 1];
+        if (mode == 0) {
+            plane(b, c, P_KPH)[k] = xc;
+            plane(b, c, P_KV)[k] = y;
+            red[0] = plane(b, c, P_KRH)[k] * y;
+        } else {
+            plane(b, c, P_KSH)[k] = xc;
+            plane(b, c, P_KT)[k] = y;
+            red[0] = y * plane(b, c, P_KS)[k];
+            red[1] = y * y;
+        }
+    }
+    if (case_reduce<2, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0) {
+        double* sc = b.scal + (long long)t.c * NSCAL;
+        int* is = b.iscal + (long long)t.c * NISCAL;
+        if (mode == 0) {
+            if (red[0] == 0.0 || !isfinite(red[0])) {
+                is[I_PSTATUS] |= ST_BREAKDOWN;
+                is[I_PDONE] = 1;
+                atomicSub(b.active, 1);
+            } else {
+                sc[S_ALPHA] = sc[S_RHO] / red[0];
+            }
+        } else {
+            sc[S_OMEGA] = red[1] > 0.0 ? red[0] / red[1] : 0.0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(NT) k_bicg_s(BatchDev b) {
+    const Tile t = b.ftiles[blockIdx.x];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
+    const double alpha = b.scal[(long long)t.c * NSCAL + S_ALPHA];
+    const long long k = (long long)j * c.ld + i;
+    const double s = plane(b, c, P_KR)[k] - alpha * plane(b, c, P_KV)[k];
+    plane(b, c, P_KS)[k] = s;
+    const LevelDev& L = c.lev[0];
+    mplane(b, L, M_B)[(long long)j * L.ld + i] = (float)s;
+    store_mirrored(mplane(b, L, M_X), L.ld, i, j, L.W, c.periodic, 0.0f);
+}
+
+__global__ void __launch_bounds__(NT) k_bicg_x(BatchDev b, int maxit) {
+    const Tile t = b.ftiles[blockIdx.x];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    const double* sc0 = b.scal + (long long)t.c * NSCAL;
+    const double alpha = sc0[S_ALPHA], omega = sc0[S_OMEGA];
+    double red[2] = {0.0, 0.0};
+    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
+        const int ld = c.ld;
+        const long long k = (long long)j * ld + i;
+        double* X = plane(b, c, P_PCOR);
+        const double x = X[k] + alpha * plane(b, c, P_KPH)[k] + omega * plane(b, c, P_KSH)[k];
+        store_mirrored(X, ld, i, j, c.W, c.periodic, x);
+        const double r = plane(b, c, P_KS)[k] - omega * plane(b, c, P_KT)[k];
+        plane(b, c, P_KR)[k] = r;
+        red[0] = plane(b, c, P_KRH)[k] * r;
+        red[1] = fabs(r);
+    }
+    if (case_reduce<2, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0) {
+        double* sc = b.scal + (long long)t.c * NSCAL;
+        int* is = b.iscal + (long long)t.c * NISCAL;
+        const int it = ++is[I_PIT];
+        const double rho_new = red[0];
+        sc[S_RL1] = red[1];
+        const bool conv = red[1] <= c.tol_p * sc[S_NB1] || red[1] <= c.atol_p;
+        bool stop = conv;
+        if (!isfinite(red[1])) { is[I_STATUS] |= ST_NAN; stop = true; }
+        else if (!conv && (omega == 0.0 || rho_new == 0.0)) { is[I_PSTATUS] |= ST_BREAKDOWN; stop = true; }
+        else if (!conv && it >= maxit) { is[I_PSTATUS] |= ST_MAXITER; stop = true; }
+        if (!stop) {
+            sc[S_BETA] = (rho_new / sc[S_RHO]) * (alpha / omega);
+            sc[S_RHO] = rho_new;
+        } else {
+            is[I_PDONE] = 1;
+            atomicSub(b.active, 1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// multigrid preconditioner, FP32, level tiles
+__device__ __forceinline__ int mg_colour(int i, int j, int W, int periodic) {
+    // 4 colours by parity; an odd periodic width gets 2 extra colours for its last column
+    if (periodic && (W & 1) && i == W - 1) return 4 + (j & 1);
+    return (i & 1) | ((j & 1) << 1);
+}
+
+__global__ void __launch_bounds__(NT) k_mg_smooth(BatchDev b, int l, int colour) {
+    const Tile t = b.mtiles[l][blockIdx.x];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const LevelDev& L = c.lev[l];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    if (i < L.ilo || i > L.ihi || j > L.n1 - 2) return;
+    if (mg_colour(i, j, L.W, c.periodic) != colour) return;
+    const int ld = L.ld;
+    const long long k = (long long)j * ld + i;
+    float* X = mplane(b, L, M_X);
+    const float s = mplane(b, L, M_AE)[k] * X[k + 1] + mplane(b, L, M_AW)[k] * X[k - 1] +
+                    mplane(b, L, M_AN)[k] * X[k + ld] + mplane(b, L, M_AS)[k] * X[k - ld] +
+                    mplane(b, L, M_ANE)[k] * X[k + ld + 1] + mplane(b, L, M_ANW)[k] * X[k + ld - 1] +
+                    mplane(b, L, M_ASE)[k] * X[k - ld + 1] + mplane(b, L, M_ASW)[k] * X[k - ld - 1];
+    store_mirrored(X, ld, i, j, L.W, c.periodic, (mplane(b, L, M_B)[k] - s) / mplane(b, L, M_AP)[k]);
+}
+
+__global__ void __launch_bounds__(NT) k_mg_resid(BatchDev b, int l) {
+    const Tile t = b.mtiles[l][blockIdx.x];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const LevelDev& L = c.lev[l];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    if (i < L.ilo || i > L.ihi || j > L.n1 - 2) return;
+    const int ld = L.ld;
+    const long long k = (long long)j * ld + i;
+    const float* X = mplane(b, L, M_X);
+    const float ax = mplane(b, L, M_AP)[k] * X[k] + mplane(b, L, M_AE)[k] * X[k + 1] +
+                     mplane(b, L, M_AW)[k] * X[k - 1] + mplane(b, L, M_AN)[k] * X[k + ld] +
+                     mplane(b, L, M_AS)[k] * X[k - ld] + mplane(b, L, M_ANE)[k] * X[k + ld + 1] +
+                     mplane(b, L, M_ANW)[k] * X[k + ld - 1] + mplane(b, L, M_ASE)[k] * X[k - ld + 1] +
+                     mplane(b, L, M_ASW)[k] * X[k - ld - 1];
+    store_mirrored(mplane(b, L, M_R), ld, i, j, L.W, c.periodic, mplane(b, L, M_B)[k] - ax);
+}
+
+// full-weighting restriction of level l's residual into level l+1 (tiles of level l+1)
+__global__ void __launch_bounds__(NT) k_mg_restrict(BatchDev b, int l) {
+    const Tile t = b.atiles[l + 1][blockIdx.x];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const LevelDev& F = c.lev[l];
+    const LevelDev& C = c.lev[l + 1];
+    const int I = t.i0 + (int)(threadIdx.x % TX), J = t.j0 + (int)(threadIdx.x / TX);
+    if (I < C.ilo || I > C.ihi || J > C.n1 - 2) return;
+    const int fl = F.ld;
+    const float* R = mplane(b, F, M_R);
+    const long long f = (long long)(2 * J) * fl + 2 * I;
+    const float v = 0.0625f * (R[f - fl - 1] + R[f - fl + 1] + R[f + fl - 1] + R[f + fl + 1]) +
+                    0.125f * (R[f - fl] + R[f + fl] + R[f - 1] + R[f + 1]) + 0.25f * R[f];
+    const long long kc = (long long)J * C.ld + I;
+    mplane(b, C, M_B)[kc] = v;
+    store_mirrored(mplane(b, C, M_X), C.ld, I, J, C.W, c.periodic, 0.0f);
+}
+
+// bilinear prolongation + correction of level l from level l+1 (tiles of level l)
+__global__ void __launch_bounds__(NT) k_mg_prolong(BatchDev b, int l) {
+    const Tile t = b.mtiles[l][blockIdx.x];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const LevelDev& F = c.lev[l];
+    const LevelDev& C = c.lev[l + 1];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    if (i < F.ilo || i > F.ihi || j > F.n1 - 2) return;
+    const float* XC = mplane(b, C, M_X);
+    const int cl = C.ld;
+    const int I = i >> 1, J = j >> 1;
+    const long long q = (long long)J * cl + I;
+    float v;
+    if (!(i & 1) && !(j & 1)) v = XC[q];
+    else if (!(j & 1)) v = 0.5f * (XC[q] + XC[q + 1]);
+    else if (!(i & 1)) v = 0.5f * (XC[q] + XC[q + cl]);
+    else v = 0.25f * (XC[q] + XC[q + 1] + XC[q + cl] + XC[q + cl + 1]);
+    float* X = mplane(b, F, M_X);
+    const long long k = (long long)j * F.ld + i;
+    store_mirrored(X, F.ld, i, j, F.W, c.periodic, X[k] + v);
+}
+
+// coarsest level: `sweeps` multicolour GS sweeps by one CTA per case
+__global__ void __launch_bounds__(1024) k_mg_coarse(BatchDev b, int l, int sweeps) {
+    const int cid = b.ccases[l][blockIdx.x];
+    if (b.iscal[(long long)cid * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[cid];
+    const LevelDev& L = c.lev[l];
+    const int ld = L.ld;
+    const int nx = L.ihi - L.ilo + 1, ny = L.n1 - 2;
+    float* X = mplane(b, L, M_X);
+    const float* Bv = mplane(b, L, M_B);
+    const int ncol = (c.periodic && (L.W & 1)) ? 6 : 4;
+    for (int s = 0; s < sweeps; s++) {
+        for (int col = 0; col < ncol; col++) {
+            for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
+                const int i = L.ilo + e % nx, j = 1 + e / nx;
+                if (mg_colour(i, j, L.W, c.periodic) != col) continue;
+                const long long k = (long long)j * ld + i;
+                const float sm = mplane(b, L, M_AE)[k] * X[k + 1] + mplane(b, L, M_AW)[k] * X[k - 1] +
+                                 mplane(b, L, M_AN)[k] * X[k + ld] + mplane(b, L, M_AS)[k] * X[k - ld] +
+                                 mplane(b, L, M_ANE)[k] * X[k + ld + 1] + mplane(b, L, M_ANW)[k] * X[k + ld - 1] +
+                                 mplane(b, L, M_ASE)[k] * X[k - ld + 1] + mplane(b, L, M_ASW)[k] * X[k - ld - 1];
+                store_mirrored(X, ld, i, j, L.W, c.periodic, (Bv[k] - sm) / mplane(b, L, M_AP)[k]);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Galerkin coarse operator A_{l+1} = R A_l P (R full weighting, P bilinear, R = P^T / 4)
+__device__ __forceinline__ bool lev_unknown(const LevelDev& L, int periodic, int i, int j) {
+    if (j < 1 || j > L.n1 - 2) return false;
+    if (periodic) return true;
+    return i >= L.ilo && i <= L.ihi;
+}
+
+__global__ void __launch_bounds__(NT) k_mg_galerkin(BatchDev b, int l) {
+    const Tile t = b.atiles[l + 1][blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    const LevelDev& F = c.lev[l];
+    const LevelDev& C = c.lev[l + 1];
+    const int I = t.i0 + (int)(threadIdx.x % TX), J = t.j0 + (int)(threadIdx.x / TX);
+    if (I < C.ilo || I > C.ihi || J > C.n1 - 2) return;
+    const int per = c.periodic;
+    const int fl = F.ld;
+    const float* fa[9];
+#pragma unroll
+    for (int m = 0; m < 9; m++) fa[m] = mplane(b, F, M_AP + m);
+    // stencil offsets in M_AP.. order: p, e, w, n, s, ne, nw, se, sw
+    const int ox[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
+    const int oy[9] = {0, 0, 0, 1, -1, 1, 1, -1, -1};
+    double acc[9];  // indexed (dy + 1) * 3 + (dx + 1)
+#pragma unroll
+    for (int m = 0; m < 9; m++) acc[m] = 0.0;
+    for (int bj = -1; bj <= 1; bj++) {
+        for (int bi = -1; bi <= 1; bi++) {
+            const int fi = 2 * I + bi, fj = 2 * J + bj;
+            if (!lev_unknown(F, per, fi, fj)) continue;
+            const double wr = 0.25 * (bi == 0 ? 1.0 : 0.5) * (bj == 0 ? 1.0 : 0.5);
+            const long long kf = (long long)fj * fl + fi;
+            for (int m = 0; m < 9; m++) {
+                const int gi = fi + ox[m], gj = fj + oy[m];
+                if (!lev_unknown(F, per, gi, gj)) continue;
+                const double a = wr * (double)fa[m][kf];
+                // coarse parents of fine point (gi, gj)
+                int pi[2], pj[2];
+                double wi[2], wj[2];
+                int ni, nj;
+                if (!(gi & 1)) { pi[0] = gi >> 1; wi[0] = 1.0; ni = 1; }
+                else { pi[0] = (gi - 1) >> 1; pi[1] = (gi + 1) >> 1; wi[0] = wi[1] = 0.5; ni = 2; }
+                if (!(gj & 1)) { pj[0] = gj >> 1; wj[0] = 1.0; nj = 1; }
+                else { pj[0] = (gj - 1) >> 1; pj[1] = (gj + 1) >> 1; wj[0] = wj[1] = 0.5; nj = 2; }
+                for (int x = 0; x < ni; x++) {
+                    for (int y = 0; y < nj; y++) {
+                        if (!lev_unknown(C, per, pi[x], pj[y])) continue;
+                        const int dx = pi[x] - I, dy = pj[y] - J;
+                        acc[(dy + 1) * 3 + (dx + 1)] += a * wi[x] * wj[y];
+                    }
+                }
+            }
+        }
+    }
+    const long long kc = (long long)J * C.ld + I;
+    const int idx[9] = {4, 5, 3, 7, 1, 8, 6, 2, 0};  // p, e, w, n, s, ne, nw, se, sw
+#pragma unroll
+    for (int m = 0; m < 9; m++)
+        store_mirrored(mplane(b, C, M_AP + m), C.ld, I, J, C.W, per, (float)acc[idx[m]]);
+    (void)kc;
+}
+
+// ---------------------------------------------------------------------------
+// pcor boundary conditions + velocity / pressure correction (PSolver.cpp:1471-1542)
+__global__ void __launch_bounds__(NT) k_correct(BatchDev b) {
+    const Tile t = b.ftiles[blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
+    const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
+    const bool cav = c.profile == CAVITY;
+    double* PC = plane(b, c, P_PCOR);
+    const long long k = (long long)j * ld + i;
+    const double pc = PC[k];
+    // pcor on the boundary after its conditions: wall copy, far field 0 / copy at inflow
+    double far = 0.0;
+    if (!cav && j == n1 - 2) {
+        const double* VEC = plane(b, c, P_VEC);
+        const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
+        if (vnn >= 0) far = pc;
+    }
+    double pN = (j == n1 - 2) ? (cav ? pc : far) : PC[k + ld];
+    double pS = (j == 1) ? pc : PC[k - ld];
+    double pE = (cav && i == n0 - 2) ? pc : PC[k + 1];
+    double pW = (cav && i == 1) ? pc : PC[k - 1];
+    const double d0 = c.d0, d1 = c.d1, dt = c.dt;
+    const double dpcor_dxi = 0.5 * (pE - pW) / d0;
+    const double dpcor_de = 0.5 * (pN - pS) / d1;
+    double* U = plane(b, c, P_U);
+    double* V = plane(b, c, P_V);
+    double* P = plane(b, c, P_P);
+    const double un = plane(b, c, P_US)[k] - dt * (plane(b, c, P_XIX)[k] * dpcor_dxi + plane(b, c, P_ETX)[k] * dpcor_de);
+    const double vn = plane(b, c, P_VS)[k] - dt * (plane(b, c, P_XIY)[k] * dpcor_dxi + plane(b, c, P_ETY)[k] * dpcor_de);
+    store_mirrored(U, ld, i, j, W, per, un);
+    store_mirrored(V, ld, i, j, W, per, vn);
+    const double pn = (c.omega_p == 1.0) ? P[k] + pc : P[k] + c.omega_p * pc;
+    store_mirrored(P, ld, i, j, W, per, pn);
+    // record the boundary pcor (output only)
+    if (j == 1) store_mirrored(PC, ld, i, 0, W, per, pc);
+    if (j == n1 - 2) store_mirrored(PC, ld, i, n1 - 1, W, per, cav ? pc : far);
+    if (cav) {
+        if (i == 1) PC[k - 1] = pc;
+        if (i == n0 - 2) PC[k + 1] = pc;
+        if (i == 1 && j == 1) PC[0] = pc;
+        if (i == n0 - 2 && j == 1) PC[n0 - 1] = pc;
+        if (i == 1 && j == n1 - 2) PC[(long long)(n1 - 1) * ld] = pc;
+        if (i == n0 - 2 && j == n1 - 2) PC[(long long)(n1 - 1) * ld + n0 - 1] = pc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// boundary update, boundary pressure and wall integrals: one CTA per case
+// (O-grid: PSolver.cpp:1549-1783 and 1855-1983; cavity: this project's walls)
+__global__ void __launch_bounds__(BC_THREADS) k_bc(BatchDev b) {
+    const int cid = blockIdx.x;
+    const CaseDev& c = b.cases[cid];
+    const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
+    const int cur = b.cur, nxt = cur ^ 1;
+    const bool cav = c.profile == CAVITY;
+    const double d0 = c.d0, d1 = c.d1, dt = c.dt, Re = c.Re, Ri = c.Ri, Pi = c.Pi;
+    double* U = plane(b, c, P_U);
+    double* V = plane(b, c, P_V);
+    double* Tn = plane(b, c, P_T0 + nxt);
+    const double* To = plane(b, c, P_T0 + cur);
+    double* UPn = plane(b, c, P_UP0 + nxt);
+    double* VPn = plane(b, c, P_VP0 + nxt);
+    double* P = plane(b, c, P_P);
+    double* VORT = plane(b, c, P_VORT);
+    const double* X = plane(b, c, P_X);
+    const double* Yc = plane(b, c, P_Y);
+    const double* XIX = plane(b, c, P_XIX);
+    const double* XIY = plane(b, c, P_XIY);
+    const double* ETX = plane(b, c, P_ETX);
+    const double* ETY = plane(b, c, P_ETY);
+    const double* ALPH = plane(b, c, P_ALPH);
+    const double* BETA = plane(b, c, P_BETA);
+    const double* GAM = plane(b, c, P_GAM);
+    const double* JAC = plane(b, c, P_JAC);
+    const double* VEC = plane(b, c, P_VEC);
+    __shared__ double red[16 * 32];
+    __shared__ double s_circ;
+    int* is = b.iscal + (long long)cid * NISCAL;
+    double* sc = b.scal + (long long)cid * NSCAL;
+    const int time_new = (int)((double)is[I_TIME] + dt);
+    const int jf = n1 - 1;
+    // far-field u/v before this update (uold of PSolver.cpp:1456); W <= 4096
+    extern __shared__ double s_old[];  // 2 * (W + 1)
+
+    if (!cav) {
+        // circulation at j = n1-2 (PSolver.cpp:1568-1576)
+        {
+            const int j = n1 - 2;
+            const double de = c.fix_circ_de ? 1.0 / (n0 - 1) : 1.0 / (n0 - 2);
+            double acc[1] = {0.0};
+            for (int i = threadIdx.x; i < W; i += blockDim.x) {
+                const long long k = (long long)j * ld + i, kp = k + 1;
+                double f1 = (U[k] * ETY[k] - V[k] * ETX[k]) * fabs(JAC[k]);
+                double f2 = (U[kp] * ETY[kp] - V[kp] * ETX[kp]) * fabs(JAC[kp]);
+                acc[0] += de * 0.5 * (f1 + f2);
+                const long long kf = (long long)jf * ld + i;
+                s_old[i] = U[kf];
+                s_old[W + 1 + i] = V[kf];
+            }
+            block_sum<1>(acc, red);
+            if (threadIdx.x == 0) s_circ = acc[0];
+            __syncthreads();
+        }
+        const double circ = s_circ;
+        const double cwall = cos(2.0 * Pi * c.F * time_new);
+        for (int i = threadIdx.x; i < W; i += blockDim.x) {
+            // vr/vth just inside (PSolver.cpp:1549-1562) and their far-field prediction (:1582-1609)
+            const long long kb = (long long)(jf - 1) * ld + i, k = (long long)jf * ld + i;
+            const double costb = X[kb] / sqrt(X[kb] * X[kb] + Yc[kb] * Yc[kb]);
+            const double sintb = Yc[kb] / sqrt(X[kb] * X[kb] + Yc[kb] * Yc[kb]);
+            const double vr0 = U[kb] * costb + V[kb] * sintb;
+            const double vth0 = -U[kb] * sintb + V[kb] * costb;
+            const double cr = sqrt(X[kb] * X[kb] + Yc[kb] * Yc[kb]) / sqrt(X[k] * X[k] + Yc[k] * Yc[k]);
+            const double costh = X[k] / sqrt(X[k] * X[k] + Yc[k] * Yc[k]);
+            const double sinth = Yc[k] / sqrt(X[k] * X[k] + Yc[k] * Yc[k]);
+            const double vrinf = c.uinf * costh + c.vinf * sinth;
+            const double vtinf = -c.uinf * sinth + c.vinf * costh;
+            const double cr2 = cr * cr;
+            const double crk = fabs(circ) > 1e-2 ? cr : cr2;
+            const double vr1 = vr0 * cr2 + vrinf * (1 - cr2);
+            const double vth1 = vth0 * crk + vtinf * (1 - crk);
+            // far-field u/v/T (PSolver.cpp:1632-1656)
+            const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
+            double un, vn, tn;
+            if (vnn >= 0) {
+                un = c.uinf; vn = c.vinf; tn = 0.0;
+            } else {
+                un = costh * vr1 - sinth * vth1;
+                vn = sinth * vr1 + costh * vth1;
+                const double uet_old = ETX[k] * s_old[i] + ETY[k] * s_old[W + 1 + i];
+                tn = To[k] - (uet_old * dt / d1) * (To[k] - To[k - ld]);
+            }
+            store_mirrored(U, ld, i, jf, W, per, un);
+            store_mirrored(V, ld, i, jf, W, per, vn);
+            store_mirrored(Tn, ld, i, jf, W, per, tn);
+            // wall velocity (PSolver.cpp:1617-1630)
+            const double uw = -c.speed_amp * cwall * Yc[i];
+            const double vw = c.speed_amp * cwall * X[i];
+            store_mirrored(U, ld, i, 0, W, per, uw);
+            store_mirrored(V, ld, i, 0, W, per, vw);
+            store_mirrored(UPn, ld, i, 0, W, per, uw);
+            store_mirrored(VPn, ld, i, 0, W, per, vw);
+        }
+        __syncthreads();
+        // boundary pressure (PSolver.cpp:1668-1783)
+        const double swall = sin(2.0 * Pi * c.F * time_new);
+        const double* Fl[2] = {U, V};
+        for (int i = threadIdx.x; i < W; i += blockDim.x) {
+            {   // wall, j = 0
+                const long long k = i;
+                double dpd[2];
+                const double uxi = XIX[k] * U[k] + XIY[k] * V[k];
+                const double uet = ETX[k] * U[k] + ETY[k] * V[k];
+                for (int m = 0; m < 2; m++) {
+                    const double* f = Fl[m];
+                    const double aa = ALPH[k] * (f[k + 1] + f[k - 1] - 2 * f[k]) / (d0 * d0);
+                    const double gg = GAM[k] * (f[k + 2LL * ld] + f[k] - 2 * f[k + ld]) / (d1 * d1);
+                    const double bb = BETA[k] * (f[k + ld + 1] + f[k - 1] - f[k + ld - 1] - f[k + 1]) / (2 * d0 * d1);
+                    const double d2u = aa + gg - 2 * bb;
+                    double cv = uxi * 0.5 * (f[k + 1] - f[k - 1]) / d0;
+                    cv = cv + uet * (f[k + ld] - f[k]) / d1;
+                    const double alc = (m == 0) ? c.accn_amp * swall * Yc[k] : -c.accn_amp * swall * X[k];
+                    dpd[m] = 1.0 * d2u / Re - cv - alc + (m == 1 ? Ri * Tn[k] : 0.0);
+                }
+                const double pw = P[k + ld] - (dpd[0] * (-XIY[k] * JAC[k]) + dpd[1] * (XIX[k] * JAC[k])) * d1;
+                store_mirrored(P, ld, i, 0, W, per, pw);
+            }
+            {   // far field, j = n1-1
+                const long long k = (long long)jf * ld + i;
+                const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
+                double pf;
+                if (vnn >= 0) {
+                    const double uxi = XIX[k] * U[k] + XIY[k] * V[k];
+                    const double uet = ETX[k] * U[k] + ETY[k] * V[k];
+                    double dpd[2];
+                    for (int m = 0; m < 2; m++) {
+                        const double* f = Fl[m];
+                        const double fo = s_old[m * (W + 1) + i];
+                        const double aa = ALPH[k] * (f[k + 1] + f[k - 1] - 2 * f[k]) / (d0 * d0);
+                        const double gg = GAM[k] * (f[k] + f[k - 2LL * ld] - 2 * f[k - ld]) / (d1 * d1);
+                        const double bb = BETA[k] * (f[k + 1] + f[k - ld - 1] - f[k - ld + 1] - f[k - 1]) / (2 * d0 * d1);
+                        const double d2u = aa + gg - 2 * bb;
+                        double cv = uxi * 0.5 * (f[k + 1] - f[k - 1]) / d0;
+                        cv = cv + uet * (3.0 * f[k] - 4 * f[k - ld] + f[k - 2LL * ld]) / (2 * d1);
+                        const double alc = (f[k] - fo) / dt;
+                        dpd[m] = 1.0 * d2u / Re - cv - alc + (m == 1 ? Ri * Tn[k] : 0.0);
+                    }
+                    pf = P[k - ld] + (dpd[0] * (-XIY[k] * JAC[k]) + dpd[1] * (XIX[k] * JAC[k])) * d1;
+                } else {
+                    const double e0 = ETX[k] * U[k] + ETY[k] * V[k];
+                    const long long k1 = k - ld, k2 = k - 2LL * ld;
+                    const double e1 = ETX[k1] * U[k1] + ETY[k1] * V[k1];
+                    const double e2 = ETX[k2] * U[k2] + ETY[k2] * V[k2];
+                    pf = 0.5 * (1.0 / Re) * ((3 * e0 - 4 * e1 + e2) / d1);
+                }
+                store_mirrored(P, ld, i, jf, W, per, pf);
+            }
+        }
+    } else {
+        // cavity: adiabatic side walls, zero normal pressure gradient, static walls
+        for (int j = 1 + threadIdx.x; j <= n1 - 2; j += blockDim.x) {
+            const long long r = (long long)j * ld;
+            Tn[r] = (4.0 * Tn[r + 1] - Tn[r + 2]) / 3.0;
+            Tn[r + n0 - 1] = (4.0 * Tn[r + n0 - 2] - Tn[r + n0 - 3]) / 3.0;
+            P[r] = P[r + 1];
+            P[r + n0 - 1] = P[r + n0 - 2];
+        }
+        for (int i = 1 + threadIdx.x; i <= n0 - 2; i += blockDim.x) {
+            P[i] = P[i + ld];
+            P[(long long)jf * ld + i] = P[(long long)(jf - 1) * ld + i];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            P[0] = 0.5 * (P[1] + P[ld]);
+            P[n0 - 1] = 0.5 * (P[n0 - 2] + P[ld + n0 - 1]);
+            const long long r = (long long)jf * ld;
+            P[r] = 0.5 * (P[r + 1] + P[r - ld]);
+            P[r + n0 - 1] = 0.5 * (P[r + n0 - 2] + P[r - ld + n0 - 1]);
+        }
+    }
+    __syncthreads();
+    // vorticity on the j-boundaries (PSolver.cpp:1855-1888)
+    for (int e = threadIdx.x; e < 2 * (c.ihi - c.ilo + 1); e += blockDim.x) {
+        const int nb = c.ihi - c.ilo + 1;
+        const int i = c.ilo + e % nb;
+        const int j = (e < nb) ? 0 : jf;
+        const long long k = (long long)j * ld + i;
+        const double dv_dxi = 0.5 / d0 * (V[k + 1] - V[k - 1]);
+        const double dv_det = (j == 0) ? 1.0 / d1 * (V[k + ld] - V[k]) : 1.0 / d1 * (V[k] - V[k - ld]);
+        const double dv_dx = XIX[k] * dv_dxi + ETX[k] * dv_det;
+        const double du_dxi = 0.5 / d0 * (U[k + 1] - U[k - 1]);
+        const double du_det = (j == 0) ? 1.0 / d1 * (U[k + ld] - U[k]) : 1.0 / d1 * (U[k] - U[k - ld]);
+        const double du_dy = XIY[k] * du_dxi + ETY[k] * du_det;
+        store_mirrored(VORT, ld, i, j, W, per, dv_dx - du_dy);
+    }
+    __syncthreads();
+    // forces, moment, Nusselt number on j = 0 (PSolver.cpp:1901-1983)
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i <= n0 - 2; i += blockDim.x) {
+        const long long k = i, kp = i + 1;
+        const double PJ1 = P[k] * JAC[k], pj2 = P[kp] * JAC[kp];
+        const double VJ1 = VORT[k] * JAC[k], VJ2 = VORT[kp] * JAC[kp];
+        acc[0] += 0.5 * d0 * (PJ1 * ETX[k] + pj2 * ETX[kp]);
+        acc[1] += 0.5 * d0 * (PJ1 * ETY[k] + pj2 * ETY[kp]);
+        acc[2] += 0.5 * d0 * (VJ1 * ETY[k] + VJ2 * ETY[kp]);
+        acc[3] += 0.5 * d0 * (VJ1 * ETX[k] + VJ2 * ETX[kp]);
+        const double TJ1 = JAC[k] * (ETX[k] * ETX[k] + ETY[k] * ETY[k]);
+        const double TJ2 = JAC[kp] * (ETX[kp] * ETX[kp] + ETY[kp] * ETY[kp]);
+        const double fp1 = PJ1 * (X[k] * ETY[k] - Yc[k] * ETX[k]);
+        const double fp2 = pj2 * (X[kp] * ETY[kp] - Yc[kp] * ETX[kp]);
+        const double fv1 = VJ1 * (X[k] * ETX[k] + Yc[k] * ETY[k]);
+        const double fv2 = VJ2 * (X[kp] * ETX[kp] + Yc[kp] * ETY[kp]);
+        const double fh1 = TJ1 * (4 * Tn[k + ld] - 3 * Tn[k] - Tn[k + 2LL * ld]) / (2 * d1);
+        const double fh2 = TJ2 * (4 * Tn[kp + ld] - 3 * Tn[kp] - Tn[kp + 2LL * ld]) / (2 * d1);
+        acc[4] += 0.5 * d0 * (fp1 + fp2);
+        acc[5] += 0.5 * d0 * (fv1 + fv2);
+        acc[6] += 0.5 * (fh1 + fh2) * d0;
+    }
+    block_sum<7>(acc, red);
+    if (threadIdx.x == 0) {
+        const double pr_x = acc[0], pr_y = acc[1], vor_x = acc[2], vor_y = acc[3];
+        const double cx = 2 * pr_x + (2.0 / Re) * vor_x;
+        const double cy = 2 * pr_y - (2.0 / Re) * vor_y;
+        const double sa = c.sa, ca = c.ca;
+        sc[S_CLP] = 2 * pr_y * sa - 2 * pr_x * ca;
+        sc[S_CDP] = 2 * pr_y * ca + 2 * pr_x * sa;
+        sc[S_CLV] = -(2.0 / Re) * vor_y * sa - (2.0 / Re) * vor_x * ca;
+        sc[S_CDV] = -(2.0 / Re) * vor_y * ca + (2.0 / Re) * vor_x * sa;
+        sc[S_CL] = cy * sa - cx * ca;
+        sc[S_CD] = cy * ca + cx * sa;
+        sc[S_CM] = 2 * acc[4] - (2.0 / Re) * acc[5];
+        const double ar = c.ar;
+        if (!cav)
+            sc[S_NU] = (2 * acc[6]) / (Pi * (3 * (1 + (1.0 / ar)) - sqrt((3 + (1.0 / ar)) * ((3.0 / ar) + 1))));
+        else
+            sc[S_NU] = -acc[6];
+        sc[S_CIRC] = cav ? 0.0 : s_circ;
+        is[I_TIME] = time_new;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// dilatation, interior vorticity, dmax and the energy residual (PSolver.cpp:1807-1853)
+__global__ void __launch_bounds__(NT) k_diag(BatchDev b) {
+    const Tile t = b.ftiles[blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    double red[3] = {0.0, 0.0, 0.0};
+    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
+        const int ld = c.ld;
+        const long long k = (long long)j * ld + i;
+        const double* U = plane(b, c, P_U);
+        const double* V = plane(b, c, P_V);
+        const double d0 = c.d0, d1 = c.d1;
+        const double xix = plane(b, c, P_XIX)[k], xiy = plane(b, c, P_XIY)[k];
+        const double etx = plane(b, c, P_ETX)[k], ety = plane(b, c, P_ETY)[k];
+        const double dil = xix * (U[k + 1] - U[k - 1]) / (2 * d0) + etx * (U[k + ld] - U[k - ld]) / (2 * d1) +
+                           ety * (V[k + ld] - V[k - ld]) / (2 * d1) + xiy * (V[k + 1] - V[k - 1]) / (2 * d0);
+        const double dv_dxi = 0.5 / d0 * (V[k + 1] - V[k - 1]);
+        const double dv_det = 0.5 / d1 * (V[k + ld] - V[k - ld]);
+        const double du_dxi = 0.5 / d0 * (U[k + 1] - U[k - 1]);
+        const double du_det = 0.5 / d1 * (U[k + ld] - U[k - ld]);
+        const double vort = (xix * dv_dxi + etx * dv_det) - (xiy * du_dxi + ety * du_det);
+        store_mirrored(plane(b, c, P_VORT), ld, i, j, c.W, c.periodic, vort);
+        store_mirrored(plane(b, c, P_DIL), ld, i, j, c.W, c.periodic, dil);
+        const double dT = fabs(plane(b, c, P_T0 + (b.cur ^ 1))[k] - plane(b, c, P_T0 + b.cur)[k]);
+        red[0] = dil;
+        red[1] = dT;
+        red[2] = dT;
+    }
+    if (case_reduce<3, 0x5u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0) {
+        double* sc = b.scal + (long long)t.c * NSCAL;
+        sc[S_DMAX] = fmax(red[0], 0.0);
+        sc[S_DTL1] = red[1];
+        sc[S_DTMAX] = red[2];
+    }
+}
+
+// stream function, a scan along j per column (PSolver.cpp:1789-1801)
+__global__ void __launch_bounds__(BC_THREADS) k_si(BatchDev b) {
+    const CaseDev& c = b.cases[blockIdx.x];
+    const int ld = c.ld;
+    double* SI = plane(b, c, P_SI);
+    const double* U = plane(b, c, P_U);
+    const double* V = plane(b, c, P_V);
+    const double* XIX = plane(b, c, P_XIX);
+    const double* XIY = plane(b, c, P_XIY);
+    const double* JAC = plane(b, c, P_JAC);
+    const int ncol = c.periodic ? c.W : c.n0;
+    for (int i = threadIdx.x; i < ncol; i += blockDim.x) {
+        double s = 0.0;
+        store_mirrored(SI, ld, i, 0, c.W, c.periodic, 0.0);
+        for (int j = 1; j < c.n1; j++) {
+            const long long k = (long long)j * ld + i, kb = k - ld;
+            const double ca = (XIX[k] * U[k] * fabs(JAC[k]) + XIX[kb] * U[kb] * fabs(JAC[kb]));
+            const double cb = (XIY[k] * V[k] * fabs(JAC[k]) + XIY[kb] * V[kb] * fabs(JAC[kb]));
+            s = s + (ca + cb) * 0.5 * c.d1;
+            store_mirrored(SI, ld, i, j, c.W, c.periodic, s);
+        }
+    }
+}
+
+#undef AT
+}  // namespace cfd

@@ -1,0 +1,148 @@
+"""Host side of the drop-in: batches of cases on the GPU and an INP.DAT-driven
+`Solver` that mirrors the reference's `class Solver` (PSolver.cpp:11-2453).
+
+The reference's constructor reads INP.DAT, applies the initial and boundary
+conditions, assembles the coefficient matrices and runs the whole time loop;
+`timeLoop()` is the per-step body. `Solver` here keeps that shape: the
+constructor loads the grid and sets up the device case, `timeLoop(nsteps)`
+advances it and writes the reference's output files every 100 steps
+(PSolver.cpp:1989-2040).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+from .grid import Grid, read_inp
+from .outputs import write_coeff_his, write_spt, write_surf_dist
+
+
+class Batch:
+    """Many cases advanced together by one set of launches (cfd_batch_* of the C ABI)."""
+
+    def __init__(self, grids, params):
+        L = _lib.lib()
+        if len(grids) != len(params) or not grids:
+            raise ValueError("grids and params must be non-empty and of equal length")
+        self.grids = list(grids)
+        structs, self._keep = [], []
+        for g in self.grids:
+            s, keep = _lib.make_grid(g)
+            structs.append(s)
+            self._keep.extend(keep)
+        self._garr = (_lib.CfdGrid * len(structs))(*structs)
+        self._parr = (_lib.CfdParams * len(params))(*params)
+        self.h = ctypes.c_void_p()
+        _lib.check(L.cfd_batch_create(len(structs), self._garr, self._parr, ctypes.byref(self.h)),
+                   "cfd_batch_create")
+        self.steps = 0
+
+    def step(self, n: int = 1):
+        _lib.check(_lib.lib().cfd_batch_step(self.h, int(n)), "cfd_batch_step")
+        self.steps += n
+
+    def stats(self, i: int = 0) -> dict:
+        s = _lib.CfdStepStats()
+        _lib.check(_lib.lib().cfd_batch_stats(self.h, i, ctypes.byref(s)), "cfd_batch_stats")
+        return s.as_dict()
+
+    def plane(self, i: int, name: str) -> np.ndarray:
+        g = self.grids[i]
+        out = np.empty((g.n1, g.n0), dtype=np.float64)
+        _lib.check(_lib.lib().cfd_batch_get_plane(self.h, i, name.encode(),
+                                                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+                   f"cfd_batch_get_plane({name})")
+        return out
+
+    def profile(self, enable: bool = True):
+        _lib.check(_lib.lib().cfd_batch_profile(self.h, int(enable)), "cfd_batch_profile")
+
+    def kernel_times(self) -> dict:
+        cap = 64
+        names = (ctypes.c_char_p * cap)()
+        ms = (ctypes.c_double * cap)()
+        cnt = (ctypes.c_longlong * cap)()
+        n = _lib.lib().cfd_batch_kernel_times(self.h, names, ms, cnt, cap)
+        if n < 0:
+            _lib.check(n, "cfd_batch_kernel_times")
+        return {names[k].decode(): (ms[k], cnt[k]) for k in range(min(n, cap))}
+
+    def sync(self):
+        _lib.check(_lib.lib().cfd_batch_sync(self.h), "cfd_batch_sync")
+
+    def close(self):
+        if self.h:
+            _lib.lib().cfd_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def case_params(grid: Grid | None = None, **kw) -> _lib.CfdParams:
+    """cfd_params with the reference's defaults, the profile taken from the grid."""
+    if grid is not None and "profile" not in kw:
+        kw["profile"] = _lib.PROFILE_CAVITY if grid.kind == "cavity" else _lib.PROFILE_OGRID
+    return _lib.default_params(**kw)
+
+
+class Solver:
+    """INP.DAT-driven solver with the reference's outputs (PSolver.cpp:502-1043, 1051-2065)."""
+
+    def __init__(self, inp: str | Path = "INP.DAT", workdir: str | Path | None = None,
+                 grid: Grid | None = None, profile: str = "ogrid", **params):
+        self.workdir = Path(workdir) if workdir is not None else Path(inp).resolve().parent
+        self.grid = grid if grid is not None else read_inp(inp, kind=profile)
+        self.params = case_params(self.grid, **params)
+        self.batch = Batch([self.grid], [self.params])
+        self.loop = 0
+        self.time = 0  # the reference keeps time as an int (PSolver.cpp:186)
+        self.history = []
+
+    def fields(self) -> dict:
+        return {k: self.batch.plane(0, k) for k in ("u", "v", "T", "p", "si", "vort")}
+
+    def timeLoop(self, nsteps: int, output_every: int = 100, write: bool = True):
+        """Advance nsteps; write spt100.dat / COEFF_HIS*.dat / SURF_DIST.dat when loop % 100 == 0."""
+        for _ in range(nsteps):
+            self.batch.step(1)
+            self.time = int(self.time + self.params.dt)
+            st = self.batch.stats(0)
+            self.history.append(st)
+            if write and output_every and self.loop % output_every == 0:
+                self.write_outputs(st)
+            self.loop += 1
+        return self.history[-1] if self.history else None
+
+    def run_steps(self, nsteps: int):
+        """Advance nsteps without per-step host work (throughput path)."""
+        self.batch.step(nsteps)
+        self.loop += nsteps
+        for _ in range(nsteps):
+            self.time = int(self.time + self.params.dt)
+        return self.batch.stats(0)
+
+    def write_outputs(self, st: dict):
+        f = self.fields()
+        g = self.grid
+        write_spt(self.workdir / "spt100.dat", g, f)
+        write_coeff_his(self.workdir / "COEFF_HIS.dat", self.time, st["cl"], st["cd"], st["cm"], st["nu"])
+        write_coeff_his(self.workdir / "COEFF_HIS_pr_vor.dat", self.time, st["cl_pr"], st["cd_pr"],
+                        st["cl_vor"], st["cd_vor"])
+        write_surf_dist(self.workdir / "SURF_DIST.dat", g, f)
+
+    def close(self):
+        self.batch.close()

@@ -1,0 +1,128 @@
+/*
+ * cfd_b200.h -- C ABI of the B200 (sm_100a) projection-step solver.
+ *
+ * Drop-in boundary for the hot path of mhsuhail00/CFD_Solver. The reference is
+ * one C++ class (`class Solver`, PSolver.cpp:11-2447) with no plugin or FFI
+ * interface; its per-step body `Solver::timeLoop()` (PSolver.cpp:1051-2065)
+ * and the two solver members it calls,
+ *     void gauss(double** ap, ..., double** phi, double** q)   PSolver.cpp:2280-2286
+ *     void sip9p(double** ap, ..., double** phi, double** q)   PSolver.cpp:2067-2069
+ * are what this library replaces. The grid comes from the reference's INP.DAT
+ * (PSolver.cpp:517-547); the physics constants that the reference hard-codes
+ * as members (PSolver.cpp:160-183) and the solver tolerances it keeps as
+ * locals (PSolver.cpp:2086-2088, 2290-2291) are per-case parameters here.
+ *
+ * Conventions
+ *  - Every call returns CFD_OK (0) or a negative CFD_E_* code; cfd_last_error()
+ *    gives the message of the last failure on the calling thread.
+ *  - Host arrays are float64, n1*n0 in [j][i] order (i fastest) -- the order of
+ *    INP.DAT -- with the O-grid's seam column i = n0-1 included.
+ *  - The library owns all device memory; the caller owns every host buffer.
+ *  - A handle is driven by one host thread at a time; each batch has its own
+ *    CUDA stream. There is no CPU fallback: without a usable CUDA device every
+ *    entry point that needs one fails with CFD_E_CUDA.
+ */
+#ifndef CFD_B200_H
+#define CFD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFD_OK 0
+#define CFD_E_ARG (-1)      /* bad argument / grid */
+#define CFD_E_CUDA (-2)     /* CUDA error or no device */
+#define CFD_E_OOM (-3)      /* device memory exhausted / over budget */
+#define CFD_E_DIVERGED (-4) /* NaN in a case */
+#define CFD_E_MAXITER (-5)  /* an inner solve hit its iteration cap */
+#define CFD_E_BREAKDOWN (-6)/* Krylov breakdown */
+#define CFD_E_NOTCONV (-7)  /* solve_to: max_steps reached */
+
+#define CFD_PROFILE_OGRID 0  /* the reference's O-grid (periodic xi, body + far field) */
+#define CFD_PROFILE_CAVITY 1 /* lid-driven unit square on a curvilinear grid */
+
+/* One INP.DAT grid (PSolver.cpp:517-547); planes are n1*n0 host float64, [j][i]. */
+typedef struct cfd_grid {
+    int n0, n1;
+    double dxi0, dxi1;
+    double p_grid, a_grid, ar;
+    const double *x, *y;
+    const double *xix, *xiy, *etx, *ety; /* xi_x, xi_y, eta_x, eta_y */
+    const double *alph, *beta, *gam;     /* alpha, beta, gamma */
+    const double *jac;                   /* J = x_xi y_eta - x_eta y_xi */
+    const double *xnix, *xniy, *xnox, *xnoy; /* n0 each */
+} cfd_grid;
+
+/* Per-case parameters. cfd_params_default() gives the reference's values. */
+typedef struct cfd_params {
+    double Re, Ri, Pr, F, alpha_deg, dt;  /* PSolver.cpp:160-174 */
+    double tol_mom, atol_mom;  /* u/v/T solves: relative / absolute L1 residual (ref 0.75e-2, 0) */
+    double tol_p, atol_p;      /* pressure correction: relative / absolute L1 residual */
+    int maxit_mom, maxit_p;    /* iteration caps per solve */
+    int profile;               /* CFD_PROFILE_* */
+    int fix_T_annw;            /* 1: T solve uses atnnw (Fortran intent); 0: reference C++ */
+    int fix_circ_de;           /* 1: circulation spacing 1/(n0-1) (Fortran); 0: 1/(n0-2) */
+    int warm_start;            /* 1: up/vp solves start from the previous step; 0: from zero */
+    double omega_p;            /* p += omega_p * pcor (reference: 1) */
+    double lid_u;              /* cavity lid velocity */
+} cfd_params;
+
+/* Statistics of the last completed step of a case. */
+typedef struct cfd_step_stats {
+    int steps;        /* steps taken by the call */
+    int status;       /* bit set of the CFD solver status flags (0 = clean) */
+    int it_mom[5];    /* sweeps of the u*, v*, T, up, vp solves */
+    int it_p;         /* pressure-correction iterations */
+    double dmax;      /* max dilatation, the reference's per-step print (PSolver.cpp:1890) */
+    double cl, cd, cm, nu, circ;
+    double cl_pr, cd_pr, cl_vor, cd_vor;
+    double q_l1, q_l2, q_max; /* continuity source q (mass residual) norms */
+    double dT_l1, dT_max;     /* energy residual: |T^{n+1} - T^n| */
+    double p_res_rel;         /* final relative L1 residual of the pressure solve */
+    double mass_res_rel;      /* q_l2 / q_l2 of the case's first step */
+} cfd_step_stats;
+
+typedef struct cfd_batch cfd_batch;
+typedef cfd_batch cfd_case; /* a single case is a batch of one */
+
+void cfd_params_default(cfd_params* p);
+const char* cfd_last_error(void);
+int cfd_device_count(int* count);
+
+/* ---- single case (replaces Solver::Solver() + Solver::timeLoop()) ---- */
+int cfd_case_create(const cfd_grid* g, const cfd_params* prm, cfd_case** out);
+/* advance nsteps time steps (the body of timeLoop, PSolver.cpp:1058-1983) */
+int cfd_case_step(cfd_case* c, int nsteps, cfd_step_stats* last);
+/* step until mass_res_rel <= mass_tol (or max_steps) */
+int cfd_case_solve_to(cfd_case* c, double mass_tol, int max_steps, cfd_step_stats* last);
+/* host copies of the fields, n1*n0 each, [j][i]; any pointer may be NULL */
+int cfd_case_get_fields(cfd_case* c, double* u, double* v, double* T, double* p, double* si,
+                        double* vort);
+int cfd_case_destroy(cfd_case* c);
+
+/* ---- batch: many cases of uneven size and parameters in one set of launches ---- */
+int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params,
+                     cfd_batch** out);
+int cfd_batch_step(cfd_batch* b, int nsteps);
+int cfd_batch_stats(cfd_batch* b, int case_index, cfd_step_stats* out);
+/* named plane of one case ("u", "v", "T", "p", "up", "vp", "us", "vs", "pcor", "q",
+ * "qu", "qv", "qt", "qup", "qvp", "si", "vort", "dil", "ap", "ae", ...) as n1*n0 [j][i] */
+int cfd_batch_get_plane(cfd_batch* b, int case_index, const char* name, double* out);
+int cfd_batch_destroy(cfd_batch* b);
+/* device bytes a case of this size needs (admission by HBM budget) */
+size_t cfd_case_bytes(int n0, int n1, int profile);
+
+/* ---- timing: per-kernel CUDA-event durations accumulated on the batch's stream ---- */
+int cfd_batch_profile(cfd_batch* b, int enable);
+/* fills up to cap entries; returns the number of kernel names known */
+int cfd_batch_kernel_times(cfd_batch* b, const char** names, double* total_ms, long long* launches,
+                           int cap);
+int cfd_batch_sync(cfd_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
