@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Throughput of the batched projection time step on B200.
+
+Workload (default): the 256-case batched sweep -- seeded draws N in {65,129,193,257},
+skew U[0,0.2], Re logU[50,1000], Ri logU[0.1,10], Pr in {0.71,7} -- in its O-grid twin
+form (the reference's own geometry, boundary conditions, flow angle and dt = 1e-4), the
+form the compiled reference can run; `--form cavity` runs the lid-driven cavity form.
+One bench step = one outer time step of every case of the sweep (PSolver.cpp:1058-1983:
+RHS, five u/v/T/up/vp solves, continuity source, pressure correction, correction, BCs,
+diagnostics). value = grid points advanced per second over all ranks (cell-updates/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU (torchrun); every rank runs its own seeded sweep
+(weak scaling, no collective in the data path); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from concurrent.futures import ProcessPoolExecutor
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--form", choices=["twin", "cavity"], default="twin")
+    ap.add_argument("--ncases", type=int, default=256)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ reference (CPU) runs
+def _ref_case_worker(task):
+    """Run the compiled reference on one twin case at two step counts; per-step wall time
+    from the difference (cancels set-up and the loop-0 file writes)."""
+    from cfd_solver_b200.grid import write_inp
+    from cfd_solver_b200.workloads import make_case
+    d, s1, s2, binary = task
+    g, prm = make_case(d, "twin")
+    env = dict(os.environ)
+    env.update({"CFD_RE": repr(prm["Re"]), "CFD_RI": repr(prm["Ri"]), "CFD_PR": repr(prm["Pr"]),
+                "CFD_DT": repr(prm["dt"]), "CFD_ALPHA": repr(prm["alpha"])})
+    with tempfile.TemporaryDirectory(prefix="cfdbench_") as td:
+        write_inp(g, Path(td) / "INP.DAT")
+        times = []
+        for s in (s1, s2):
+            env["CFD_MAXSTEP"] = str(s)
+            t0 = time.perf_counter()
+            subprocess.run([binary], cwd=td, env=env, stdout=subprocess.DEVNULL, check=True)
+            times.append(time.perf_counter() - t0)
+    return g.n0 * g.n1 * (s2 - s1), max(times[1] - times[0], 1e-9)
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_sample(draws, budget_s: float, cores: int, offset: int = 0):
+    """cell-updates/s of the reference on a bounded sample of the sweep, all cores busy."""
+    binary = str(ROOT / "oracle" / "_ref" / "cfd_ref")
+    if not Path(binary).exists():
+        return None, "oracle/_ref/cfd_ref not built"
+    # ~0.84 s per 257^2 step on one core (survey probe); size the sample to the budget
+    per_step = {65: 0.02, 129: 0.1, 193: 0.35, 257: 0.84}
+    tasks, est = [], 0.0
+    k = offset
+    while est < budget_s * cores and len(tasks) < 4 * cores:
+        d = draws[k % len(draws)]
+        k += 1
+        s1, s2 = 1, 3
+        tasks.append((d, s1, s2, binary))
+        est += per_step[d["N"]] * (s1 + s2) + 0.5
+    t0 = time.perf_counter()
+    import multiprocessing as mp
+    with ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context("spawn")) as ex:
+        res = list(ex.map(_ref_case_worker, tasks))
+    wall = time.perf_counter() - t0
+    cells = sum(r[0] for r in res)
+    busy = sum(r[1] for r in res)
+    value = cells / (busy / cores)
+    sizes = sorted({t[0]["N"] for t in tasks})
+    sample = (f"{len(tasks)} twin cases of the sweep (N in {sizes}), 2 reference steps each "
+              f"(difference of 1- and 3-step runs), {cores} processes, {wall:.1f} s wall")
+    return value, sample
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from cfd_solver_b200.workloads import sweep_draws
+    draws = sweep_draws(args.ncases)
+    cores = host_cores()
+    vals = []
+    sample = None
+    for s in range(args.warmup + args.steps):
+        v, sample = reference_sample(draws, budget_s=2.0, cores=cores, offset=s * cores)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": sample}))
+            return
+        if s >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded sweep draws)",
+            "config": workload_config(args),
+            "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores,
+                             "kind": "reference", "sample": "per step: " + sample},
+            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def workload_config(args):
+    return {"workload": f"256-case batched sweep ({args.form} form)" if args.ncases == 256
+            else f"{args.ncases}-case batched sweep ({args.form} form)",
+            "cases": args.ncases, "sizes": "N x N, N in {65,129,193,257}",
+            "params": "skew U[0,0.2], Re logU[50,1000], Ri logU[0.1,10], Pr {0.71,7}, seed 1234+rank",
+            "dt": "1e-4 (reference)" if args.form == "twin" else "CFL 0.4 / max(1, sqrt(Ri))",
+            "inner_tolerances": "reference: relative L1 0.75e-2 (momentum and pressure)",
+            "l2_flush": "inputs larger than L2 (>= 2.4 GB resident per step)",
+            "parallelism": f"case-sharded, dp{args.gpus}"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, index: int):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(index)], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ our arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    import torch
+    import torch.distributed as dist
+    from cfd_solver_b200 import _lib
+    from cfd_solver_b200.solver import Batch, case_params
+    from cfd_solver_b200.workloads import SWEEP_SEED, make_case, sweep_draws
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    _lib.check(_lib.lib().cfd_set_device(local), "cfd_set_device")
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+
+    draws = sweep_draws(args.ncases, seed=SWEEP_SEED + rank)
+    grids, params = [], []
+    for d in draws:
+        g, prm = make_case(d, args.form)
+        grids.append(g)
+        params.append(case_params(g, **prm))
+    cells = sum(g.n0 * g.n1 for g in grids)
+    b = Batch(grids, params)
+    stream = torch.cuda.ExternalStream(b.stream())
+
+    for _ in range(args.warmup):
+        b.step(1)
+    b.sync()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    b.profile(True)
+    launches0 = b.launches()
+    work0 = b.work()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.step(1)
+    e1.record(stream)
+    e1.synchronize()
+    b.sync()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = b.launches() - launches0
+    work1 = b.work()
+    kt = b.kernel_times()
+    b.profile(False)
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = cells * args.steps * world / (ms_max / 1e3)
+
+    # roofline of the dominant kernel (the u/v/T sweeps): algorithmic bytes per launch from
+    # the traffic counters: per field-cell read x_k, rhs, x_{k-1} and write x_{k+1} (32 B; the
+    # first sweep skips x_{k-1}); per cell read alpha, beta, gamma (24 B)
+    dom = max(kt.items(), key=lambda kv: kv[1][0])
+    jac_ms, jac_n = kt.get("k_jac", (0.0, 0))
+    fc = work1[0] - work0[0]
+    cc = work1[1] - work0[1]
+    f0 = work1[2] - work0[2]
+    jac_bytes = 32 * fc - 8 * f0 + 24 * cc
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = (jac_bytes / 1e9) / (jac_ms / 1e3) if jac_ms > 0 else 0.0
+    traffic = None
+    tf = ROOT / "profiles" / "k_jac_traffic.json"
+    if tf.exists() and jac_n:
+        try:
+            tj = json.loads(tf.read_text())
+            # dram bytes per swept cell from the ncu capture, scaled to this run's launches
+            traffic = tj["dram_bytes_per_cell"] * cc / jac_n
+        except Exception:
+            traffic = None
+    roofline = {"kernel": "k_jac", "bound": "hbm", "achieved": achieved, "peak": peak,
+                "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "algorithmic_bytes_per_launch": jac_bytes / max(jac_n, 1),
+                "avg_launch_us": jac_ms / max(jac_n, 1) * 1e3, "launches": jac_n,
+                "share_of_kernel_time": jac_ms / max(sum(v[0] for v in kt.values()), 1e-12)}
+    kernels = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in kt.items() if v[1]}
+
+    # end to end through the C ABI with host-owned state: every step uploads the state of
+    # every case from pinned host memory, steps, and reads the new state and stats back
+    nbytes = b.state_bytes()
+    host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    b.get_state(host)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        b.set_state(host)
+        b.step(1)
+        b.get_state(host)
+        b.stats(0)
+    b.sync()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = cells * args.e2e_steps * world / float(te.item())
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline and args.form == "twin":
+        v, sample = reference_sample(draws, budget_s=args.cpu_budget, cores=host_cores())
+        if v is not None:
+            cpu = {"value": v, "unit": "cell-updates/s", "cores": host_cores(), "kind": "reference",
+                   "sample": sample}
+        else:
+            cpu = {"value": None, "unavailable": sample}
+    st0 = b.stats(0)
+    b.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded sweep draws; grids generated in INP.DAT format)",
+                "config": workload_config(args),
+                "cells_per_step": cells * world,
+                "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": "cell-updates/s",
+                        "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 200},
+                "clocks": clk, "gpu_launches": launches, "kernels": kernels,
+                "dominant_kernel": dom[0],
+                "baseline_metric_note": ("BASELINE metric is converged cases/s; one case needs "
+                                         "1e4-1e5 steps to its steady state, so a bench step is one "
+                                         "outer step of the whole sweep (see DESIGN.md)"),
+                "case0": {"it_mom": st0["it_mom"], "it_p": st0["it_p"], "status": st0["status"]}}
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

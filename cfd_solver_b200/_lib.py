@@ -20,11 +20,13 @@ ERRORS = {-1: "CFD_E_ARG", -2: "CFD_E_CUDA", -3: "CFD_E_OOM", -4: "CFD_E_DIVERGE
 PROFILE_OGRID, PROFILE_CAVITY = 0, 1
 
 # exported symbols (kept in sync with include/cfd_b200.h; tests check both)
-SYMBOLS = ("cfd_params_default", "cfd_last_error", "cfd_device_count", "cfd_case_create",
+SYMBOLS = ("cfd_params_default", "cfd_last_error", "cfd_device_count", "cfd_set_device",
+           "cfd_case_create",
            "cfd_case_step", "cfd_case_solve_to", "cfd_case_get_fields", "cfd_case_destroy",
            "cfd_batch_create", "cfd_batch_step", "cfd_batch_stats", "cfd_batch_get_plane",
            "cfd_batch_destroy", "cfd_case_bytes", "cfd_batch_profile", "cfd_batch_kernel_times",
-           "cfd_batch_sync")
+           "cfd_batch_sync", "cfd_batch_stream", "cfd_batch_launches", "cfd_batch_work",
+           "cfd_batch_state_bytes", "cfd_batch_get_state", "cfd_batch_set_state")
 
 _D = ctypes.c_double
 _PD = ctypes.POINTER(ctypes.c_double)
@@ -51,7 +53,8 @@ class CfdStepStats(ctypes.Structure):
                 ("it_p", ctypes.c_int), ("dmax", _D), ("cl", _D), ("cd", _D), ("cm", _D),
                 ("nu", _D), ("circ", _D), ("cl_pr", _D), ("cd_pr", _D), ("cl_vor", _D),
                 ("cd_vor", _D), ("q_l1", _D), ("q_l2", _D), ("q_max", _D), ("dT_l1", _D),
-                ("dT_max", _D), ("p_res_rel", _D), ("mass_res_rel", _D)]
+                ("dT_max", _D), ("p_res_rel", _D), ("mass_res_rel", _D), ("steady_res", _D),
+                ("steady_res_rel", _D)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "it_mom"}
@@ -81,6 +84,7 @@ def lib():
     L.cfd_params_default.restype = None
     L.cfd_last_error.restype = ctypes.c_char_p
     L.cfd_device_count.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    L.cfd_set_device.argtypes = [ctypes.c_int]
     L.cfd_case_create.argtypes = [ctypes.POINTER(CfdGrid), ctypes.POINTER(CfdParams), ctypes.POINTER(vp)]
     L.cfd_case_step.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CfdStepStats)]
     L.cfd_case_solve_to.argtypes = [vp, _D, ctypes.c_int, ctypes.POINTER(CfdStepStats)]
@@ -98,8 +102,19 @@ def lib():
     L.cfd_batch_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p), _PD,
                                          ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
     L.cfd_batch_sync.argtypes = [vp]
+    L.cfd_batch_stream.argtypes = [vp]
+    L.cfd_batch_stream.restype = vp
+    L.cfd_batch_launches.argtypes = [vp]
+    L.cfd_batch_launches.restype = ctypes.c_longlong
+    L.cfd_batch_work.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
+    L.cfd_batch_state_bytes.argtypes = [vp]
+    L.cfd_batch_state_bytes.restype = ctypes.c_size_t
+    L.cfd_batch_get_state.argtypes = [vp, vp, ctypes.c_size_t]
+    L.cfd_batch_set_state.argtypes = [vp, vp, ctypes.c_size_t]
+    special = {"cfd_params_default", "cfd_last_error", "cfd_case_bytes", "cfd_batch_stream",
+               "cfd_batch_launches", "cfd_batch_state_bytes"}
     for name in SYMBOLS:
-        if name not in ("cfd_params_default", "cfd_last_error", "cfd_case_bytes"):
+        if name not in special:
             getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

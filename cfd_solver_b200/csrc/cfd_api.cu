@@ -124,7 +124,7 @@ struct cfd_batch {
     std::vector<CaseDev> hc;
     std::vector<cfd_params> prm;
     std::vector<CaseGeom> geom;
-    std::vector<double> q_l2_first;
+    std::vector<double> q_l2_first, sr_first;
     CaseDev* dc = nullptr;
     double* f64 = nullptr;
     float* f32 = nullptr;
@@ -134,6 +134,8 @@ struct cfd_batch {
     double* partial = nullptr;
     unsigned int* counter = nullptr;
     int* flags = nullptr;  // [0] active (pressure), [1] mactive (momentum)
+    unsigned long long* work = nullptr;  // k_jac traffic counters
+    long long launches = 0;              // kernels launched since creation
     int* h_flags = nullptr;
     Tile* dtiles = nullptr;
     int* dcc = nullptr;
@@ -176,6 +178,7 @@ struct Prof {
     int id;
     cudaEvent_t e0{}, e1{};
     Prof(cfd_batch* b_, int id_) : b(b_), id(id_) {
+        b->launches++;
         if (b->prof) {
             e0 = get_event(b);
             e1 = get_event(b);
@@ -308,6 +311,30 @@ void initial_state(const cfd_grid* g, const cfd_params* p, const CaseDev& c, std
     }
 }
 
+// Eigenvalue bounds of D^-1 A for the Chebyshev sweeps. With E = dt/Re (alpha/dxi0^2 +
+// gamma/dxi1^2) the smooth modes of the 25-point operator sit at 1/(1 + 2.5 E) and Gershgorin
+// bounds the top: 1 + ((17/6) E + 4.5 |beta| dt/(Re dxi0 dxi1)) / (1 + 2.5 E); the 9-point
+// rows lie inside both. Margins: 0.9 below, 1.05 above. T uses Re*Pr; the reference's T
+// slot bug (atnw for annw) adds 7/9 |beta| c to the off-diagonal sum.
+void cheb_bounds(const cfd_grid& g, const cfd_params& p, CaseDev& d) {
+    const int n0 = g.n0, n1 = g.n1;
+    for (int ty = 0; ty < 2; ty++) {
+        const double scale = ty == 0 ? p.Re : p.Re * p.Pr;
+        const double cross = (ty == 1 && !p.fix_T_annw) ? 4.5 + 7.0 / 9.0 : 4.5;
+        const double cc = p.dt / (scale * g.dxi0 * g.dxi1);
+        double emax = 0.0, rmax = 0.0;
+        for (int j = 1; j < n1 - 1; j++)
+            for (int i = 0; i < n0; i++) {
+                const size_t k = (size_t)j * n0 + i;
+                const double E = p.dt / scale * (g.alph[k] / (g.dxi0 * g.dxi0) + g.gam[k] / (g.dxi1 * g.dxi1));
+                emax = std::max(emax, E);
+                rmax = std::max(rmax, ((17.0 / 6.0) * E + cross * std::fabs(g.beta[k]) * cc) / (1.0 + 2.5 * E));
+            }
+        d.cheb_a[ty] = 0.9 / (1.0 + 2.5 * emax);
+        d.cheb_b[ty] = 1.05 * (1.0 + rmax);
+    }
+}
+
 void make_tiles(int ilo, int ihi, int n1, int cid, std::vector<Tile>& out) {
     int k = 0;
     for (int j0 = 1; j0 <= n1 - 2; j0 += TY)
@@ -366,11 +393,11 @@ int one_step(cfd_batch* b) {
     for (int pair = 0; pair < npairs; pair++) {
         {
             Prof pr(b, K_JAC);
-            k_jac<<<nf, NT, 0, b->st>>>(bd, 1, pair == 0, 0);
+            k_jac<<<nf, NT, 0, b->st>>>(bd, 1, 2 * pair, 0);
         }
         {
             Prof pr(b, K_JAC);
-            k_jac<<<nf, NT, 0, b->st>>>(bd, 0, 0, 1);
+            k_jac<<<nf, NT, 0, b->st>>>(bd, 0, 2 * pair + 1, 1);
         }
         int m = 0;
         int rc = read_flag(b, 1, &m);
@@ -417,6 +444,14 @@ int one_step(cfd_batch* b) {
     return CFD_OK;
 }
 
+// steady residual: mean |du| + |dv| + |dT| per unknown cell and unit time
+double steady_res(const cfd_batch* b, int c) {
+    const double* sc = b->hscal.data() + (size_t)c * NSCAL;
+    const CaseDev& d = b->hc[c];
+    const double ncell = (double)(d.ihi - d.ilo + 1) * (d.n1 - 2);
+    return (sc[S_DUL1] + sc[S_DTL1]) / (d.dt * ncell);
+}
+
 int fetch_scalars(cfd_batch* b) {
     b->hscal.resize((size_t)b->n * NSCAL);
     b->hiscal.resize((size_t)b->n * NISCAL);
@@ -424,7 +459,10 @@ int fetch_scalars(cfd_batch* b) {
     CK(cudaMemcpyAsync(b->hiscal.data(), b->iscal, b->hiscal.size() * sizeof(int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
     for (int c = 0; c < b->n; c++) {
-        if (b->q_l2_first[c] < 0 && b->steps_done > 0) b->q_l2_first[c] = b->hscal[(size_t)c * NSCAL + S_QL2];
+        if (b->q_l2_first[c] < 0 && b->steps_done > 0) {
+            b->q_l2_first[c] = b->hscal[(size_t)c * NSCAL + S_QL2];
+            b->sr_first[c] = steady_res(b, c);
+        }
     }
     return CFD_OK;
 }
@@ -444,6 +482,9 @@ void fill_stats(cfd_batch* b, int c, cfd_step_stats* s) {
     s->p_res_rel = sc[S_NB1] > 0 ? sc[S_RL1] / sc[S_NB1] : 0.0;
     const double q0 = b->q_l2_first[c];
     s->mass_res_rel = q0 > 0 ? sc[S_QL2] / q0 : (sc[S_QL2] == 0 ? 0.0 : 1.0);
+    s->steady_res = steady_res(b, c);
+    const double r0 = b->sr_first[c];
+    s->steady_res_rel = r0 > 0 ? s->steady_res / r0 : (s->steady_res == 0 ? 0.0 : 1.0);
 }
 
 int plane_id(const char* name, int cur) {
@@ -477,6 +518,11 @@ void cfd_params_default(cfd_params* p) {
 }
 
 const char* cfd_last_error(void) { return g_err.c_str(); }
+
+int cfd_set_device(int device) {
+    CK(cudaSetDevice(device));
+    return CFD_OK;
+}
 
 int cfd_device_count(int* count) {
     int n = 0;
@@ -519,6 +565,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     b->hc.resize(ncases);
     b->prm.assign(params, params + ncases);
     b->q_l2_first.assign(ncases, -1.0);
+    b->sr_first.assign(ncases, -1.0);
     b->maxit_mom = 0;
     b->maxit_p = 0;
     for (int c = 0; c < ncases; c++) {
@@ -546,6 +593,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         d.ca = cos(p.alpha_deg * d.Pi / 180.0);
         d.ar = g.ar; d.omega_p = p.omega_p; d.lid_u = p.lid_u;
         d.tol_mom = p.tol_mom; d.atol_mom = p.atol_mom; d.tol_p = p.tol_p; d.atol_p = p.atol_p;
+        cheb_bounds(g, p, d);
         d.tile_begin = (int)ftiles.size();
         make_tiles(G.ilo, G.ihi, g.n1, c, ftiles);
         d.tile_count = (int)ftiles.size() - d.tile_begin;
@@ -593,6 +641,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     ALLOC(b->partial, sizeof(double) * PSTRIDE * std::max<size_t>(ftiles.size(), 1));
     ALLOC(b->counter, sizeof(unsigned) * ncases);
     ALLOC(b->flags, sizeof(int) * 4);
+    ALLOC(b->work, sizeof(unsigned long long) * 4);
     ALLOC(b->dtiles, sizeof(Tile) * std::max<size_t>(ntl, 1));
     ALLOC(b->dcc, sizeof(int) * std::max<size_t>(ncc, 1));
 #undef ALLOC
@@ -603,6 +652,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     cudaMemsetAsync(b->scal, 0, sizeof(double) * NSCAL * ncases, b->st);
     cudaMemsetAsync(b->iscal, 0, sizeof(int) * NISCAL * ncases, b->st);
     cudaMemsetAsync(b->counter, 0, sizeof(unsigned) * ncases, b->st);
+    cudaMemsetAsync(b->work, 0, sizeof(unsigned long long) * 4, b->st);
     CK(cudaStreamSynchronize(b->st));
     {
         const size_t smem = 2 * (size_t)(b->max_W + 1) * sizeof(double);
@@ -631,6 +681,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     bd.cases = b->dc; bd.ncases = ncases; bd.f64 = b->f64; bd.f32 = b->f32;
     bd.scal = b->scal; bd.iscal = b->iscal; bd.partial = b->partial; bd.counter = b->counter;
     bd.active = b->flags; bd.mactive = b->flags + 1;
+    bd.work = b->work;
     bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
     for (int l = 0; l < MAXLEV; l++) {
         bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
@@ -732,7 +783,7 @@ int cfd_batch_destroy(cfd_batch* b) {
     for (auto& l : b->pending) { cudaEventDestroy(l.e0); cudaEventDestroy(l.e1); }
     for (auto e : b->pool) cudaEventDestroy(e);
     cudaFree(b->f64); cudaFree(b->f32); cudaFree(b->dc); cudaFree(b->scal); cudaFree(b->iscal);
-    cudaFree(b->partial); cudaFree(b->counter); cudaFree(b->flags); cudaFree(b->dtiles); cudaFree(b->dcc);
+    cudaFree(b->partial); cudaFree(b->counter); cudaFree(b->flags); cudaFree(b->work); cudaFree(b->dtiles); cudaFree(b->dcc);
     if (b->h_flags) cudaFreeHost(b->h_flags);
     if (b->st) cudaStreamDestroy(b->st);
     delete b;
@@ -764,6 +815,58 @@ int cfd_batch_sync(cfd_batch* b) {
     return CFD_OK;
 }
 
+void* cfd_batch_stream(cfd_batch* b) { return b ? (void*)b->st : nullptr; }
+
+long long cfd_batch_launches(cfd_batch* b) { return b ? b->launches : -1; }
+
+int cfd_batch_work(cfd_batch* b, unsigned long long* out3) {
+    if (!b || !out3) return fail(CFD_E_ARG, "bad arguments");
+    CK(cudaMemcpyAsync(out3, b->work, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    return CFD_OK;
+}
+
+// the resident state of every case: u, v, p, T, up, vp (padded device planes, in case order)
+static const int kStatePlanes = 6;
+static int state_plane(const cfd_batch* b, int m) {
+    const int ids[kStatePlanes] = {P_U, P_V, P_P, P_T0 + b->cur, P_UP0 + b->cur, P_VP0 + b->cur};
+    return ids[m];
+}
+
+size_t cfd_batch_state_bytes(cfd_batch* b) {
+    if (!b) return 0;
+    size_t s = 0;
+    for (auto& d : b->hc) s += (size_t)kStatePlanes * d.ps * sizeof(double);
+    return s + 16 * sizeof(double) * b->n;
+}
+
+static int state_copy(cfd_batch* b, void* host, size_t bytes, bool to_host) {
+    if (!b || !host) return fail(CFD_E_ARG, "bad arguments");
+    if (bytes < cfd_batch_state_bytes(b)) return fail(CFD_E_ARG, "state buffer too small");
+    char* h = (char*)host;
+    for (int c = 0; c < b->n; c++) {
+        const CaseDev& d = b->hc[c];
+        for (int m = 0; m < kStatePlanes; m++) {
+            double* dev = b->f64 + d.base + H - 16 + (long long)state_plane(b, m) * d.ps;
+            const size_t nb = sizeof(double) * d.ps;
+            if (to_host) CK(cudaMemcpyAsync(h, dev, nb, cudaMemcpyDeviceToHost, b->st));
+            else CK(cudaMemcpyAsync(dev, h, nb, cudaMemcpyHostToDevice, b->st));
+            h += nb;
+        }
+        // per-case scalars that carry across steps: the reference's int time
+        if (to_host) CK(cudaMemcpyAsync(h, b->iscal + (long long)c * NISCAL + I_TIME, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+        else CK(cudaMemcpyAsync(b->iscal + (long long)c * NISCAL + I_TIME, h, sizeof(int), cudaMemcpyHostToDevice, b->st));
+        h += 16 * sizeof(double);
+    }
+    CK(cudaStreamSynchronize(b->st));
+    return CFD_OK;
+}
+
+int cfd_batch_get_state(cfd_batch* b, void* host, size_t bytes) { return state_copy(b, host, bytes, true); }
+int cfd_batch_set_state(cfd_batch* b, const void* host, size_t bytes) {
+    return state_copy(b, const_cast<void*>(host), bytes, false);
+}
+
 // ---- single case
 int cfd_case_create(const cfd_grid* g, const cfd_params* prm, cfd_case** out) {
     return cfd_batch_create(1, g, prm, out);
@@ -781,7 +884,7 @@ int cfd_case_step(cfd_case* c, int nsteps, cfd_step_stats* last) {
     return CFD_OK;
 }
 
-int cfd_case_solve_to(cfd_case* c, double mass_tol, int max_steps, cfd_step_stats* last) {
+int cfd_case_solve_to(cfd_case* c, double tol, int max_steps, cfd_step_stats* last) {
     if (!c || max_steps < 0) return fail(CFD_E_ARG, "bad arguments");
     cfd_step_stats s{};
     int done = 0;
@@ -798,11 +901,11 @@ int cfd_case_solve_to(cfd_case* c, double mass_tol, int max_steps, cfd_step_stat
             if (last) *last = s;
             return fail(CFD_E_DIVERGED, "NaN in the solution");
         }
-        if (s.mass_res_rel <= mass_tol) break;
+        if (s.steady_res_rel <= tol) break;
     }
     s.steps = done;
     if (last) *last = s;
-    if (s.mass_res_rel > mass_tol) return fail(CFD_E_NOTCONV, "max_steps reached before mass_tol");
+    if (s.steady_res_rel > tol) return fail(CFD_E_NOTCONV, "max_steps reached before the steady residual reached tol");
     return CFD_OK;
 }
 

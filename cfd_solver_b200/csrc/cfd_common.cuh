@@ -53,8 +53,8 @@ enum Field { F_U, F_V, F_T, F_UP, F_VP, NFIELD };
 enum Scalar {
     S_RHO, S_ALPHA, S_OMEGA, S_BETA, S_NB1, S_RL1, S_RL1_0,
     S_QL1, S_QL2, S_QMAX, S_DMAX, S_CL, S_CD, S_CM, S_NU, S_CIRC, S_CLP, S_CDP, S_CLV, S_CDV,
-    S_DTL1, S_DTMAX, S_DUL1,
-    S_MR0 = 24,           // 5 initial momentum residuals (L1)
+    S_DTL1, S_DTMAX, S_DUL1, S_CW0, S_CW1,  // Chebyshev weights of the u-type / T systems
+    S_MR0 = 26,           // 5 initial momentum residuals (L1)
     S_MR = S_MR0 + NFIELD,  // 5 latest momentum residuals
     NSCAL = S_MR + NFIELD + 2
 };
@@ -88,6 +88,7 @@ struct CaseDev {
     double d0, d1, dt, Re, Pr, Ri, F;
     double uinf, vinf, speed_amp, accn_amp, Pi, ar, omega_p, lid_u, sa, ca;
     double tol_mom, atol_mom, tol_p, atol_p;
+    double cheb_a[2], cheb_b[2];  // eigenvalue bounds of D^-1 A (u-type, T) for the Chebyshev sweeps
     LevelDev lev[MAXLEV];
 };
 
@@ -115,6 +116,7 @@ struct BatchDev {
     int natiles[MAXLEV];
     const int* ccases[MAXLEV];    // cases whose coarsest level is l
     int nccases[MAXLEV];
+    unsigned long long* work;  // [0] field-cells and [1] cells swept by k_jac, [2] field-cells of sweep 0
     int cur;               // which of T0/T1 (up0/up1, vp0/vp1) holds the current state
 };
 

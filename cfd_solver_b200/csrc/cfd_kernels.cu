@@ -338,12 +338,17 @@ __global__ void __launch_bounds__(NT) k_rhs(BatchDev b) {
 }
 
 // ---------------------------------------------------------------------------
-// one Jacobi sweep of the five momentum / energy systems (replaces gauss(),
-// PSolver.cpp:2280-2446). Iterates ping-pong between buffer A (the solution)
-// and the scratch B; sweeps come in pairs so the solution ends in A. The stop
-// rule is the reference's: relative L1 residual before a sweep below tol_mom
-// (or the absolute floor atol_mom) ends the solve after that sweep.
-__global__ void __launch_bounds__(NT) k_jac(BatchDev b, int to_scratch, int first, int decide) {
+// one Chebyshev-accelerated Jacobi sweep of the five momentum / energy systems
+// (replaces gauss(), PSolver.cpp:2280-2446). With the Jacobi value
+// xJ = (rhs - sum_nb a_nb x_k) / ap the three-term recurrence is
+//     x_{k+1} = w_{k+1} (x_k + g (xJ - x_k) - x_{k-1}) + x_{k-1},  g = 2 / (a + b),
+// w_1 = 1, w_2 = 1 / (1 - 1 / (2 s^2)), w_{k+1} = 1 / (1 - w_k / (4 s^2)), s = (b + a) / (b - a),
+// for eigenvalues of D^-1 A in [a, b] (bounds computed per case on the host).
+// x_{k+1} overwrites x_{k-1} in place, so the iterates ping-pong between the
+// solution buffer A and the scratch B; sweeps come in pairs and end in A. The
+// stop rule is the reference's: the relative L1 residual before a sweep below
+// tol_mom (or the absolute floor atol_mom) ends the solve after that sweep.
+__global__ void __launch_bounds__(NT) k_jac(BatchDev b, int to_scratch, int sweep, int decide) {
     const Tile t = b.ftiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
     const int* isc = b.iscal + (long long)t.c * NISCAL;
@@ -354,12 +359,23 @@ __global__ void __launch_bounds__(NT) k_jac(BatchDev b, int to_scratch, int firs
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
     const int ld = c.ld;
     double r[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
+    const bool in = i >= c.ilo && i <= c.ihi && j <= c.n1 - 2;
+    const int ncell = __syncthreads_count(in);
+    if (threadIdx.x == 0) {  // algorithmic-traffic counters (cells and field-cells swept)
+        const unsigned long long nf = (unsigned long long)__popc(mask) * ncell;
+        atomicAdd(&b.work[0], nf);
+        atomicAdd(&b.work[1], (unsigned long long)ncell);
+        if (sweep == 0) atomicAdd(&b.work[2], nf);
+    }
+    if (in) {
         const long long k = (long long)j * ld + i;
         const bool nearw = near_wall(c, i, j);
         Coef25 A, TT;
         build_coefs(c, plane(b, c, P_ALPH)[k], plane(b, c, P_BETA)[k], plane(b, c, P_GAM)[k],
                     nearw, j, A, TT);
+        const double* sc = b.scal + (long long)t.c * NSCAL;
+        const double g0 = 2.0 / (c.cheb_a[0] + c.cheb_b[0]), g1 = 2.0 / (c.cheb_a[1] + c.cheb_b[1]);
+        const double w0 = sweep == 0 ? 1.0 : sc[S_CW0], w1 = sweep == 0 ? 1.0 : sc[S_CW1];
         const int nxt = b.cur ^ 1;
         const int pa[NFIELD] = {P_US, P_VS, P_T0 + nxt, P_UP0 + nxt, P_VP0 + nxt};
         const int pb[NFIELD] = {P_BU, P_BV, P_BT, P_BUP, P_BVP};
@@ -372,9 +388,19 @@ __global__ void __launch_bounds__(NT) k_jac(BatchDev b, int to_scratch, int firs
             const Coef25& a = (f == F_T) ? TT : A;
             const double s = offsum(src, k, ld, a, nearw);
             const double rhs = plane(b, c, pr[f])[k];
-            const double res = rhs - a.p * src[k] - s;
-            store_mirrored(dst, ld, i, j, c.W, c.periodic, (rhs - s) / a.p);
-            r[f] = fabs(res);
+            const double xk = src[k];
+            const double xj = (rhs - s) / a.p;
+            const double g = (f == F_T) ? g1 : g0;
+            double xn;
+            if (sweep == 0) {
+                xn = xk + g * (xj - xk);
+            } else {
+                const double w = (f == F_T) ? w1 : w0;
+                const double xm = dst[k];
+                xn = w * (xk + g * (xj - xk) - xm) + xm;
+            }
+            store_mirrored(dst, ld, i, j, c.W, c.periodic, xn);
+            r[f] = fabs(rhs - a.p * xk - s);
         }
     }
     if (case_reduce<NFIELD, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, r) &&
@@ -383,7 +409,7 @@ __global__ void __launch_bounds__(NT) k_jac(BatchDev b, int to_scratch, int firs
         int* is = b.iscal + (long long)t.c * NISCAL;
         for (int f = 0; f < NFIELD; f++) {
             if (!(mask & (1 << f))) continue;
-            if (first) sc[S_MR0 + f] = (r[f] != 0.0) ? r[f] : 1.0;
+            if (sweep == 0) sc[S_MR0 + f] = (r[f] != 0.0) ? r[f] : 1.0;
             sc[S_MR + f] = r[f];
             is[I_MIT0 + f] += 1;
             if (decide) {
@@ -391,6 +417,13 @@ __global__ void __launch_bounds__(NT) k_jac(BatchDev b, int to_scratch, int firs
                 if (!isfinite(r[f])) { is[I_STATUS] |= ST_NAN; done = true; }
                 if (done) { is[I_MDONE0 + f] = 1; atomicSub(b.mactive, 1); }
             }
+        }
+        // Chebyshev weight of the next sweep
+        for (int ty = 0; ty < 2; ty++) {
+            const double a = c.cheb_a[ty], bb = c.cheb_b[ty];
+            const double s2 = ((bb + a) / (bb - a)) * ((bb + a) / (bb - a));
+            sc[S_CW0 + ty] = (sweep == 0) ? 1.0 / (1.0 - 1.0 / (2.0 * s2))
+                                          : 1.0 / (1.0 - sc[S_CW0 + ty] / (4.0 * s2));
         }
     }
 }
@@ -798,51 +831,57 @@ __global__ void __launch_bounds__(NT) k_mg_galerkin(BatchDev b, int l) {
 }
 
 // ---------------------------------------------------------------------------
-// pcor boundary conditions + velocity / pressure correction (PSolver.cpp:1471-1542)
+// pcor boundary conditions + velocity / pressure correction (PSolver.cpp:1471-1542);
+// also the momentum part of the steady residual, sum |u^{n+1} - u^n| + |v^{n+1} - v^n|
 __global__ void __launch_bounds__(NT) k_correct(BatchDev b) {
     const Tile t = b.ftiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
-    if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
-    const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
-    const bool cav = c.profile == CAVITY;
-    double* PC = plane(b, c, P_PCOR);
-    const long long k = (long long)j * ld + i;
-    const double pc = PC[k];
-    // pcor on the boundary after its conditions: wall copy, far field 0 / copy at inflow
-    double far = 0.0;
-    if (!cav && j == n1 - 2) {
-        const double* VEC = plane(b, c, P_VEC);
-        const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
-        if (vnn >= 0) far = pc;
+    double red[1] = {0.0};
+    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
+        const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
+        const bool cav = c.profile == CAVITY;
+        double* PC = plane(b, c, P_PCOR);
+        const long long k = (long long)j * ld + i;
+        const double pc = PC[k];
+        // pcor on the boundary after its conditions: wall copy, far field 0 / copy at inflow
+        double far = 0.0;
+        if (!cav && j == n1 - 2) {
+            const double* VEC = plane(b, c, P_VEC);
+            const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
+            if (vnn >= 0) far = pc;
+        }
+        const double pN = (j == n1 - 2) ? (cav ? pc : far) : PC[k + ld];
+        const double pS = (j == 1) ? pc : PC[k - ld];
+        const double pE = (cav && i == n0 - 2) ? pc : PC[k + 1];
+        const double pW = (cav && i == 1) ? pc : PC[k - 1];
+        const double d0 = c.d0, d1 = c.d1, dt = c.dt;
+        const double dpcor_dxi = 0.5 * (pE - pW) / d0;
+        const double dpcor_de = 0.5 * (pN - pS) / d1;
+        double* U = plane(b, c, P_U);
+        double* V = plane(b, c, P_V);
+        double* P = plane(b, c, P_P);
+        const double un = plane(b, c, P_US)[k] - dt * (plane(b, c, P_XIX)[k] * dpcor_dxi + plane(b, c, P_ETX)[k] * dpcor_de);
+        const double vn = plane(b, c, P_VS)[k] - dt * (plane(b, c, P_XIY)[k] * dpcor_dxi + plane(b, c, P_ETY)[k] * dpcor_de);
+        red[0] = fabs(un - U[k]) + fabs(vn - V[k]);
+        store_mirrored(U, ld, i, j, W, per, un);
+        store_mirrored(V, ld, i, j, W, per, vn);
+        const double pn = (c.omega_p == 1.0) ? P[k] + pc : P[k] + c.omega_p * pc;
+        store_mirrored(P, ld, i, j, W, per, pn);
+        // record the boundary pcor (output only)
+        if (j == 1) store_mirrored(PC, ld, i, 0, W, per, pc);
+        if (j == n1 - 2) store_mirrored(PC, ld, i, n1 - 1, W, per, cav ? pc : far);
+        if (cav) {
+            if (i == 1) PC[k - 1] = pc;
+            if (i == n0 - 2) PC[k + 1] = pc;
+            if (i == 1 && j == 1) PC[0] = pc;
+            if (i == n0 - 2 && j == 1) PC[n0 - 1] = pc;
+            if (i == 1 && j == n1 - 2) PC[(long long)(n1 - 1) * ld] = pc;
+            if (i == n0 - 2 && j == n1 - 2) PC[(long long)(n1 - 1) * ld + n0 - 1] = pc;
+        }
     }
-    double pN = (j == n1 - 2) ? (cav ? pc : far) : PC[k + ld];
-    double pS = (j == 1) ? pc : PC[k - ld];
-    double pE = (cav && i == n0 - 2) ? pc : PC[k + 1];
-    double pW = (cav && i == 1) ? pc : PC[k - 1];
-    const double d0 = c.d0, d1 = c.d1, dt = c.dt;
-    const double dpcor_dxi = 0.5 * (pE - pW) / d0;
-    const double dpcor_de = 0.5 * (pN - pS) / d1;
-    double* U = plane(b, c, P_U);
-    double* V = plane(b, c, P_V);
-    double* P = plane(b, c, P_P);
-    const double un = plane(b, c, P_US)[k] - dt * (plane(b, c, P_XIX)[k] * dpcor_dxi + plane(b, c, P_ETX)[k] * dpcor_de);
-    const double vn = plane(b, c, P_VS)[k] - dt * (plane(b, c, P_XIY)[k] * dpcor_dxi + plane(b, c, P_ETY)[k] * dpcor_de);
-    store_mirrored(U, ld, i, j, W, per, un);
-    store_mirrored(V, ld, i, j, W, per, vn);
-    const double pn = (c.omega_p == 1.0) ? P[k] + pc : P[k] + c.omega_p * pc;
-    store_mirrored(P, ld, i, j, W, per, pn);
-    // record the boundary pcor (output only)
-    if (j == 1) store_mirrored(PC, ld, i, 0, W, per, pc);
-    if (j == n1 - 2) store_mirrored(PC, ld, i, n1 - 1, W, per, cav ? pc : far);
-    if (cav) {
-        if (i == 1) PC[k - 1] = pc;
-        if (i == n0 - 2) PC[k + 1] = pc;
-        if (i == 1 && j == 1) PC[0] = pc;
-        if (i == n0 - 2 && j == 1) PC[n0 - 1] = pc;
-        if (i == 1 && j == n1 - 2) PC[(long long)(n1 - 1) * ld] = pc;
-        if (i == n0 - 2 && j == n1 - 2) PC[(long long)(n1 - 1) * ld + n0 - 1] = pc;
-    }
+    if (case_reduce<1, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0)
+        b.scal[(long long)t.c * NSCAL + S_DUL1] = red[0];
 }
 
 // ---------------------------------------------------------------------------

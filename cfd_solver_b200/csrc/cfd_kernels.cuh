@@ -5,7 +5,7 @@
 namespace cfd {
 __global__ void k_assemble_p(BatchDev b);
 __global__ void k_rhs(BatchDev b);
-__global__ void k_jac(BatchDev b, int to_scratch, int first, int decide);
+__global__ void k_jac(BatchDev b, int to_scratch, int sweep, int decide);
 __global__ void k_upbc(BatchDev b);
 __global__ void k_face_q(BatchDev b);
 __global__ void k_bicg_p(BatchDev b);

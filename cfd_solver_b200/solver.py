@@ -74,6 +74,29 @@ class Batch:
     def sync(self):
         _lib.check(_lib.lib().cfd_batch_sync(self.h), "cfd_batch_sync")
 
+    def stream(self) -> int:
+        return int(_lib.lib().cfd_batch_stream(self.h) or 0)
+
+    def launches(self) -> int:
+        return int(_lib.lib().cfd_batch_launches(self.h))
+
+    def work(self) -> tuple:
+        w = (ctypes.c_ulonglong * 3)()
+        _lib.check(_lib.lib().cfd_batch_work(self.h, w), "cfd_batch_work")
+        return tuple(int(x) for x in w)
+
+    def state_bytes(self) -> int:
+        return int(_lib.lib().cfd_batch_state_bytes(self.h))
+
+    def get_state(self, buf):
+        """Copy the resident state into `buf` (a writable buffer of state_bytes())."""
+        _lib.check(_lib.lib().cfd_batch_get_state(self.h, ctypes.c_void_p(_addr(buf)), self.state_bytes()),
+                   "cfd_batch_get_state")
+
+    def set_state(self, buf):
+        _lib.check(_lib.lib().cfd_batch_set_state(self.h, ctypes.c_void_p(_addr(buf)), self.state_bytes()),
+                   "cfd_batch_set_state")
+
     def close(self):
         if self.h:
             _lib.lib().cfd_batch_destroy(self.h)
@@ -92,10 +115,23 @@ class Batch:
             pass
 
 
+def _addr(buf) -> int:
+    if isinstance(buf, np.ndarray):
+        return buf.ctypes.data
+    if hasattr(buf, "data_ptr"):  # torch tensor (pinned host memory)
+        return buf.data_ptr()
+    return ctypes.addressof(ctypes.c_char.from_buffer(buf))
+
+
 def case_params(grid: Grid | None = None, **kw) -> _lib.CfdParams:
     """cfd_params with the reference's defaults, the profile taken from the grid."""
     if grid is not None and "profile" not in kw:
         kw["profile"] = _lib.PROFILE_CAVITY if grid.kind == "cavity" else _lib.PROFILE_OGRID
+    if kw.get("profile") == _lib.PROFILE_CAVITY:
+        # the reference's T-solve coefficient slip (atnw in the annw slot, PSolver.cpp:1290)
+        # makes the energy equation unstable on skewed grids; the cavity uses the
+        # Fortran-intent coefficient (solver.for:907) unless told otherwise
+        kw.setdefault("fix_T_annw", 1)
     return _lib.default_params(**kw)
 
 

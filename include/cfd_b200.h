@@ -83,6 +83,8 @@ typedef struct cfd_step_stats {
     double dT_l1, dT_max;     /* energy residual: |T^{n+1} - T^n| */
     double p_res_rel;         /* final relative L1 residual of the pressure solve */
     double mass_res_rel;      /* q_l2 / q_l2 of the case's first step */
+    double steady_res;        /* mean (|du| + |dv| + |dT|) / dt over the unknown cells */
+    double steady_res_rel;    /* steady_res / steady_res of the case's first step */
 } cfd_step_stats;
 
 typedef struct cfd_batch cfd_batch;
@@ -91,13 +93,17 @@ typedef cfd_batch cfd_case; /* a single case is a batch of one */
 void cfd_params_default(cfd_params* p);
 const char* cfd_last_error(void);
 int cfd_device_count(int* count);
+/* make `device` current for this thread's later calls (one process per GPU) */
+int cfd_set_device(int device);
 
 /* ---- single case (replaces Solver::Solver() + Solver::timeLoop()) ---- */
 int cfd_case_create(const cfd_grid* g, const cfd_params* prm, cfd_case** out);
 /* advance nsteps time steps (the body of timeLoop, PSolver.cpp:1058-1983) */
 int cfd_case_step(cfd_case* c, int nsteps, cfd_step_stats* last);
-/* step until mass_res_rel <= mass_tol (or max_steps) */
-int cfd_case_solve_to(cfd_case* c, double mass_tol, int max_steps, cfd_step_stats* last);
+/* step until steady_res_rel <= tol (or max_steps: CFD_E_NOTCONV). The continuity source q
+ * of this projection scheme keeps a compatibility defect in a closed cavity (the pressure
+ * level drifts uniformly), so convergence is judged on the steady residual. */
+int cfd_case_solve_to(cfd_case* c, double tol, int max_steps, cfd_step_stats* last);
 /* host copies of the fields, n1*n0 each, [j][i]; any pointer may be NULL */
 int cfd_case_get_fields(cfd_case* c, double* u, double* v, double* T, double* p, double* si,
                         double* vort);
@@ -121,6 +127,20 @@ int cfd_batch_profile(cfd_batch* b, int enable);
 int cfd_batch_kernel_times(cfd_batch* b, const char** names, double* total_ms, long long* launches,
                            int cap);
 int cfd_batch_sync(cfd_batch* b);
+/* the batch's CUDA stream (cudaStream_t), for callers that time or order work on it */
+void* cfd_batch_stream(cfd_batch* b);
+/* kernels launched by the batch since creation */
+long long cfd_batch_launches(cfd_batch* b);
+/* algorithmic-traffic counters of the u/v/T sweeps: [0] field-cells swept, [1] cells swept,
+ * [2] field-cells of first sweeps (which read one array less) */
+int cfd_batch_work(cfd_batch* b, unsigned long long* out3);
+
+/* ---- resident state snapshot (checkpoint / restart, host-owned stepping) ----
+ * An opaque image of every case's u, v, p, T, up, vp and step counter in the device
+ * layout; cfd_batch_state_bytes() gives its size. Use pinned host memory for speed. */
+size_t cfd_batch_state_bytes(cfd_batch* b);
+int cfd_batch_get_state(cfd_batch* b, void* host, size_t bytes);
+int cfd_batch_set_state(cfd_batch* b, const void* host, size_t bytes);
 
 #ifdef __cplusplus
 }

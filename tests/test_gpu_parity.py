@@ -99,7 +99,7 @@ def test_ogrid_rotating_wall_and_circle():
 
 def test_cavity_steps_match_oracle():
     g = cavity(33, 33, skew=0.1)
-    phys = dict(Re=100.0, Ri=1.0, dt=2e-3)
+    phys = dict(Re=100.0, Ri=1.0, dt=2e-3, fix_T_annw=1)
     gpu, ref, st, d = run_pair(g, phys, 4, fields=("u", "v", "T", "p"))
     assert st["status"] == 0
     for k in gpu:
@@ -115,7 +115,7 @@ def test_batch_invariance_bitwise():
     g2 = cavity(41, 33, skew=0.15)
     g3 = ogrid(65, 33, ar=3.0, skew=0.05)
     p1 = case_params(g1, Re=100.0, Ri=1.0, dt=1e-3)
-    p2 = case_params(g2, Re=400.0, Ri=2.0, Pr=7.0, dt=1e-3)
+    p2 = case_params(g2, Re=400.0, Ri=2.0, Pr=7.0, dt=1e-3, fix_T_annw=1)
     p3 = case_params(g3, Re=300.0, dt=5e-4)
     with Batch([g1], [p1]) as b:
         b.step(3)
