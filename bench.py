@@ -37,7 +37,7 @@ METRIC = "cell-updates/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--form", choices=["twin", "cavity"], default="twin")
@@ -148,29 +148,50 @@ def workload_config(args):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
+    """nvidia-smi samples stamped on arrival; only those inside [mark_start, mark_end] count."""
+
     def __init__(self, index: int):
+        import threading
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.lines = []
+        self.t0 = self.t1 = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200", "-i", str(index)], stdout=subprocess.PIPE,
+                                       "-lms", "100", "-i", str(index)], stdout=subprocess.PIPE,
                                       stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.p = None
+            return
+
+        def reader():
+            for line in self.p.stdout:
+                self.lines.append((time.time(), line))
+
+        self.th = threading.Thread(target=reader, daemon=True)
+        self.th.start()
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def stop(self):
         if not self.p:
             return None
         self.p.terminate()
         try:
-            out, _ = self.p.communicate(timeout=5)
+            self.p.wait(timeout=5)
         except Exception:
             self.p.kill()
-            out, _ = self.p.communicate()
+        self.th.join(timeout=5)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
+        for ts, line in self.lines:
+            if self.t0 is not None and not (self.t0 <= ts <= (self.t1 or ts)):
+                continue
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -223,12 +244,13 @@ def main():
     b = Batch(grids, params)
     stream = torch.cuda.ExternalStream(b.stream())
 
+    clocks = ClockSampler(local)
     for _ in range(args.warmup):
         b.step(1)
     b.sync()
     barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
+    clocks.mark_start()
     b.profile(True)
     launches0 = b.launches()
     work0 = b.work()
@@ -240,6 +262,7 @@ def main():
     e1.synchronize()
     b.sync()
     torch.cuda.synchronize()
+    clocks.mark_end()
     barrier()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
@@ -274,8 +297,9 @@ def main():
     if tf.exists() and jac_n:
         try:
             tj = json.loads(tf.read_text())
-            # dram bytes per swept cell from the ncu capture, scaled to this run's launches
-            traffic = tj["dram_bytes_per_cell"] * cc / jac_n
+            # ncu-measured DRAM bytes per algorithmic byte of this kernel (captured on the
+            # 64-case sweep), scaled to this run's per-launch algorithmic bytes
+            traffic = tj["dram_over_algorithmic"] * jac_bytes / jac_n
         except Exception:
             traffic = None
     roofline = {"kernel": "k_jac", "bound": "hbm", "achieved": achieved, "peak": peak,
