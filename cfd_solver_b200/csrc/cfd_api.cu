@@ -30,6 +30,12 @@ int fail(int code, const std::string& msg) {
     g_err = msg;
     return code;
 }
+}  // namespace
+
+// lets the other translation units of the library report through cfd_last_error()
+void cfd_internal_set_error(const char* msg) { g_err = msg ? msg : ""; }
+
+namespace {
 
 #define CK(call)                                                                          \
     do {                                                                                  \

@@ -135,6 +135,20 @@ long long cfd_batch_launches(cfd_batch* b);
  * [2] field-cells of first sweeps (which read one array less) */
 int cfd_batch_work(cfd_batch* b, unsigned long long* out3);
 
+/* ---- the gauss() seam on device arrays (replaces PSolver.cpp:2280-2446) ----
+ * Solves one momentum / energy system given its 25 stored coefficient planes in
+ * gauss()'s argument order (ap, ae, as, an, aw, ase, asw, ane, anw, ass, assee, assww,
+ * asse, assw, asee, asww, ann, annee, annww, anne, annw, anee, anww, aee, aww), each a
+ * device array of n1*n0 float64 in [j][i] order. phi (device, in/out) carries the
+ * initial guess and the boundary values; q is the right-hand side. periodic = 1: xi is
+ * periodic with the seam column n0-1 duplicating column 0 (the reference's O-grid);
+ * 0: columns 0 and n0-1 are fixed. Chebyshev-accelerated Jacobi sweeps until the
+ * relative L1 residual before a sweep is below tol (gauss()'s rule, PSolver.cpp:2438).
+ * Scratch (a second iterate and reduction partials) is allocated and freed per call.
+ * Returns CFD_OK, CFD_E_MAXITER or CFD_E_DIVERGED; *sweeps receives the sweep count. */
+int cfd_gauss_solve(int n0, int n1, int periodic, const double* const* coef, double* phi,
+                    const double* q, double tol, int maxit, int* sweeps, void* stream);
+
 /* ---- resident state snapshot (checkpoint / restart, host-owned stepping) ----
  * An opaque image of every case's u, v, p, T, up, vp and step counter in the device
  * layout; cfd_batch_state_bytes() gives its size. Use pinned host memory for speed. */

@@ -1,0 +1,70 @@
+"""The gauss() seam (cfd_gauss_solve) against the oracle's own gauss() solves.
+
+Inputs are the oracle's assembled coefficient planes, its initial field and the
+right-hand side it built in one step; the oracle's result is its tightly converged
+lexicographic Gauss-Seidel solution (PSolver.cpp:2280-2446 restated)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from cfd_solver_b200.grid import cavity, ogrid
+
+pytestmark = pytest.mark.gpu
+
+GAUSS_ORDER = ("p", "e", "s", "n", "w", "se", "sw", "ne", "nw", "ss", "ssee", "ssww", "sse",
+               "ssw", "see", "sww", "nn", "nnee", "nnww", "nne", "nnw", "nee", "nww", "ee", "ww")
+
+
+def system(g, which, fix_T=0):
+    """(coefficient planes in gauss() order, phi0, q, oracle result) of one system."""
+    from oracle import oracle
+    c = oracle.OracleCase(g, Re=100.0, Ri=1.0, dt=2e-3, tol_gs=1e-13, maxit_gs=600,
+                          fix_T_annw=fix_T)
+    field, rhs, out, pre = {"u": ("u", "qu", "us", "au"), "T": ("T", "qt", "T", "at")}[which]
+    phi0 = c.field(field).copy()
+    c.step(1)
+    coefs = []
+    for s in GAUSS_ORDER:
+        name = pre + s
+        if pre == "at" and s == "nnw" and not fix_T:
+            name = "atnw"  # the reference's T call passes atnw in the annw slot (PSolver.cpp:1290)
+        coefs.append(c.field(name))
+    return coefs, phi0, c.field(rhs), c.field(out)
+
+
+def gpu_solve(fn, g, coefs, phi0, q, periodic, tol=1e-13, maxit=600, **kw):
+    import torch
+    from cfd_solver_b200 import _lib
+    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in coefs]
+    ptrs = (ctypes.c_void_p * 25)(*[t.data_ptr() for t in dev])
+    phi = torch.from_numpy(phi0.copy()).cuda()
+    qd = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+    sweeps = ctypes.c_int(0)
+    torch.cuda.synchronize()
+    rc = fn(g.n0, g.n1, periodic, ptrs, ctypes.c_void_p(phi.data_ptr()), ctypes.c_void_p(qd.data_ptr()),
+            tol, maxit, ctypes.byref(sweeps), None)
+    torch.cuda.synchronize()
+    assert rc == 0, _lib.lib().cfd_last_error()
+    return phi.cpu().numpy(), sweeps.value
+
+
+@pytest.mark.parametrize("which", ["u", "T"])
+def test_gauss_seam_ogrid(which):
+    from cfd_solver_b200 import _lib
+    g = ogrid(33, 25, skew=0.1)
+    coefs, phi0, q, ref = system(g, which)
+    phi, sweeps = gpu_solve(_lib.lib().cfd_gauss_solve, g, coefs, phi0, q, 1)
+    err = np.linalg.norm(phi[1:-1] - ref[1:-1]) / np.linalg.norm(ref[1:-1])
+    assert err < 1e-10, err
+    assert np.array_equal(phi[:, -1], phi[:, 0])  # seam column kept
+    assert sweeps >= 2
+
+
+def test_gauss_seam_cavity():
+    from cfd_solver_b200 import _lib
+    g = cavity(33, 29, skew=0.15)
+    coefs, phi0, q, ref = system(g, "u", fix_T=1)
+    phi, _ = gpu_solve(_lib.lib().cfd_gauss_solve, g, coefs, phi0, q, 0)
+    err = np.linalg.norm(phi[1:-1, 1:-1] - ref[1:-1, 1:-1]) / np.linalg.norm(ref[1:-1, 1:-1])
+    assert err < 1e-10, err
