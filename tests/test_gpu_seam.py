@@ -54,7 +54,9 @@ def test_gauss_seam_ogrid(which):
     from cfd_solver_b200 import _lib
     g = ogrid(33, 25, skew=0.1)
     coefs, phi0, q, ref = system(g, which)
-    phi, sweeps = gpu_solve(_lib.lib().cfd_gauss_solve, g, coefs, phi0, q, 1)
+    # the u system starts within ~1e-3 of its solution, so 1e-13 relative is below the
+    # round-off floor; 1e-11 still leaves the result far inside the 1e-10 bar
+    phi, sweeps = gpu_solve(_lib.lib().cfd_gauss_solve, g, coefs, phi0, q, 1, tol=1e-11)
     err = np.linalg.norm(phi[1:-1] - ref[1:-1]) / np.linalg.norm(ref[1:-1])
     assert err < 1e-10, err
     assert np.array_equal(phi[:, -1], phi[:, 0])  # seam column kept
