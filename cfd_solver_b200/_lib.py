@@ -27,7 +27,7 @@ SYMBOLS = ("cfd_params_default", "cfd_last_error", "cfd_device_count", "cfd_set_
            "cfd_batch_destroy", "cfd_case_bytes", "cfd_batch_profile", "cfd_batch_kernel_times",
            "cfd_batch_sync", "cfd_batch_stream", "cfd_batch_launches", "cfd_batch_work",
            "cfd_batch_state_bytes", "cfd_batch_get_state", "cfd_batch_set_state",
-           "cfd_gauss_solve")
+           "cfd_gauss_solve", "cfd_gauss_solve_noalloc")
 
 _D = ctypes.c_double
 _PD = ctypes.POINTER(ctypes.c_double)
@@ -115,6 +115,7 @@ def lib():
     L.cfd_gauss_solve.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p,
                                   _D, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]
+    L.cfd_gauss_solve_noalloc.argtypes = L.cfd_gauss_solve.argtypes
     special = {"cfd_params_default", "cfd_last_error", "cfd_case_bytes", "cfd_batch_stream",
                "cfd_batch_launches", "cfd_batch_state_bytes"}
     for name in SYMBOLS:

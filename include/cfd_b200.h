@@ -149,6 +149,21 @@ int cfd_batch_work(cfd_batch* b, unsigned long long* out3);
 int cfd_gauss_solve(int n0, int n1, int periodic, const double* const* coef, double* phi,
                     const double* q, double tol, int maxit, int* sweeps, void* stream);
 
+/* Same solve as cfd_gauss_solve() for callers that cannot allocate device memory: code
+ * being captured into a CUDA graph, hosts whose device memory belongs to another
+ * allocator, loops that must not take the allocator's locks. No counterpart in the
+ * reference (its gauss() allocates two full arrays per call, PSolver.cpp:2288-2289).
+ * The scratch lives in one static device array sized for n0*n1 <= CFD_NOALLOC_MAX_POINTS
+ * (about 8.4 MB, held by every GPU that loads the library until the process exits);
+ * larger grids are rejected with CFD_E_ARG. The first call on a device looks up the
+ * array's device address (make that first call before any stream capture). All calls
+ * on a device share the array: calls that overlap on the GPU race, so serialise them
+ * (one stream, or one call at a time). The call allocates nothing; it clears the part
+ * of the scratch that must start at zero itself. */
+#define CFD_NOALLOC_MAX_POINTS (1 << 20)
+int cfd_gauss_solve_noalloc(int n0, int n1, int periodic, const double* const* coef, double* phi,
+                            const double* q, double tol, int maxit, int* sweeps, void* stream);
+
 /* ---- resident state snapshot (checkpoint / restart, host-owned stepping) ----
  * An opaque image of every case's u, v, p, T, up, vp and step counter in the device
  * layout; cfd_batch_state_bytes() gives its size. Use pinned host memory for speed. */
