@@ -110,7 +110,7 @@ CaseGeom case_geom(int n0, int n1, int profile) {
     CaseGeom g;
     g.periodic = profile == CFD_PROFILE_OGRID;
     g.W = g.periodic ? n0 - 1 : n0;
-    g.ld = (int)rup(g.W + 2 * H, 16);
+    g.ld = (int)rup(g.W + 2 * H + 2, 16);  // 2 columns of slack for 16-byte row copies
     g.ps = rup(16 + (long long)n1 * g.ld, 16);
     g.ilo = g.periodic ? 0 : 1;
     g.ihi = g.periodic ? g.W - 1 : n0 - 2;
@@ -139,7 +139,7 @@ struct cfd_batch {
     int* iscal = nullptr;
     double* partial = nullptr;
     unsigned int* counter = nullptr;
-    int* flags = nullptr;  // [0] active (pressure), [1] mactive (momentum)
+    int* flags = nullptr;  // [0] active (pressure), [1] mactive (momentum), [2] kernel wait timeout
     unsigned long long* work = nullptr;  // k_jac traffic counters
     long long launches = 0;              // kernels launched since creation
     int* h_flags = nullptr;
@@ -214,10 +214,12 @@ int flush_profile(cfd_batch* b) {
     return CFD_OK;
 }
 
+// reads the device flags (all four, one copy); fails if a kernel's bounded wait gave up
 int read_flag(cfd_batch* b, int idx, int* out) {
-    CK(cudaMemcpyAsync(b->h_flags + idx, b->flags + idx, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(b->h_flags, b->flags, 4 * sizeof(int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
     *out = b->h_flags[idx];
+    if (b->h_flags[2]) return fail(CFD_E_CUDA, "a bounded wait inside a kernel timed out");
     return CFD_OK;
 }
 
@@ -341,9 +343,9 @@ void cheb_bounds(const cfd_grid& g, const cfd_params& p, CaseDev& d) {
     }
 }
 
-void make_tiles(int ilo, int ihi, int n1, int cid, std::vector<Tile>& out) {
+void make_tiles(int ilo, int ihi, int n1, int cid, std::vector<Tile>& out, int ty = TY) {
     int k = 0;
-    for (int j0 = 1; j0 <= n1 - 2; j0 += TY)
+    for (int j0 = 1; j0 <= n1 - 2; j0 += ty)
         for (int i0 = (ilo / TX) * TX; i0 <= ihi; i0 += TX) out.push_back({cid, i0, j0, k++});
 }
 
@@ -399,11 +401,11 @@ int one_step(cfd_batch* b) {
     for (int pair = 0; pair < npairs; pair++) {
         {
             Prof pr(b, K_JAC);
-            k_jac<<<nf, NT, 0, b->st>>>(bd, 1, 2 * pair, 0);
+            k_jac<<<bd.njtiles, NT, kJacSmem, b->st>>>(bd, 1, 2 * pair, 0);
         }
         {
             Prof pr(b, K_JAC);
-            k_jac<<<nf, NT, 0, b->st>>>(bd, 0, 2 * pair + 1, 1);
+            k_jac<<<bd.njtiles, NT, kJacSmem, b->st>>>(bd, 0, 2 * pair + 1, 1);
         }
         int m = 0;
         int rc = read_flag(b, 1, &m);
@@ -565,7 +567,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
 
     // ---- geometry, offsets, tiles
     long long off64 = 0, off32 = 0;
-    std::vector<Tile> ftiles;
+    std::vector<Tile> ftiles, jtiles;
     std::vector<std::vector<Tile>> at(MAXLEV), mt(MAXLEV);
     std::vector<std::vector<int>> cc(MAXLEV);
     b->hc.resize(ncases);
@@ -603,6 +605,9 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         d.tile_begin = (int)ftiles.size();
         make_tiles(G.ilo, G.ihi, g.n1, c, ftiles);
         d.tile_count = (int)ftiles.size() - d.tile_begin;
+        d.jt_begin = (int)jtiles.size();
+        make_tiles(G.ilo, G.ihi, g.n1, c, jtiles, TYJ);
+        d.jt_count = (int)jtiles.size() - d.jt_begin;
         d.nlev = (int)G.lev.size();
         for (int l = 0; l < d.nlev; l++) {
             const LevelGeom& lg = G.lev[l];
@@ -629,7 +634,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     b->n32 = off32 + 32;
 
     // ---- device allocations
-    size_t ntl = ftiles.size();
+    size_t ntl = ftiles.size() + jtiles.size();
     for (int l = 0; l < MAXLEV; l++) ntl += at[l].size() + mt[l].size();
     size_t ncc = 0;
     for (int l = 0; l < MAXLEV; l++) ncc += cc[l].size();
@@ -664,10 +669,13 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         const size_t smem = 2 * (size_t)(b->max_W + 1) * sizeof(double);
         if (smem > 48 * 1024)
             CK(cudaFuncSetAttribute(k_bc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(k_jac, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacSmem));
     }
 
     // ---- tile tables
     std::vector<Tile> all(ftiles);
+    const size_t pos_jt = all.size();
+    all.insert(all.end(), jtiles.begin(), jtiles.end());
     std::vector<int> allcc;
     size_t pos_at[MAXLEV], pos_mt[MAXLEV], pos_cc[MAXLEV];
     for (int l = 0; l < MAXLEV; l++) {
@@ -689,6 +697,8 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     bd.active = b->flags; bd.mactive = b->flags + 1;
     bd.work = b->work;
     bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
+    bd.jtiles = b->dtiles + pos_jt; bd.njtiles = (int)jtiles.size();
+    bd.error = b->flags + 2;
     for (int l = 0; l < MAXLEV; l++) {
         bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
         bd.mtiles[l] = b->dtiles + pos_mt[l]; bd.nmtiles[l] = (int)mt[l].size();

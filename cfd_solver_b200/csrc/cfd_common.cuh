@@ -23,6 +23,7 @@ namespace cfd {
 constexpr int H = 2;          // halo columns on each side
 constexpr int TX = 32;        // tile width (cells), one warp per tile row
 constexpr int TY = 8;         // tile height
+constexpr int TYJ = 16;       // tile height of the u/v/T sweep kernel (two cells per thread)
 constexpr int NT = TX * TY;   // threads per tile kernel
 constexpr int MAXLEV = 12;    // multigrid levels per case
 constexpr int BC_THREADS = 256;
@@ -83,6 +84,7 @@ struct CaseDev {
     int periodic, ilo, ihi, profile;
     long long base, ps;
     int tile_begin, tile_count;     // fine-grid tiles of this case
+    int jt_begin, jt_count;         // 32 x 16 tiles of this case (u/v/T sweeps)
     int nlev;
     int fix_T_annw, fix_circ_de, warm_up;
     double d0, d1, dt, Re, Pr, Ri, F;
@@ -108,8 +110,11 @@ struct BatchDev {
     unsigned int* counter; // per case, last-block detection
     int* active;           // global count of cases still iterating (pressure)
     int* mactive;          // global count of (case, field) pairs still iterating (momentum)
+    int* error;            // set when a bounded wait in a kernel gives up
     const Tile* ftiles;    // fine-grid tiles of every case (FP64 kernels, multigrid level 0)
     int nftiles;
+    const Tile* jtiles;    // 32 x 16 tiles of every case (u/v/T sweeps)
+    int njtiles;
     const Tile* mtiles[MAXLEV];   // level-l tiles of the cases for which l is not the coarsest level
     int nmtiles[MAXLEV];
     const Tile* atiles[MAXLEV];   // level-l tiles of every case that has level l (set-up)

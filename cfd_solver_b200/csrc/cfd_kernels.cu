@@ -20,6 +20,7 @@
 #include "cfd_common.cuh"
 #include "cfd_reduce.cuh"
 #include "cfd_kernels.cuh"
+#include "cfd_bulk.cuh"
 
 namespace cfd {
 
@@ -345,85 +346,216 @@ __global__ void __launch_bounds__(NT) k_rhs(BatchDev b) {
 // w_1 = 1, w_2 = 1 / (1 - 1 / (2 s^2)), w_{k+1} = 1 / (1 - w_k / (4 s^2)), s = (b + a) / (b - a),
 // for eigenvalues of D^-1 A in [a, b] (bounds computed per case on the host).
 // x_{k+1} overwrites x_{k-1} in place, so the iterates ping-pong between the
-// solution buffer A and the scratch B; sweeps come in pairs and end in A. The
-// stop rule is the reference's: the relative L1 residual before a sweep below
-// tol_mom (or the absolute floor atol_mom) ends the solve after that sweep.
-__global__ void __launch_bounds__(NT) k_jac(BatchDev b, int to_scratch, int sweep, int decide) {
-    const Tile t = b.ftiles[blockIdx.x];
+// solution buffer A and the scratch B; sweeps come in pairs and end in A. The stop
+// rule is the reference's: the relative L1 residual before a sweep below tol_mom (or
+// the absolute floor atol_mom) ends the solve after that sweep.
+//
+// A CTA owns a 32 x 16 tile (two cells per thread). For each active field the tile of
+// x_k plus its 2-cell halo is brought into shared memory by bulk asynchronous copies
+// (one per row, completed on an mbarrier), double-buffered so the next field's tile
+// streams in while this one is swept. The 25-point operator has 10 distinct
+// coefficients (PSolver.cpp:791-848), built in registers from alpha, beta, gamma.
+constexpr int JTW = TX + 4;   // tile columns incl. halo
+constexpr int JTH = TYJ + 4;  // tile rows incl. halo
+
+// Per cell the operator is fixed by E = dt alpha/(Re dxi0^2), G = dt gamma/(Re dxi1^2) and
+// B = dt beta/(Re dxi0 dxi1): 4th-order rows (PSolver.cpp:791-821) have
+//   ae = aw = -4/3 E, aee = aww = E/12, an = as = -4/3 G, ann = ass = G/12,
+//   ane = asw = 8/9 B, anw = ase = -8/9 B, annee = assww = B/72, annww = assee = -B/72,
+//   anne = assw = anee = asww = -B/9, annw = asse = anww = asee = B/9, ap = 1 + 5/2 (E + G);
+// 9-point rows (PSolver.cpp:766-775): ae = aw = -E, an = as = -G, ane = asw = B/2,
+// anw = ase = -B/2, ap = 1 + 2 (E + G), with the wall-row couplings folded out on the
+// O-grid (PSolver.cpp:851-882). The T system divides E, G, B by Pr.
+struct CellOp {
+    double E, G, B;
+    unsigned char nearw, drop_s, drop_n;
+};
+
+__device__ __forceinline__ void cell_op(const CaseDev& c, double al, double be, double ga, int i, int j,
+                                        CellOp& o) {
+    const double dt = c.dt, Re = c.Re;
+    o.E = dt * al / (Re * c.d0 * c.d0);
+    o.G = dt * ga / (Re * c.d1 * c.d1);
+    o.B = dt * be / (Re * c.d0 * c.d1);
+    o.nearw = near_wall(c, i, j);
+    o.drop_s = c.profile == OGRID && j == 1;
+    o.drop_n = c.profile == OGRID && j == c.n1 - 2;
+}
+
+// off-centre sum of the operator on the shared-memory tile, u-type scaling
+__device__ __forceinline__ double tile_sum(const double* S, int o, const CellOp& a) {
+    constexpr int R = JTW, R2 = 2 * JTW;
+    if (a.nearw) {
+        double s = -a.E * (S[o + 1] + S[o - 1]);
+        double n = -a.G * S[o + R] + 0.5 * a.B * (S[o + R + 1] - S[o + R - 1]);
+        double so = -a.G * S[o - R] + 0.5 * a.B * (S[o - R - 1] - S[o - R + 1]);
+        if (!a.drop_n) s += n;
+        if (!a.drop_s) s += so;
+        return s;
+    }
+    const double ex = (-4.0 / 3.0) * (S[o + 1] + S[o - 1]) + (1.0 / 12.0) * (S[o + 2] + S[o - 2]);
+    const double gy = (-4.0 / 3.0) * (S[o + R] + S[o - R]) + (1.0 / 12.0) * (S[o + R2] + S[o - R2]);
+    const double bx = (8.0 / 9.0) * (S[o + R + 1] + S[o - R - 1] - S[o + R - 1] - S[o - R + 1]) +
+                      (1.0 / 72.0) * (S[o + R2 + 2] + S[o - R2 - 2] - S[o + R2 - 2] - S[o - R2 + 2]) +
+                      (1.0 / 9.0) * (S[o + R2 - 1] + S[o - R2 + 1] + S[o + R - 2] + S[o - R + 2] -
+                                     S[o + R2 + 1] - S[o - R2 - 1] - S[o + R + 2] - S[o - R - 2]);
+    return a.E * ex + a.G * gy + a.B * bx;
+}
+
+// shared memory per field: x_k tile with halo, rhs tile, x_{k-1} tile
+constexpr int JT_FIELD = JTW * JTH + 2 * TX * TYJ;
+constexpr size_t JAC_SMEM = (size_t)NFIELD * JT_FIELD * sizeof(double);
+const size_t kJacSmem = JAC_SMEM;
+
+__global__ void __launch_bounds__(NT, 3) k_jac(BatchDev b, int to_scratch, int sweep, int decide) {
+    extern __shared__ __align__(128) double jsm[];
+    __shared__ __align__(8) uint64_t bar[NFIELD];
+    const Tile t = b.jtiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
     const int* isc = b.iscal + (long long)t.c * NISCAL;
     int mask = 0;
 #pragma unroll
     for (int f = 0; f < NFIELD; f++) mask |= (isc[I_MDONE0 + f] == 0) << f;
     if (mask == 0) return;  // uniform over the case's CTAs
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
-    const int ld = c.ld;
+    const int tid = threadIdx.x;
+    const int ld = c.ld, n1 = c.n1;
+    const int nxt = b.cur ^ 1;
+
+    // tile geometry: halo tile = global rows jlo..jhi, columns c0 .. c0+ncol-1 (ncol even,
+    // 16-byte rows); interior tiles = rows j0..jin_hi, columns i0 .. i0+nint-1
+    const int c0 = t.i0 - 2;
+    const int jlo = max(t.j0 - 2, 0), jhi = min(t.j0 + TYJ + 1, n1 - 1);
+    const int jin_hi = min(t.j0 + TYJ - 1, n1 - 2);
+    int ncol = min(JTW, c.ihi + 2 - c0 + 1);
+    ncol += ncol & 1;
+    int nint = min(TX, c.ihi - t.i0 + 1);
+    nint += nint & 1;
+    const unsigned hrow = (unsigned)ncol * 8u, irow = (unsigned)nint * 8u;
+    const unsigned nh = (unsigned)(jhi - jlo + 1), ni = (unsigned)(jin_hi - t.j0 + 1);
+    const bool need_prev = sweep > 0;
+    if (tid == 0) {
+#pragma unroll
+        for (int f = 0; f < NFIELD; f++) mbar_init(&bar[f], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    // warp 0 puts every active field's tiles in flight at once
+    if (tid < 32) {
+        for (int f = 0; f < NFIELD; f++) {
+            if (!(mask & (1 << f))) continue;
+            const int pa = f < 2 ? P_US + f : P_T0 + 2 * (f - 2) + nxt;
+            const double* src = plane(b, c, to_scratch ? pa : P_BU + f);
+            const double* rhs = plane(b, c, P_RU + f);
+            const double* prv = plane(b, c, to_scratch ? P_BU + f : pa);
+            double* sm = jsm + f * JT_FIELD;
+            if (tid == 0)
+                mbar_arrive_expect_tx(&bar[f], hrow * nh + irow * ni * (need_prev ? 2u : 1u));
+            __syncwarp();
+            for (int r = jlo + tid; r <= jhi; r += 32)
+                bulk_g2s(sm + (r - (t.j0 - 2)) * JTW, src + (long long)r * ld + c0, hrow, &bar[f]);
+            for (int r = t.j0 + tid; r <= jin_hi; r += 32) {
+                bulk_g2s(sm + JTW * JTH + (r - t.j0) * TX, rhs + (long long)r * ld + t.i0, irow, &bar[f]);
+                if (need_prev)
+                    bulk_g2s(sm + JTW * JTH + TX * TYJ + (r - t.j0) * TX, prv + (long long)r * ld + t.i0, irow,
+                             &bar[f]);
+            }
+        }
+    }
+
+    const int li = tid % TX, lj = tid / TX;
+    const int i = t.i0 + li;
+    const int jA = t.j0 + lj, jB = jA + TY;
+    const bool inA = i >= c.ilo && i <= c.ihi && jA <= n1 - 2;
+    const bool inB = i >= c.ilo && i <= c.ihi && jB <= n1 - 2;
+    // operators of the two cells
+    CellOp A0, A1;
+    const long long kA = (long long)jA * ld + i, kB = (long long)jB * ld + i;
+    const double* AL = plane(b, c, P_ALPH);
+    const double* BE = plane(b, c, P_BETA);
+    const double* GA = plane(b, c, P_GAM);
+    if (inA) cell_op(c, AL[kA], BE[kA], GA[kA], i, jA, A0);
+    if (inB) cell_op(c, AL[kB], BE[kB], GA[kB], i, jB, A1);
+    const double* sc = b.scal + (long long)t.c * NSCAL;
+    const double g0 = 2.0 / (c.cheb_a[0] + c.cheb_b[0]), g1 = 2.0 / (c.cheb_a[1] + c.cheb_b[1]);
+    const double w0 = sweep == 0 ? 1.0 : sc[S_CW0], w1 = sweep == 0 ? 1.0 : sc[S_CW1];
+    const double rPr = 1.0 / c.Pr;
+    const bool tbug = !c.fix_T_annw;
+    const int oA = (lj + 2) * JTW + (li + 2), oB = oA + TY * JTW;
+
     double r[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const bool in = i >= c.ilo && i <= c.ihi && j <= c.n1 - 2;
-    const int ncell = __syncthreads_count(in);
-    if (threadIdx.x == 0) {  // algorithmic-traffic counters (cells and field-cells swept)
+    bool ok = true;
+#pragma unroll
+    for (int f = 0; f < NFIELD; f++) {
+        if (!(mask & (1 << f))) continue;
+        ok = __syncthreads_and(mbar_wait_bounded(&bar[f], 0)) && ok;
+        if (!ok) continue;
+        const double* S = jsm + f * JT_FIELD;
+        const double* Rs = S + JTW * JTH;
+        const double* Ps = Rs + TX * TYJ;
+        const int pa = f < 2 ? P_US + f : P_T0 + 2 * (f - 2) + nxt;
+        double* dst = plane(b, c, to_scratch ? P_BU + f : pa);
+        const bool isT = f == F_T;
+        const double g = isT ? g1 : g0, w = isT ? w1 : w0;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const bool in = h ? inB : inA;
+            if (!in) continue;
+            const CellOp& a = h ? A1 : A0;
+            const int o = h ? oB : oA;
+            const int oi = (lj + h * TY) * TX + li;
+            double sum = tile_sum(S, o, a);
+            const double ratio = a.nearw ? 2.0 : 2.5;
+            double ap = 1.0 + ratio * (a.E + a.G);
+            if (isT) {
+                // the reference's T solve passes atnw in the annw slot (PSolver.cpp:1290):
+                // the (i-1, j+2) coefficient becomes anw = -8/9 B instead of B/9
+                if (tbug && !a.nearw) sum -= a.B * S[o + 2 * JTW - 1];
+                sum *= rPr;
+                ap = 1.0 + ratio * (a.E + a.G) * rPr;
+            }
+            const double rhs = Rs[oi], xk = S[o];
+            const double xj = (rhs - sum) / ap;
+            double xn = xk + g * (xj - xk);
+            if (need_prev) {
+                const double xm = Ps[oi];
+                xn = w * (xk + g * (xj - xk) - xm) + xm;
+            }
+            store_mirrored(dst, ld, i, h ? jB : jA, c.W, c.periodic, xn);
+            r[f] += fabs(rhs - ap * xk - sum);
+        }
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(b.error, 1);
+        // let copies still in flight land before the CTA leaves
+        for (int f = 0; f < NFIELD; f++)
+            if (mask & (1 << f)) mbar_wait_bounded(&bar[f], 0);
+    }
+    const int ncell = __syncthreads_count(inA) + __syncthreads_count(inB);
+    if (tid == 0) {  // algorithmic-traffic counters (cells and field-cells swept)
         const unsigned long long nf = (unsigned long long)__popc(mask) * ncell;
         atomicAdd(&b.work[0], nf);
         atomicAdd(&b.work[1], (unsigned long long)ncell);
         if (sweep == 0) atomicAdd(&b.work[2], nf);
     }
-    if (in) {
-        const long long k = (long long)j * ld + i;
-        const bool nearw = near_wall(c, i, j);
-        Coef25 A, TT;
-        build_coefs(c, plane(b, c, P_ALPH)[k], plane(b, c, P_BETA)[k], plane(b, c, P_GAM)[k],
-                    nearw, j, A, TT);
-        const double* sc = b.scal + (long long)t.c * NSCAL;
-        const double g0 = 2.0 / (c.cheb_a[0] + c.cheb_b[0]), g1 = 2.0 / (c.cheb_a[1] + c.cheb_b[1]);
-        const double w0 = sweep == 0 ? 1.0 : sc[S_CW0], w1 = sweep == 0 ? 1.0 : sc[S_CW1];
-        const int nxt = b.cur ^ 1;
-        const int pa[NFIELD] = {P_US, P_VS, P_T0 + nxt, P_UP0 + nxt, P_VP0 + nxt};
-        const int pb[NFIELD] = {P_BU, P_BV, P_BT, P_BUP, P_BVP};
-        const int pr[NFIELD] = {P_RU, P_RV, P_RT, P_RUP, P_RVP};
-#pragma unroll
-        for (int f = 0; f < NFIELD; f++) {
-            if (!(mask & (1 << f))) continue;
-            const double* src = plane(b, c, to_scratch ? pa[f] : pb[f]);
-            double* dst = plane(b, c, to_scratch ? pb[f] : pa[f]);
-            const Coef25& a = (f == F_T) ? TT : A;
-            const double s = offsum(src, k, ld, a, nearw);
-            const double rhs = plane(b, c, pr[f])[k];
-            const double xk = src[k];
-            const double xj = (rhs - s) / a.p;
-            const double g = (f == F_T) ? g1 : g0;
-            double xn;
-            if (sweep == 0) {
-                xn = xk + g * (xj - xk);
-            } else {
-                const double w = (f == F_T) ? w1 : w0;
-                const double xm = dst[k];
-                xn = w * (xk + g * (xj - xk) - xm) + xm;
-            }
-            store_mirrored(dst, ld, i, j, c.W, c.periodic, xn);
-            r[f] = fabs(rhs - a.p * xk - s);
-        }
-    }
-    if (case_reduce<NFIELD, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, r) &&
-        threadIdx.x == 0) {
-        double* sc = b.scal + (long long)t.c * NSCAL;
+    if (case_reduce<NFIELD, 0u>(b, t.c, blockIdx.x, c.jt_begin, c.jt_count, r) && tid == 0) {
+        double* scw = b.scal + (long long)t.c * NSCAL;
         int* is = b.iscal + (long long)t.c * NISCAL;
         for (int f = 0; f < NFIELD; f++) {
             if (!(mask & (1 << f))) continue;
-            if (sweep == 0) sc[S_MR0 + f] = (r[f] != 0.0) ? r[f] : 1.0;
-            sc[S_MR + f] = r[f];
+            if (sweep == 0) scw[S_MR0 + f] = (r[f] != 0.0) ? r[f] : 1.0;
+            scw[S_MR + f] = r[f];
             is[I_MIT0 + f] += 1;
             if (decide) {
-                bool done = (r[f] / sc[S_MR0 + f] < c.tol_mom) || (r[f] <= c.atol_mom);
+                bool done = (r[f] / scw[S_MR0 + f] < c.tol_mom) || (r[f] <= c.atol_mom);
                 if (!isfinite(r[f])) { is[I_STATUS] |= ST_NAN; done = true; }
                 if (done) { is[I_MDONE0 + f] = 1; atomicSub(b.mactive, 1); }
             }
         }
-        // Chebyshev weight of the next sweep
-        for (int ty = 0; ty < 2; ty++) {
+        for (int ty = 0; ty < 2; ty++) {  // Chebyshev weight of the next sweep
             const double a = c.cheb_a[ty], bb = c.cheb_b[ty];
             const double s2 = ((bb + a) / (bb - a)) * ((bb + a) / (bb - a));
-            sc[S_CW0 + ty] = (sweep == 0) ? 1.0 / (1.0 - 1.0 / (2.0 * s2))
-                                          : 1.0 / (1.0 - sc[S_CW0 + ty] / (4.0 * s2));
+            scw[S_CW0 + ty] = (sweep == 0) ? 1.0 / (1.0 - 1.0 / (2.0 * s2))
+                                           : 1.0 / (1.0 - scw[S_CW0 + ty] / (4.0 * s2));
         }
     }
 }
