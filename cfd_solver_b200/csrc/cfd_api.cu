@@ -6,6 +6,7 @@
 // sequence of launches (the step of PSolver.cpp:1058-1983); the inner solves
 // iterate on the device and the host only reads a 4-byte "cases still
 // iterating" counter to decide when to stop launching.
+#include <cuda.h>  // CUtensorMap types (the encoder is fetched through the runtime)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -123,6 +124,22 @@ struct Launch {
     cudaEvent_t e0, e1;
 };
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn tensor_map_encoder() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
 }  // namespace
 
 struct cfd_batch {
@@ -145,11 +162,12 @@ struct cfd_batch {
     int* h_flags = nullptr;
     Tile* dtiles = nullptr;
     int* dcc = nullptr;
+    char* dtmaps = nullptr;  // two CUtensorMaps per case
     BatchDev bd{};
     int nlev_max = 0;
     int ncol[MAXLEV] = {};
     int maxit_mom = 100, maxit_p = 200;
-    int coarse_sweeps = 30;
+    int coarse_sweeps = 12;
     int max_W = 0;
     int cur = 0;
     long long steps_done = 0;
@@ -359,9 +377,9 @@ int run_vcycle(cfd_batch* b) {
             k_mg_coarse<<<bd.nccases[l], 1024, 0, b->st>>>(bd, l, b->coarse_sweeps);
         }
         if (bd.nmtiles[l] > 0) {
-            for (int col = 0; col < b->ncol[l]; col++) {
+            {   // pre-smoothing from the zero guess the restriction (or the Krylov step) left
                 Prof pr(b, K_MG_SMOOTH);
-                k_mg_smooth<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l, col);
+                k_mg_smooth_blk<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l, 0, 1);
             }
             {
                 Prof pr(b, K_MG_RESID);
@@ -379,9 +397,9 @@ int run_vcycle(cfd_batch* b) {
             Prof pr(b, K_MG_PROLONG);
             k_mg_prolong<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l);
         }
-        for (int col = b->ncol[l] - 1; col >= 0; col--) {
+        {
             Prof pr(b, K_MG_SMOOTH);
-            k_mg_smooth<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l, col);
+            k_mg_smooth_blk<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l, 1, 0);
         }
     }
     return CFD_OK;
@@ -653,6 +671,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     ALLOC(b->counter, sizeof(unsigned) * ncases);
     ALLOC(b->flags, sizeof(int) * 4);
     ALLOC(b->work, sizeof(unsigned long long) * 4);
+    ALLOC(b->dtmaps, (size_t)256 * ncases);
     ALLOC(b->dtiles, sizeof(Tile) * std::max<size_t>(ntl, 1));
     ALLOC(b->dcc, sizeof(int) * std::max<size_t>(ncc, 1));
 #undef ALLOC
@@ -696,6 +715,30 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     bd.scal = b->scal; bd.iscal = b->iscal; bd.partial = b->partial; bd.counter = b->counter;
     bd.active = b->flags; bd.mactive = b->flags + 1;
     bd.work = b->work;
+    bd.tmaps = b->dtmaps;
+    {
+        // 3-D tensor maps over each case's FP64 planes: x = column + 2 (from the halo column
+        // -2), y = row, z = plane; boxes 36 x 20 (tile + halo) and 32 x 16 (tile)
+        EncodeTiledFn enc = tensor_map_encoder();
+        if (!enc) return cleanup(fail(CFD_E_CUDA, "cuTensorMapEncodeTiled unavailable"));
+        std::vector<unsigned char> maps((size_t)256 * ncases);
+        for (int c = 0; c < ncases; c++) {
+            const CaseDev& d = b->hc[c];
+            void* gaddr = b->f64 + d.base + H - 2;
+            const cuuint64_t dims[3] = {(cuuint64_t)d.ld, (cuuint64_t)d.n1, (cuuint64_t)NPLANES};
+            const cuuint64_t strides[2] = {(cuuint64_t)d.ld * 8, (cuuint64_t)d.ps * 8};
+            const cuuint32_t box0[3] = {TX + 4, TYJ + 4, 1}, box1[3] = {TX, TYJ, 1}, es[3] = {1, 1, 1};
+            CUtensorMap* m = reinterpret_cast<CUtensorMap*>(maps.data() + (size_t)256 * c);
+            for (int k = 0; k < 2; k++) {
+                CUresult r = enc(m + k, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, gaddr, dims, strides, k ? box1 : box0, es,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                if (r != CUDA_SUCCESS)
+                    return cleanup(fail(CFD_E_CUDA, "cuTensorMapEncodeTiled failed for case " + std::to_string(c)));
+            }
+        }
+        CK(cudaMemcpy(b->dtmaps, maps.data(), maps.size(), cudaMemcpyHostToDevice));
+    }
     bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
     bd.jtiles = b->dtiles + pos_jt; bd.njtiles = (int)jtiles.size();
     bd.error = b->flags + 2;
@@ -799,7 +842,7 @@ int cfd_batch_destroy(cfd_batch* b) {
     for (auto& l : b->pending) { cudaEventDestroy(l.e0); cudaEventDestroy(l.e1); }
     for (auto e : b->pool) cudaEventDestroy(e);
     cudaFree(b->f64); cudaFree(b->f32); cudaFree(b->dc); cudaFree(b->scal); cudaFree(b->iscal);
-    cudaFree(b->partial); cudaFree(b->counter); cudaFree(b->flags); cudaFree(b->work); cudaFree(b->dtiles); cudaFree(b->dcc);
+    cudaFree(b->partial); cudaFree(b->counter); cudaFree(b->flags); cudaFree(b->work); cudaFree(b->dtiles); cudaFree(b->dcc); cudaFree(b->dtmaps);
     if (b->h_flags) cudaFreeHost(b->h_flags);
     if (b->st) cudaStreamDestroy(b->st);
     delete b;

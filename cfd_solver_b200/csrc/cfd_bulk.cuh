@@ -55,6 +55,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     return ok != 0;
 }
 
+// 3-D tiled tensor load (box from a CUtensorMap in global memory) into shared memory;
+// x must be a multiple of 16 bytes / element size (2 for float64), other coordinates free
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
 // bounded wait for phase `parity` of `bar`; false when it gave up
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
     for (unsigned n = 0; n < kWaitPolls; n++)

@@ -122,6 +122,8 @@ struct BatchDev {
     const int* ccases[MAXLEV];    // cases whose coarsest level is l
     int nccases[MAXLEV];
     unsigned long long* work;  // [0] field-cells and [1] cells swept by k_jac, [2] field-cells of sweep 0
+    const char* tmaps;     // per case two 128-byte CUtensorMaps over its FP64 planes (x, y, plane):
+                           // [0] box 36 x 20 (tile + 2-cell halo), [1] box 32 x 16 (tile)
     int cur;               // which of T0/T1 (up0/up1, vp0/vp1) holds the current state
 };
 

@@ -402,14 +402,15 @@ __device__ __forceinline__ double tile_sum(const double* S, int o, const CellOp&
     return a.E * ex + a.G * gy + a.B * bx;
 }
 
-// shared memory per field: x_k tile with halo, rhs tile, x_{k-1} tile
+// shared memory per field: x_k tile with halo, rhs tile, x_{k-1} tile (each 128-byte aligned)
 constexpr int JT_FIELD = JTW * JTH + 2 * TX * TYJ;
-constexpr size_t JAC_SMEM = (size_t)NFIELD * JT_FIELD * sizeof(double);
+constexpr size_t JAC_SMEM = (size_t)NFIELD * JT_FIELD * sizeof(double) + 128;
 const size_t kJacSmem = JAC_SMEM;
 
 __global__ void __launch_bounds__(NT, 3) k_jac(BatchDev b, int to_scratch, int sweep, int decide) {
-    extern __shared__ __align__(128) double jsm[];
+    extern __shared__ __align__(128) unsigned char jraw[];
     __shared__ __align__(8) uint64_t bar[NFIELD];
+    double* jsm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(jraw) + 127) & ~uintptr_t(127));
     const Tile t = b.jtiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
     const int* isc = b.iscal + (long long)t.c * NISCAL;
@@ -420,47 +421,28 @@ __global__ void __launch_bounds__(NT, 3) k_jac(BatchDev b, int to_scratch, int s
     const int tid = threadIdx.x;
     const int ld = c.ld, n1 = c.n1;
     const int nxt = b.cur ^ 1;
-
-    // tile geometry: halo tile = global rows jlo..jhi, columns c0 .. c0+ncol-1 (ncol even,
-    // 16-byte rows); interior tiles = rows j0..jin_hi, columns i0 .. i0+nint-1
-    const int c0 = t.i0 - 2;
-    const int jlo = max(t.j0 - 2, 0), jhi = min(t.j0 + TYJ + 1, n1 - 1);
-    const int jin_hi = min(t.j0 + TYJ - 1, n1 - 2);
-    int ncol = min(JTW, c.ihi + 2 - c0 + 1);
-    ncol += ncol & 1;
-    int nint = min(TX, c.ihi - t.i0 + 1);
-    nint += nint & 1;
-    const unsigned hrow = (unsigned)ncol * 8u, irow = (unsigned)nint * 8u;
-    const unsigned nh = (unsigned)(jhi - jlo + 1), ni = (unsigned)(jin_hi - t.j0 + 1);
     const bool need_prev = sweep > 0;
     if (tid == 0) {
 #pragma unroll
         for (int f = 0; f < NFIELD; f++) mbar_init(&bar[f], 1);
         fence_mbar_init();
-    }
-    __syncthreads();
-    // warp 0 puts every active field's tiles in flight at once
-    if (tid < 32) {
+        // every active field's tiles in flight at once: three tensor loads per field
+        // (x_k with halo, rhs, x_{k-1}); tensor x coordinate = column + 2, y = row, z = plane
+        const char* maps = b.tmaps + (size_t)t.c * 256;
+        const unsigned bytes = (JTW * JTH + TX * TYJ * (need_prev ? 2 : 1)) * sizeof(double);
         for (int f = 0; f < NFIELD; f++) {
             if (!(mask & (1 << f))) continue;
             const int pa = f < 2 ? P_US + f : P_T0 + 2 * (f - 2) + nxt;
-            const double* src = plane(b, c, to_scratch ? pa : P_BU + f);
-            const double* rhs = plane(b, c, P_RU + f);
-            const double* prv = plane(b, c, to_scratch ? P_BU + f : pa);
             double* sm = jsm + f * JT_FIELD;
-            if (tid == 0)
-                mbar_arrive_expect_tx(&bar[f], hrow * nh + irow * ni * (need_prev ? 2u : 1u));
-            __syncwarp();
-            for (int r = jlo + tid; r <= jhi; r += 32)
-                bulk_g2s(sm + (r - (t.j0 - 2)) * JTW, src + (long long)r * ld + c0, hrow, &bar[f]);
-            for (int r = t.j0 + tid; r <= jin_hi; r += 32) {
-                bulk_g2s(sm + JTW * JTH + (r - t.j0) * TX, rhs + (long long)r * ld + t.i0, irow, &bar[f]);
-                if (need_prev)
-                    bulk_g2s(sm + JTW * JTH + TX * TYJ + (r - t.j0) * TX, prv + (long long)r * ld + t.i0, irow,
-                             &bar[f]);
-            }
+            mbar_arrive_expect_tx(&bar[f], bytes);
+            tma_load_3d(sm, maps, t.i0, t.j0 - 2, to_scratch ? pa : P_BU + f, &bar[f]);
+            tma_load_3d(sm + JTW * JTH, maps + 128, t.i0 + 2, t.j0, P_RU + f, &bar[f]);
+            if (need_prev)
+                tma_load_3d(sm + JTW * JTH + TX * TYJ, maps + 128, t.i0 + 2, t.j0, to_scratch ? P_BU + f : pa,
+                            &bar[f]);
         }
     }
+    __syncthreads();
 
     const int li = tid % TX, lj = tid / TX;
     const int i = t.i0 + li;
@@ -811,6 +793,57 @@ __global__ void __launch_bounds__(NT) k_mg_smooth(BatchDev b, int l, int colour)
                     mplane(b, L, M_ANE)[k] * X[k + ld + 1] + mplane(b, L, M_ANW)[k] * X[k + ld - 1] +
                     mplane(b, L, M_ASE)[k] * X[k - ld + 1] + mplane(b, L, M_ASW)[k] * X[k - ld - 1];
     store_mirrored(X, ld, i, j, L.W, c.periodic, (mplane(b, L, M_B)[k] - s) / mplane(b, L, M_AP)[k]);
+}
+
+// One full multicolour Gauss-Seidel sweep per launch: the CTA keeps its tile of x plus a
+// one-cell halo in shared memory and sweeps the colours in order (reverse when `reverse`),
+// with a barrier between colours. Neighbouring tiles' values stay as they were at the start
+// of the sweep (block Gauss-Seidel at tile edges), so the smoother is a fixed linear map.
+// zero_init: the level's x is zero on entry (first smoothing after a restriction).
+__global__ void __launch_bounds__(NT) k_mg_smooth_blk(BatchDev b, int l, int reverse, int zero_init) {
+    __shared__ float xs[(TY + 2) * (TX + 2)];
+    const Tile t = b.mtiles[l][blockIdx.x];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const LevelDev& L = c.lev[l];
+    const int tid = threadIdx.x, li = tid % TX, lj = tid / TX;
+    const int i = t.i0 + li, j = t.j0 + lj;
+    const int ld = L.ld;
+    float* X = mplane(b, L, M_X);
+    constexpr int SW = TX + 2;
+    // load the tile + halo (rows j0-1 .. j0+TY, columns i0-1 .. i0+TX), clamped to the plane
+    for (int e = tid; e < (TY + 2) * SW; e += NT) {
+        const int r = e / SW, q = e % SW;
+        const int gj = t.j0 - 1 + r, gi = t.i0 - 1 + q;
+        float v = 0.0f;
+        if (!zero_init && gj >= 0 && gj < L.n1 && gi >= -H && gi < L.W + H) v = X[(long long)gj * ld + gi];
+        xs[e] = v;
+    }
+    const bool in = i >= L.ilo && i <= L.ihi && j <= L.n1 - 2;
+    float ap = 1.f, ae = 0.f, aw = 0.f, an = 0.f, as = 0.f, ane = 0.f, anw = 0.f, ase = 0.f, asw = 0.f, bv = 0.f;
+    int col = -1;
+    if (in) {
+        const long long k = (long long)j * ld + i;
+        ap = mplane(b, L, M_AP)[k]; ae = mplane(b, L, M_AE)[k]; aw = mplane(b, L, M_AW)[k];
+        an = mplane(b, L, M_AN)[k]; as = mplane(b, L, M_AS)[k]; ane = mplane(b, L, M_ANE)[k];
+        anw = mplane(b, L, M_ANW)[k]; ase = mplane(b, L, M_ASE)[k]; asw = mplane(b, L, M_ASW)[k];
+        bv = mplane(b, L, M_B)[k];
+        col = mg_colour(i, j, L.W, c.periodic);
+    }
+    __syncthreads();
+    const int ncol = (c.periodic && (L.W & 1)) ? 6 : 4;
+    const int o = (lj + 1) * SW + (li + 1);
+    for (int n = 0; n < ncol; n++) {
+        const int cc = reverse ? ncol - 1 - n : n;
+        if (col == cc) {
+            const float s = ae * xs[o + 1] + aw * xs[o - 1] + an * xs[o + SW] + as * xs[o - SW] +
+                            ane * xs[o + SW + 1] + anw * xs[o + SW - 1] + ase * xs[o - SW + 1] +
+                            asw * xs[o - SW - 1];
+            xs[o] = (bv - s) / ap;
+        }
+        __syncthreads();
+    }
+    if (in) store_mirrored(X, ld, i, j, L.W, c.periodic, xs[o]);
 }
 
 __global__ void __launch_bounds__(NT) k_mg_resid(BatchDev b, int l) {

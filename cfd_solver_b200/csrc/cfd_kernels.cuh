@@ -14,6 +14,7 @@ __global__ void k_spmv(BatchDev b, int mode);
 __global__ void k_bicg_s(BatchDev b);
 __global__ void k_bicg_x(BatchDev b, int maxit);
 __global__ void k_mg_smooth(BatchDev b, int l, int colour);
+__global__ void k_mg_smooth_blk(BatchDev b, int l, int reverse, int zero_init);
 __global__ void k_mg_resid(BatchDev b, int l);
 __global__ void k_mg_restrict(BatchDev b, int l);
 __global__ void k_mg_prolong(BatchDev b, int l);
