@@ -414,7 +414,8 @@ int one_step(cfd_batch* b) {
         Prof pr(b, K_RHS);
         k_rhs<<<nf, NT, 0, b->st>>>(bd);
     }
-    // momentum / energy solves: sweeps in pairs until every (case, field) stopped
+    // momentum / energy solves: sweeps in pairs until every (case, field) stopped; the
+    // counter is read every second pair (a finished case's CTAs leave at once)
     const int npairs = std::max(1, b->maxit_mom / 2);
     for (int pair = 0; pair < npairs; pair++) {
         {
@@ -425,10 +426,12 @@ int one_step(cfd_batch* b) {
             Prof pr(b, K_JAC);
             k_jac<<<bd.njtiles, NT, kJacSmem, b->st>>>(bd, 0, 2 * pair + 1, 1);
         }
-        int m = 0;
-        int rc = read_flag(b, 1, &m);
-        if (rc) return rc;
-        if (m <= 0) break;
+        if (pair % 2 == 1 || pair == npairs - 1) {
+            int m = 0;
+            int rc = read_flag(b, 1, &m);
+            if (rc) return rc;
+            if (m <= 0) break;
+        }
     }
     {
         Prof pr(b, K_UPBC);
@@ -438,18 +441,22 @@ int one_step(cfd_batch* b) {
         Prof pr(b, K_FACE_Q);
         k_face_q<<<nf, NT, 0, b->st>>>(bd);
     }
+    // pressure correction: the first iteration is launched without a check (a case whose
+    // q vanished is flagged done by k_face_q and its CTAs leave at once)
     for (int it = 0; it < b->maxit_p; it++) {
-        int a = 0;
-        int rc = read_flag(b, 0, &a);
-        if (rc) return rc;
-        if (a <= 0) break;
-        { Prof pr(b, K_BICG_P); k_bicg_p<<<nf, NT, 0, b->st>>>(bd); }
+        if (it > 0) {
+            int a = 0;
+            int rc = read_flag(b, 0, &a);
+            if (rc) return rc;
+            if (a <= 0) break;
+        }
+        { Prof pr(b, K_BICG_P); k_bicg_p<<<nf, NT, 0, b->st>>>(bd, it == 0); }
         run_vcycle(b);
         { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 0); }
         { Prof pr(b, K_BICG_S); k_bicg_s<<<nf, NT, 0, b->st>>>(bd); }
         run_vcycle(b);
         { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 1); }
-        { Prof pr(b, K_BICG_X); k_bicg_x<<<nf, NT, 0, b->st>>>(bd, b->maxit_p); }
+        { Prof pr(b, K_BICG_X); k_bicg_x<<<nf, NT, 0, b->st>>>(bd, b->maxit_p, it == 0); }
     }
     {
         Prof pr(b, K_CORRECT);

@@ -611,12 +611,10 @@ __global__ void __launch_bounds__(NT) k_face_q(BatchDev b) {
         double dvsde = (vs_jp - vs_jn) / d1;
         double qq = (X[k] * dusdxi) + (E[k] * dusde) + (Y[k] * dvsdxi) + (G[k] * dvsde);
         const double q = qq / dt;
+        // q doubles as BiCGStab's shadow residual r_hat; p, v and the iterate pcor are
+        // initialised by the first iteration's kernels (beta = 0, x = 0)
         plane(b, c, P_Q)[k] = q;
         plane(b, c, P_KR)[k] = q;
-        plane(b, c, P_KRH)[k] = q;
-        plane(b, c, P_KP)[k] = 0.0;
-        plane(b, c, P_KV)[k] = 0.0;
-        store_mirrored(plane(b, c, P_PCOR), ld, i, j, c.W, c.periodic, 0.0);
         red[0] = fabs(q);
         red[1] = q * q;
         red[2] = fabs(q);
@@ -648,7 +646,7 @@ __global__ void __launch_bounds__(NT) k_face_q(BatchDev b) {
 
 // ---------------------------------------------------------------------------
 // BiCGStab, right-preconditioned, FP64 vectors; per-case scalars live on the device
-__global__ void __launch_bounds__(NT) k_bicg_p(BatchDev b) {
+__global__ void __launch_bounds__(NT) k_bicg_p(BatchDev b, int first) {
     const Tile t = b.ftiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
@@ -658,7 +656,8 @@ __global__ void __launch_bounds__(NT) k_bicg_p(BatchDev b) {
     const double beta = sc[S_BETA], omega = sc[S_OMEGA];
     const long long k = (long long)j * c.ld + i;
     double* Pv = plane(b, c, P_KP);
-    const double p = plane(b, c, P_KR)[k] + beta * (Pv[k] - omega * plane(b, c, P_KV)[k]);
+    const double r = plane(b, c, P_KR)[k];
+    const double p = first ? r : r + beta * (Pv[k] - omega * plane(b, c, P_KV)[k]);
     Pv[k] = p;
     const LevelDev& L = c.lev[0];
     const long long k0 = (long long)j * L.ld + i;
@@ -689,7 +688,7 @@ __global__ void __launch_bounds__(NT) k_spmv(BatchDev b, int mode) {
         if (mode == 0) {
             plane(b, c, P_KPH)[k] = xc;
             plane(b, c, P_KV)[k] = y;
-            red[0] = plane(b, c, P_KRH)[k] * y;
+            red[0] = plane(b, c, P_Q)[k] * y;
         } else {
             plane(b, c, P_KSH)[k] = xc;
             plane(b, c, P_KT)[k] = y;
@@ -729,7 +728,7 @@ __global__ void __launch_bounds__(NT) k_bicg_s(BatchDev b) {
     store_mirrored(mplane(b, L, M_X), L.ld, i, j, L.W, c.periodic, 0.0f);
 }
 
-__global__ void __launch_bounds__(NT) k_bicg_x(BatchDev b, int maxit) {
+__global__ void __launch_bounds__(NT) k_bicg_x(BatchDev b, int maxit, int first) {
     const Tile t = b.ftiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
@@ -741,11 +740,11 @@ __global__ void __launch_bounds__(NT) k_bicg_x(BatchDev b, int maxit) {
         const int ld = c.ld;
         const long long k = (long long)j * ld + i;
         double* X = plane(b, c, P_PCOR);
-        const double x = X[k] + alpha * plane(b, c, P_KPH)[k] + omega * plane(b, c, P_KSH)[k];
+        const double x = (first ? 0.0 : X[k]) + alpha * plane(b, c, P_KPH)[k] + omega * plane(b, c, P_KSH)[k];
         store_mirrored(X, ld, i, j, c.W, c.periodic, x);
         const double r = plane(b, c, P_KS)[k] - omega * plane(b, c, P_KT)[k];
         plane(b, c, P_KR)[k] = r;
-        red[0] = plane(b, c, P_KRH)[k] * r;
+        red[0] = plane(b, c, P_Q)[k] * r;
         red[1] = fabs(r);
     }
     if (case_reduce<2, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0) {
@@ -1002,37 +1001,43 @@ __global__ void __launch_bounds__(NT) k_correct(BatchDev b) {
     const Tile t = b.ftiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    // no pressure iteration ran (q vanished or broke down at once): pcor = 0
+    const bool none = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
     double red[1] = {0.0};
     if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
         const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
         const bool cav = c.profile == CAVITY;
         double* PC = plane(b, c, P_PCOR);
-        const long long k = (long long)j * ld + i;
-        const double pc = PC[k];
-        // pcor on the boundary after its conditions: wall copy, far field 0 / copy at inflow
-        double far = 0.0;
-        if (!cav && j == n1 - 2) {
-            const double* VEC = plane(b, c, P_VEC);
-            const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
-            if (vnn >= 0) far = pc;
-        }
-        const double pN = (j == n1 - 2) ? (cav ? pc : far) : PC[k + ld];
-        const double pS = (j == 1) ? pc : PC[k - ld];
-        const double pE = (cav && i == n0 - 2) ? pc : PC[k + 1];
-        const double pW = (cav && i == 1) ? pc : PC[k - 1];
-        const double d0 = c.d0, d1 = c.d1, dt = c.dt;
-        const double dpcor_dxi = 0.5 * (pE - pW) / d0;
-        const double dpcor_de = 0.5 * (pN - pS) / d1;
         double* U = plane(b, c, P_U);
         double* V = plane(b, c, P_V);
         double* P = plane(b, c, P_P);
-        const double un = plane(b, c, P_US)[k] - dt * (plane(b, c, P_XIX)[k] * dpcor_dxi + plane(b, c, P_ETX)[k] * dpcor_de);
-        const double vn = plane(b, c, P_VS)[k] - dt * (plane(b, c, P_XIY)[k] * dpcor_dxi + plane(b, c, P_ETY)[k] * dpcor_de);
-        red[0] = fabs(un - U[k]) + fabs(vn - V[k]);
+        const long long k = (long long)j * ld + i;
+        // every load first (independent), the boundary conditions as selects afterwards
+        const double pc0 = PC[k], pn0 = PC[k + ld], ps0 = PC[k - ld], pe0 = PC[k + 1], pw0 = PC[k - 1];
+        const double us = plane(b, c, P_US)[k], vs = plane(b, c, P_VS)[k];
+        const double xix = plane(b, c, P_XIX)[k], etx = plane(b, c, P_ETX)[k];
+        const double xiy = plane(b, c, P_XIY)[k], ety = plane(b, c, P_ETY)[k];
+        const double u0 = U[k], v0 = V[k], p0 = P[k];
+        const double* VEC = plane(b, c, P_VEC);
+        const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
+        const double pc = none ? 0.0 : pc0;
+        // pcor on the boundary after its conditions: wall copy, far field 0 / copy at inflow
+        const double far = (!cav && vnn >= 0) ? pc : 0.0;
+        const double pN = none ? 0.0 : (j == n1 - 2) ? (cav ? pc : far) : pn0;
+        const double pS = none ? 0.0 : (j == 1) ? pc : ps0;
+        const double pE = none ? 0.0 : (cav && i == n0 - 2) ? pc : pe0;
+        const double pW = none ? 0.0 : (cav && i == 1) ? pc : pw0;
+        const double d0 = c.d0, d1 = c.d1, dt = c.dt;
+        const double dpcor_dxi = 0.5 * (pE - pW) / d0;
+        const double dpcor_de = 0.5 * (pN - pS) / d1;
+        const double un = us - dt * (xix * dpcor_dxi + etx * dpcor_de);
+        const double vn = vs - dt * (xiy * dpcor_dxi + ety * dpcor_de);
+        red[0] = fabs(un - u0) + fabs(vn - v0);
         store_mirrored(U, ld, i, j, W, per, un);
         store_mirrored(V, ld, i, j, W, per, vn);
-        const double pn = (c.omega_p == 1.0) ? P[k] + pc : P[k] + c.omega_p * pc;
+        const double pn = (c.omega_p == 1.0) ? p0 + pc : p0 + c.omega_p * pc;
         store_mirrored(P, ld, i, j, W, per, pn);
+        if (none) store_mirrored(PC, ld, i, j, W, per, 0.0);
         // record the boundary pcor (output only)
         if (j == 1) store_mirrored(PC, ld, i, 0, W, per, pc);
         if (j == n1 - 2) store_mirrored(PC, ld, i, n1 - 1, W, per, cav ? pc : far);
