@@ -412,7 +412,7 @@ int one_step(cfd_batch* b) {
     CK(cudaMemsetAsync(b->flags, 0, 2 * sizeof(int), b->st));
     {
         Prof pr(b, K_RHS);
-        k_rhs<<<nf, NT, 0, b->st>>>(bd);
+        k_rhs<<<bd.njtiles, NT, kRhsSmem, b->st>>>(bd);
     }
     // momentum / energy solves: sweeps in pairs until every (case, field) stopped; the
     // counter is read every second pair (a finished case's CTAs leave at once)
@@ -439,7 +439,7 @@ int one_step(cfd_batch* b) {
     }
     {
         Prof pr(b, K_FACE_Q);
-        k_face_q<<<nf, NT, 0, b->st>>>(bd);
+        k_face_q<<<bd.njtiles, NT, kFaceQSmem, b->st>>>(bd);
     }
     // pressure correction: the first iteration is launched without a check (a case whose
     // q vanished is flagged done by k_face_q and its CTAs leave at once)
@@ -696,6 +696,8 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         if (smem > 48 * 1024)
             CK(cudaFuncSetAttribute(k_bc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         CK(cudaFuncSetAttribute(k_jac, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacSmem));
+        CK(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem));
+        CK(cudaFuncSetAttribute(k_face_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFaceQSmem));
     }
 
     // ---- tile tables

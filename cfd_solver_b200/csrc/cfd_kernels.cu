@@ -26,6 +26,9 @@ namespace cfd {
 
 #define AT(ptr, ii, jj) (ptr)[(long long)(jj) * ld + (ii)]
 
+constexpr int JTW = TX + 4;   // 32 x 16 tile columns incl. a 2-cell halo
+constexpr int JTH = TYJ + 4;  // 32 x 16 tile rows incl. a 2-cell halo
+
 __device__ __forceinline__ bool near_wall(const CaseDev& c, int i, int j) {
     if (j == 1 || j == c.n1 - 2) return true;
     return c.profile == CAVITY && (i == 1 || i == c.n0 - 2);
@@ -173,167 +176,193 @@ __device__ __forceinline__ double offsum(const double* F, long long k, int ld, c
 
 // ---------------------------------------------------------------------------
 // contravariant velocities + convection + the five right-hand sides
-// (PSolver.cpp:1063-1237); also seeds the five solves' iterates
-__global__ void __launch_bounds__(NT) k_rhs(BatchDev b) {
-    const Tile t = b.ftiles[blockIdx.x];
-    const CaseDev& c = b.cases[t.c];
-    if (t.k == 0 && threadIdx.x == 0) {
-        int* is = b.iscal + (long long)t.c * NISCAL;
-        for (int f = 0; f < NFIELD; f++) { is[I_MDONE0 + f] = 0; is[I_MIT0 + f] = 0; }
-        atomicAdd(b.mactive, NFIELD);
+// (PSolver.cpp:1063-1237); also seeds the five solves' iterates. A CTA owns a 32 x 16 tile
+// (two cells per thread); u, v, T, p, up, vp with a 2-cell halo and the seven metric
+// planes of the tile arrive by tensor TMA into shared memory.
+constexpr int RHS_HALO = 6, RHS_INT = 7;
+constexpr size_t RHS_SMEM = (size_t)(RHS_HALO * JTW * JTH + RHS_INT * TX * TYJ) * sizeof(double) + 128;
+const size_t kRhsSmem = RHS_SMEM;
+
+__device__ __forceinline__ double conv_one(const double* F, int o, bool near_i, bool near_j, double ux,
+                                           double ue, double pec1, double pec2, double d0, double d1) {
+    constexpr int R = JTW;
+    const double fc = F[o], fe = F[o + 1], fw = F[o - 1];
+    double du_xi, du_et;
+    if (near_i) {
+        du_xi = 0.5 * (fe - fw) / d0;
+    } else {
+        const double fee = F[o + 2], fww = F[o - 2];
+        if (near_j || (pec1 <= 2 && pec1 > -2)) {
+            double xpp = 8.0 * (fe - fw);
+            double xnn = fee - fww;
+            du_xi = (1.0 / 12.0) * (xpp - xnn) / d0;
+        } else {
+            double ak1 = ux * (-fee + 8 * fe - 8 * fw + fww) / (12.0 * d0);
+            double ak2 = fabs(ux) * (fee - 4 * fe + 6 * fc - 4 * fw + fww) / (4.0 * d0);
+            ak1 = ak1 + ak2;
+            du_xi = ak1 / ux;
+        }
     }
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
-    if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
-    const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
+    const double fn = F[o + R], fs = F[o - R];
+    if (near_j) {
+        du_et = 0.5 * (fn - fs) / d1;
+    } else {
+        const double fnn = F[o + 2 * R], fss = F[o - 2 * R];
+        if (near_i || (pec2 <= 2 && pec2 > -2)) {
+            double ypp = 8.0 * (fn - fs);
+            double ynn = fnn - fss;
+            du_et = (1.0 / 12.0) * (ypp - ynn) / d1;
+        } else {
+            double ak3 = ue * (-fnn + 8 * fn - 8 * fs + fss) / (12.0 * d1);
+            double ak4 = fabs(ue) * (fnn - 4 * fn + 6 * fc - 4 * fs + fss) / (4.0 * d1);
+            ak3 = ak3 + ak4;
+            du_et = ak3 / ue;
+        }
+    }
+    return ux * du_xi + ue * du_et;
+}
+
+__global__ void __launch_bounds__(NT, 2) k_rhs(BatchDev b) {
+    extern __shared__ __align__(128) unsigned char rraw[];
+    __shared__ __align__(8) uint64_t bar;
+    double* sm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(rraw) + 127) & ~uintptr_t(127));
+    const Tile t = b.jtiles[blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    const int tid = threadIdx.x;
     const int cur = b.cur, nxt = cur ^ 1;
+    // halo tiles: u, v, T, p, up, vp; interior tiles: xix, xiy, etx, ety, alpha, gamma, beta
+    double* SI = sm + RHS_HALO * JTW * JTH;
+    if (tid == 0) {
+        if (t.k == 0) {
+            int* is = b.iscal + (long long)t.c * NISCAL;
+            for (int f = 0; f < NFIELD; f++) { is[I_MDONE0 + f] = 0; is[I_MIT0 + f] = 0; }
+            atomicAdd(b.mactive, NFIELD);
+        }
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        const char* maps = b.tmaps + (size_t)t.c * 256;
+        mbar_arrive_expect_tx(&bar, (RHS_HALO * JTW * JTH + RHS_INT * TX * TYJ) * sizeof(double));
+        const int hp[RHS_HALO] = {P_U, P_V, P_T0 + cur, P_P, P_UP0 + cur, P_VP0 + cur};
+        const int ip[RHS_INT] = {P_XIX, P_XIY, P_ETX, P_ETY, P_ALPH, P_GAM, P_BETA};
+        for (int m = 0; m < RHS_HALO; m++) tma_load_3d(sm + m * JTW * JTH, maps, t.i0, t.j0 - 2, hp[m], &bar);
+        for (int m = 0; m < RHS_INT; m++) tma_load_3d(SI + m * TX * TYJ, maps + 128, t.i0 + 2, t.j0, ip[m], &bar);
+    }
+    __syncthreads();
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0));
+    if (!ok) {
+        if (tid == 0) atomicExch(b.error, 1);
+        return;
+    }
+    const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
     const bool cav = c.profile == CAVITY;
     const double d0 = c.d0, d1 = c.d1, dt = c.dt, Re = c.Re, Pr = c.Pr, Ri = c.Ri;
+    const double *Us = sm, *Vs = sm + JTW * JTH, *Ts = sm + 2 * JTW * JTH, *Ps = sm + 3 * JTW * JTH,
+                 *UPs = sm + 4 * JTW * JTH, *VPs = sm + 5 * JTW * JTH;
     const double* U = plane(b, c, P_U);
     const double* V = plane(b, c, P_V);
     const double* T = plane(b, c, P_T0 + cur);
     const double* UP = plane(b, c, P_UP0 + cur);
     const double* VP = plane(b, c, P_VP0 + cur);
-    const double* P = plane(b, c, P_P);
-    const double* XIX = plane(b, c, P_XIX);
-    const double* XIY = plane(b, c, P_XIY);
-    const double* ETX = plane(b, c, P_ETX);
-    const double* ETY = plane(b, c, P_ETY);
-    const long long k = (long long)j * ld + i;
-    const double al = plane(b, c, P_ALPH)[k], ga = plane(b, c, P_GAM)[k];
-    const double ux = XIX[k] * U[k] + XIY[k] * V[k];
-    const double ue = ETX[k] * U[k] + ETY[k] * V[k];
-    const bool near_j = (j == 1 || j == n1 - 2);
-    const bool near_i = cav && (i == 1 || i == n0 - 2);
-    const double* Fs[3] = {U, V, T};
-    double conv[3];
-#pragma unroll
-    for (int m = 0; m < 3; m++) {
-        const double* F = Fs[m];
-        double pec1, pec2;
-        if (m <= 1) {
-            pec1 = ux * Re * d0 / al;
-            pec2 = ue * Re * d1 / ga;
-        } else {
-            pec1 = ux * Re * Pr * d0 / al;
-            pec2 = ue * Re * Pr * d1 / ga;
-        }
-        const double fc = F[k], fe = F[k + 1], fw = F[k - 1];
-        double du_xi, du_et;
-        if (near_i) {
-            du_xi = 0.5 * (fe - fw) / d0;
-        } else {
-            const double fee = F[k + 2], fww = F[k - 2];
-            if (near_j || (pec1 <= 2 && pec1 > -2)) {
-                double xpp = 8.0 * (fe - fw);
-                double xnn = fee - fww;
-                du_xi = (1.0 / 12.0) * (xpp - xnn) / d0;
-            } else {
-                double ak1 = ux * (-fee + 8 * fe - 8 * fw + fww) / (12.0 * d0);
-                double ak2 = fabs(ux) * (fee - 4 * fe + 6 * fc - 4 * fw + fww) / (4.0 * d0);
-                ak1 = ak1 + ak2;
-                du_xi = ak1 / ux;
-            }
-        }
-        const double fn = F[k + ld], fs = F[k - ld];
-        if (near_j) {
-            du_et = 0.5 * (fn - fs) / d1;
-        } else {
-            const double fnn = F[k + 2LL * ld], fss = F[k - 2LL * ld];
-            if (near_i || (pec2 <= 2 && pec2 > -2)) {
-                double ypp = 8.0 * (fn - fs);
-                double ynn = fnn - fss;
-                du_et = (1.0 / 12.0) * (ypp - ynn) / d1;
-            } else {
-                double ak3 = ue * (-fnn + 8 * fn - 8 * fs + fss) / (12.0 * d1);
-                double ak4 = fabs(ue) * (fnn - 4 * fn + 6 * fc - 4 * fs + fss) / (4.0 * d1);
-                ak3 = ak3 + ak4;
-                du_et = ak3 / ue;
-            }
-        }
-        conv[m] = ux * du_xi + ue * du_et;
-    }
-    const double dp_dxi = (P[k + 1] - P[k - 1]) / (2.0 * d0);
-    const double dp_de = (P[k + ld] - P[k - ld]) / (2.0 * d1);
-    const double dp_dx = XIX[k] * dp_dxi + ETX[k] * dp_de;
-    const double dp_dy = XIY[k] * dp_dxi + ETY[k] * dp_de;
-    double qu = dt * (-conv[0] - dp_dx) + U[k];
-    double qv = dt * (-conv[1] - dp_dy + Ri * T[k]) + V[k];
-    double qt = -dt * conv[2] + T[k];
-    double qup = qu + dt * dp_dx;
-    double qvp = qv + dt * dp_dy;
-    if (!cav && near_j) {
-        // folded wall-row couplings (PSolver.cpp:1195-1227)
-        const double be = plane(b, c, P_BETA)[k];
-        const double bs = -dt * (ga / (d1 * d1)) / Re;
-        const double bpos = dt * be / (2.0 * d0 * d1 * Re);
-        const double bneg = -dt * be / (2.0 * d0 * d1 * Re);
-        const double ts = -dt * (ga / (d1 * d1)) / (Re * Pr);
-        const double tpos = dt * (be / (2.0 * d0 * d1)) / (Re * Pr);
-        const double tneg = -dt * (be / (2.0 * d0 * d1)) / (Re * Pr);
-        long long s0, s1, s2;
-        double c1, c2, t1, t2;
-        if (j == 1) {  // bus, buse (= ause), busw (= ausw)
-            s0 = k - ld; s1 = k - ld + 1; s2 = k - ld - 1;
-            c1 = bneg; c2 = bpos; t1 = tneg; t2 = tpos;
-        } else {       // bun, bune (= aune), bunw (= aunw)
-            s0 = k + ld; s1 = k + ld + 1; s2 = k + ld - 1;
-            c1 = bpos; c2 = bneg; t1 = tpos; t2 = tneg;
-        }
-        double sumu = bs * U[s0] + c1 * U[s1] + c2 * U[s2];
-        qu = qu - sumu;
-        double sumv = bs * V[s0] + c1 * V[s1] + c2 * V[s2];
-        qv = qv - sumv;
-        double sumt = ts * T[s0] + t1 * T[s1] + t2 * T[s2];
-        qt = qt - sumt;
-        sumu = bs * UP[s0] + c1 * UP[s1] + c2 * UP[s2];
-        qup = qup - sumu;
-        sumv = bs * VP[s0] + c1 * VP[s1] + c2 * VP[s2];
-        qvp = qvp - sumv;
-    }
-    plane(b, c, P_RU)[k] = qu;
-    plane(b, c, P_RV)[k] = qv;
-    plane(b, c, P_RT)[k] = qt;
-    plane(b, c, P_RUP)[k] = qup;
-    plane(b, c, P_RVP)[k] = qvp;
-
-    // seed the iterates (PSolver.cpp:1241-1337): u*, v*, T from the current
-    // fields; up/vp from the previous solution (warm start) or zero
-    double* A[NFIELD] = {plane(b, c, P_US), plane(b, c, P_VS), plane(b, c, P_T0 + nxt),
-                         plane(b, c, P_UP0 + nxt), plane(b, c, P_VP0 + nxt)};
-    double* B[NFIELD] = {plane(b, c, P_BU), plane(b, c, P_BV), plane(b, c, P_BT),
-                         plane(b, c, P_BUP), plane(b, c, P_BVP)};
+    // iterate buffers of field f: A (the solution) and B (the Jacobi scratch)
+    auto Ap = [&](int f) { return plane(b, c, f < 2 ? P_US + f : P_T0 + 2 * (f - 2) + nxt); };
+    auto Bp = [&](int f) { return plane(b, c, P_BU + f); };
     const bool warm = c.warm_up != 0;
-    store_mirrored(A[F_U], ld, i, j, W, per, U[k]);
-    store_mirrored(A[F_V], ld, i, j, W, per, V[k]);
-    store_mirrored(A[F_T], ld, i, j, W, per, T[k]);
-    store_mirrored(A[F_UP], ld, i, j, W, per, warm ? UP[k] : 0.0);
-    store_mirrored(A[F_VP], ld, i, j, W, per, warm ? VP[k] : 0.0);
-    // boundary values the stencils read (both iterate buffers)
-    auto put_bnd = [&](int bi, int bj) {
-        const long long kb = (long long)bj * ld + bi;
-        double vals[NFIELD] = {U[kb], V[kb], T[kb], UP[kb], VP[kb]};
-        if (!cav && bj == n1 - 1) {  // the up/vp solves see zero on the far-field row
-            vals[F_UP] = 0.0;
-            vals[F_VP] = 0.0;
+    const int li = tid % TX, lj = tid / TX;
+    const int i = t.i0 + li;
+#pragma unroll 1
+    for (int h = 0; h < 2; h++) {
+        const int j = t.j0 + lj + h * TY;
+        if (i < c.ilo || i > c.ihi || j > n1 - 2) continue;
+        const int o = (lj + h * TY + 2) * JTW + (li + 2);
+        const int oi = (lj + h * TY) * TX + li;
+        const long long k = (long long)j * ld + i;
+        const double xix = SI[oi], xiy = SI[TX * TYJ + oi], etx = SI[2 * TX * TYJ + oi], ety = SI[3 * TX * TYJ + oi];
+        const double al = SI[4 * TX * TYJ + oi], ga = SI[5 * TX * TYJ + oi];
+        const double uc = Us[o], vc = Vs[o], tc = Ts[o];
+        const double ux = xix * uc + xiy * vc;
+        const double ue = etx * uc + ety * vc;
+        const bool near_j = (j == 1 || j == n1 - 2);
+        const bool near_i = cav && (i == 1 || i == n0 - 2);
+        const double pu1 = ux * Re * d0 / al, pu2 = ue * Re * d1 / ga;
+        const double pt1 = ux * Re * Pr * d0 / al, pt2 = ue * Re * Pr * d1 / ga;
+        const double cv0 = conv_one(Us, o, near_i, near_j, ux, ue, pu1, pu2, d0, d1);
+        const double cv1 = conv_one(Vs, o, near_i, near_j, ux, ue, pu1, pu2, d0, d1);
+        const double cv2 = conv_one(Ts, o, near_i, near_j, ux, ue, pt1, pt2, d0, d1);
+        const double dp_dxi = (Ps[o + 1] - Ps[o - 1]) / (2.0 * d0);
+        const double dp_de = (Ps[o + JTW] - Ps[o - JTW]) / (2.0 * d1);
+        const double dp_dx = xix * dp_dxi + etx * dp_de;
+        const double dp_dy = xiy * dp_dxi + ety * dp_de;
+        double qu = dt * (-cv0 - dp_dx) + uc;
+        double qv = dt * (-cv1 - dp_dy + Ri * tc) + vc;
+        double qt = -dt * cv2 + tc;
+        double qup = qu + dt * dp_dx;
+        double qvp = qv + dt * dp_dy;
+        if (!cav && near_j) {
+            // folded wall-row couplings (PSolver.cpp:1195-1227)
+            const double be = SI[6 * TX * TYJ + oi];
+            const double bs = -dt * (ga / (d1 * d1)) / Re;
+            const double bpos = dt * be / (2.0 * d0 * d1 * Re);
+            const double bneg = -dt * be / (2.0 * d0 * d1 * Re);
+            const double ts = -dt * (ga / (d1 * d1)) / (Re * Pr);
+            const double tpos = dt * (be / (2.0 * d0 * d1)) / (Re * Pr);
+            const double tneg = -dt * (be / (2.0 * d0 * d1)) / (Re * Pr);
+            int s0, s1, s2;
+            double c1, c2, t1, t2;
+            if (j == 1) {  // bus, buse (= ause), busw (= ausw)
+                s0 = o - JTW; s1 = o - JTW + 1; s2 = o - JTW - 1;
+                c1 = bneg; c2 = bpos; t1 = tneg; t2 = tpos;
+            } else {       // bun, bune (= aune), bunw (= aunw)
+                s0 = o + JTW; s1 = o + JTW + 1; s2 = o + JTW - 1;
+                c1 = bpos; c2 = bneg; t1 = tpos; t2 = tneg;
+            }
+            double sumu = bs * Us[s0] + c1 * Us[s1] + c2 * Us[s2];
+            qu = qu - sumu;
+            double sumv = bs * Vs[s0] + c1 * Vs[s1] + c2 * Vs[s2];
+            qv = qv - sumv;
+            double sumt = ts * Ts[s0] + t1 * Ts[s1] + t2 * Ts[s2];
+            qt = qt - sumt;
+            sumu = bs * UPs[s0] + c1 * UPs[s1] + c2 * UPs[s2];
+            qup = qup - sumu;
+            sumv = bs * VPs[s0] + c1 * VPs[s1] + c2 * VPs[s2];
+            qvp = qvp - sumv;
         }
-#pragma unroll
-        for (int f = 0; f < NFIELD; f++) {
-            store_mirrored(A[f], ld, bi, bj, W, per, vals[f]);
-            store_mirrored(B[f], ld, bi, bj, W, per, vals[f]);
-        }
-    };
-    if (j == 1) put_bnd(i, 0);
-    if (j == n1 - 2) put_bnd(i, n1 - 1);
-    if (cav) {
-        if (i == 1) {
-            put_bnd(0, j);
-            if (j == 1) put_bnd(0, 0);
-            if (j == n1 - 2) put_bnd(0, n1 - 1);
-        }
-        if (i == n0 - 2) {
-            put_bnd(n0 - 1, j);
-            if (j == 1) put_bnd(n0 - 1, 0);
-            if (j == n1 - 2) put_bnd(n0 - 1, n1 - 1);
+        plane(b, c, P_RU)[k] = qu;
+        plane(b, c, P_RV)[k] = qv;
+        plane(b, c, P_RT)[k] = qt;
+        plane(b, c, P_RUP)[k] = qup;
+        plane(b, c, P_RVP)[k] = qvp;
+        // seed the iterates (PSolver.cpp:1241-1337): u*, v*, T from the current fields;
+        // up/vp from the previous solution (warm start) or zero
+        store_mirrored(Ap(F_U), ld, i, j, W, per, uc);
+        store_mirrored(Ap(F_V), ld, i, j, W, per, vc);
+        store_mirrored(Ap(F_T), ld, i, j, W, per, tc);
+        store_mirrored(Ap(F_UP), ld, i, j, W, per, warm ? UPs[o] : 0.0);
+        store_mirrored(Ap(F_VP), ld, i, j, W, per, warm ? VPs[o] : 0.0);
+        // boundary values the stencils read (both iterate buffers)
+        auto put_bnd = [&](int bi, int bj) {
+            const long long kb = (long long)bj * ld + bi;
+            const bool zero_far = !cav && bj == n1 - 1;  // up/vp solves see zero on the far row
+#pragma unroll 1
+            for (int f = 0; f < NFIELD; f++) {
+                const double* src = f == F_U ? U : f == F_V ? V : f == F_T ? T : f == F_UP ? UP : VP;
+                const double val = (zero_far && f >= F_UP) ? 0.0 : src[kb];
+                store_mirrored(Ap(f), ld, bi, bj, W, per, val);
+                store_mirrored(Bp(f), ld, bi, bj, W, per, val);
+            }
+        };
+        if (j == 1) put_bnd(i, 0);
+        if (j == n1 - 2) put_bnd(i, n1 - 1);
+        if (cav) {
+            if (i == 1) {
+                put_bnd(0, j);
+                if (j == 1) put_bnd(0, 0);
+                if (j == n1 - 2) put_bnd(0, n1 - 1);
+            }
+            if (i == n0 - 2) {
+                put_bnd(n0 - 1, j);
+                if (j == 1) put_bnd(n0 - 1, 0);
+                if (j == n1 - 2) put_bnd(n0 - 1, n1 - 1);
+            }
         }
     }
 }
@@ -355,8 +384,6 @@ __global__ void __launch_bounds__(NT) k_rhs(BatchDev b) {
 // (one per row, completed on an mbarrier), double-buffered so the next field's tile
 // streams in while this one is swept. The 25-point operator has 10 distinct
 // coefficients (PSolver.cpp:791-848), built in registers from alpha, beta, gamma.
-constexpr int JTW = TX + 4;   // tile columns incl. halo
-constexpr int JTH = TYJ + 4;  // tile rows incl. halo
 
 // Per cell the operator is fixed by E = dt alpha/(Re dxi0^2), G = dt gamma/(Re dxi1^2) and
 // B = dt beta/(Re dxi0 dxi1): 4th-order rows (PSolver.cpp:791-821) have
@@ -571,24 +598,43 @@ __global__ void __launch_bounds__(BC_THREADS) k_upbc(BatchDev b) {
 
 // ---------------------------------------------------------------------------
 // face velocities -> continuity source q (PSolver.cpp:1390-1449) with the
-// mass-residual reductions; seeds the BiCGStab vectors (pcor starts at 0)
-__global__ void __launch_bounds__(NT) k_face_q(BatchDev b) {
-    const Tile t = b.ftiles[blockIdx.x];
+// mass-residual reductions; seeds the BiCGStab residual. 32 x 16 tiles, two cells per
+// thread; p, up, vp and the four metric planes with their halo arrive by tensor TMA.
+constexpr int FQ_HALO = 7;
+constexpr size_t FQ_SMEM = (size_t)FQ_HALO * JTW * JTH * sizeof(double) + 128;
+const size_t kFaceQSmem = FQ_SMEM;
+
+__global__ void __launch_bounds__(NT, 3) k_face_q(BatchDev b) {
+    extern __shared__ __align__(128) unsigned char fraw[];
+    __shared__ __align__(8) uint64_t bar;
+    double* sm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(fraw) + 127) & ~uintptr_t(127));
+    const Tile t = b.jtiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    const int tid = threadIdx.x;
+    const int nxt = b.cur ^ 1;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        const char* maps = b.tmaps + (size_t)t.c * 256;
+        mbar_arrive_expect_tx(&bar, FQ_HALO * JTW * JTH * sizeof(double));
+        const int hp[FQ_HALO] = {P_P, P_UP0 + nxt, P_VP0 + nxt, P_XIX, P_XIY, P_ETX, P_ETY};
+        for (int m = 0; m < FQ_HALO; m++) tma_load_3d(sm + m * JTW * JTH, maps, t.i0, t.j0 - 2, hp[m], &bar);
+    }
+    __syncthreads();
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0));
+    if (!ok && tid == 0) atomicExch(b.error, 1);
+    const double *P = sm, *U = sm + JTW * JTH, *V = sm + 2 * JTW * JTH, *X = sm + 3 * JTW * JTH,
+                 *Y = sm + 4 * JTW * JTH, *E = sm + 5 * JTW * JTH, *G = sm + 6 * JTW * JTH;
     const int ld = c.ld;
+    const double d0 = c.d0, d1 = c.d1, dt = c.dt;
+    const int li = tid % TX, lj = tid / TX;
+    const int i = t.i0 + li;
     double red[3] = {0.0, 0.0, 0.0};
-    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
-        const int nxt = b.cur ^ 1;
-        const double d0 = c.d0, d1 = c.d1, dt = c.dt;
-        const double* P = plane(b, c, P_P);
-        const double* U = plane(b, c, P_UP0 + nxt);
-        const double* V = plane(b, c, P_VP0 + nxt);
-        const double* X = plane(b, c, P_XIX);
-        const double* Y = plane(b, c, P_XIY);
-        const double* E = plane(b, c, P_ETX);
-        const double* G = plane(b, c, P_ETY);
-        const long long k = (long long)j * ld + i, kE = k + 1, kW = k - 1, kN = k + ld, kS = k - ld;
+    for (int h = 0; h < 2; h++) {
+        const int j = t.j0 + lj + h * TY;
+        if (!ok || i < c.ilo || i > c.ihi || j > c.n1 - 2) continue;
+        const int k = (lj + h * TY + 2) * JTW + (li + 2);
+        const int kE = k + 1, kW = k - 1, kN = k + JTW, kS = k - JTW;
         double dpdxi_ip = (P[kE] - P[k]) / d0;
         double dpde_ip = (P[kN + 1] + P[kN] - P[kS] - P[kS + 1]) / (4.0 * d1);
         double dpdxi_in = (P[k] - P[kW]) / d0;
@@ -613,14 +659,14 @@ __global__ void __launch_bounds__(NT) k_face_q(BatchDev b) {
         const double q = qq / dt;
         // q doubles as BiCGStab's shadow residual r_hat; p, v and the iterate pcor are
         // initialised by the first iteration's kernels (beta = 0, x = 0)
-        plane(b, c, P_Q)[k] = q;
-        plane(b, c, P_KR)[k] = q;
-        red[0] = fabs(q);
-        red[1] = q * q;
-        red[2] = fabs(q);
+        const long long kg = (long long)j * ld + i;
+        plane(b, c, P_Q)[kg] = q;
+        plane(b, c, P_KR)[kg] = q;
+        red[0] += fabs(q);
+        red[1] += q * q;
+        red[2] = fmax(red[2], fabs(q));
     }
-    if (case_reduce<3, 0x4u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) &&
-        threadIdx.x == 0) {
+    if (case_reduce<3, 0x4u>(b, t.c, blockIdx.x, c.jt_begin, c.jt_count, red) && tid == 0) {
         double* sc = b.scal + (long long)t.c * NSCAL;
         int* is = b.iscal + (long long)t.c * NISCAL;
         sc[S_QL1] = red[0];

@@ -7,6 +7,8 @@ __global__ void k_assemble_p(BatchDev b);
 __global__ void k_rhs(BatchDev b);
 __global__ void k_jac(BatchDev b, int to_scratch, int sweep, int decide);
 extern const size_t kJacSmem;  // dynamic shared memory of k_jac
+extern const size_t kRhsSmem;
+extern const size_t kFaceQSmem;
 __global__ void k_upbc(BatchDev b);
 __global__ void k_face_q(BatchDev b);
 __global__ void k_bicg_p(BatchDev b, int first);
