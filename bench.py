@@ -251,9 +251,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     clocks.mark_start()
-    b.profile(True)
     launches0 = b.launches()
-    work0 = b.work()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
@@ -267,6 +265,15 @@ def main():
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     launches = b.launches() - launches0
+
+    # roofline pass: the same steps again with a CUDA event pair around every launch on the
+    # library's stream (host-driven loops instead of the step graph)
+    prof_steps = max(3, min(args.steps, 10))
+    b.profile(True)
+    work0 = b.work()
+    for _ in range(prof_steps):
+        b.step(1)
+    b.sync()
     work1 = b.work()
     kt = b.kernel_times()
     b.profile(False)
@@ -308,6 +315,7 @@ def main():
                 "avg_launch_us": jac_ms / max(jac_n, 1) * 1e3, "launches": jac_n,
                 "share_of_kernel_time": jac_ms / max(sum(v[0] for v in kt.values()), 1e-12)}
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in kt.items() if v[1]}
+    kernels["_steps"] = prof_steps
 
     # end to end through the C ABI with host-owned state: every step uploads the state of
     # every case from pinned host memory, steps, and reads the new state and stats back

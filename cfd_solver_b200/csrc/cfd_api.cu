@@ -156,7 +156,14 @@ struct cfd_batch {
     int* iscal = nullptr;
     double* partial = nullptr;
     unsigned int* counter = nullptr;
-    int* flags = nullptr;  // [0] active (pressure), [1] mactive (momentum), [2] kernel wait timeout
+    // device flags: [0] cases still in the pressure solve, [1] (case, field) pairs still in
+    // the momentum solves, [2] / [3] this step's momentum-pair / pressure-iteration counts,
+    // [4] kernel wait timeout, [5] / [6] cumulative pair / iteration counts (graph steps)
+    int* flags = nullptr;
+    bool use_graph = true;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int launches_per_pair = 2, launches_per_iter = 0, launches_fixed = 0;
+    int flags_total0[2] = {0, 0};
     unsigned long long* work = nullptr;  // k_jac traffic counters
     long long launches = 0;              // kernels launched since creation
     int* h_flags = nullptr;
@@ -232,12 +239,12 @@ int flush_profile(cfd_batch* b) {
     return CFD_OK;
 }
 
-// reads the device flags (all four, one copy); fails if a kernel's bounded wait gave up
+// reads the device flags (one copy); fails if a kernel's bounded wait gave up
 int read_flag(cfd_batch* b, int idx, int* out) {
-    CK(cudaMemcpyAsync(b->h_flags, b->flags, 4 * sizeof(int), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(b->h_flags, b->flags, 8 * sizeof(int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
     *out = b->h_flags[idx];
-    if (b->h_flags[2]) return fail(CFD_E_CUDA, "a bounded wait inside a kernel timed out");
+    if (b->h_flags[4]) return fail(CFD_E_CUDA, "a bounded wait inside a kernel timed out");
     return CFD_OK;
 }
 
@@ -405,27 +412,53 @@ int run_vcycle(cfd_batch* b) {
     return CFD_OK;
 }
 
-int one_step(cfd_batch* b) {
+// ---- the pieces of one step (also captured into the step graph)
+void enq_begin(cfd_batch* b, BatchDev& bd) {
+    cudaMemsetAsync(b->flags, 0, 4 * sizeof(int), b->st);
+    Prof pr(b, K_RHS);
+    k_rhs<<<bd.njtiles, NT, kRhsSmem, b->st>>>(bd);
+}
+void enq_mom_pair(cfd_batch* b, BatchDev& bd) {
+    for (int s = 0; s < 2; s++) {
+        Prof pr(b, K_JAC);
+        k_jac<<<bd.njtiles, NT, kJacSmem, b->st>>>(bd);
+    }
+}
+void enq_mid(cfd_batch* b, BatchDev& bd) {
+    {
+        Prof pr(b, K_UPBC);
+        k_upbc<<<b->n, BC_THREADS, 0, b->st>>>(bd);
+    }
+    Prof pr(b, K_FACE_Q);
+    k_face_q<<<bd.njtiles, NT, kFaceQSmem, b->st>>>(bd);
+}
+void enq_p_iter(cfd_batch* b, BatchDev& bd) {
+    const int nf = bd.nftiles;
+    { Prof pr(b, K_BICG_P); k_bicg_p<<<nf, NT, 0, b->st>>>(bd); }
+    run_vcycle(b);
+    { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 0); }
+    { Prof pr(b, K_BICG_S); k_bicg_s<<<nf, NT, 0, b->st>>>(bd); }
+    run_vcycle(b);
+    { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 1); }
+    { Prof pr(b, K_BICG_X); k_bicg_x<<<nf, NT, 0, b->st>>>(bd, b->maxit_p); }
+}
+void enq_end(cfd_batch* b, BatchDev& bd) {
+    const int nf = bd.nftiles;
+    { Prof pr(b, K_CORRECT); k_correct<<<nf, NT, 0, b->st>>>(bd); }
+    { Prof pr(b, K_BC); k_bc<<<b->n, BC_THREADS, 2 * (b->max_W + 1) * sizeof(double), b->st>>>(bd); }
+    { Prof pr(b, K_DIAG); k_diag<<<nf, NT, 0, b->st>>>(bd); }
+}
+
+// one step with host-side loop control (per-kernel profiling works on this path)
+int one_step_direct(cfd_batch* b) {
     BatchDev& bd = b->bd;
     bd.cur = b->cur;
-    const int nf = bd.nftiles;
-    CK(cudaMemsetAsync(b->flags, 0, 2 * sizeof(int), b->st));
-    {
-        Prof pr(b, K_RHS);
-        k_rhs<<<bd.njtiles, NT, kRhsSmem, b->st>>>(bd);
-    }
+    enq_begin(b, bd);
     // momentum / energy solves: sweeps in pairs until every (case, field) stopped; the
     // counter is read every second pair (a finished case's CTAs leave at once)
     const int npairs = std::max(1, b->maxit_mom / 2);
     for (int pair = 0; pair < npairs; pair++) {
-        {
-            Prof pr(b, K_JAC);
-            k_jac<<<bd.njtiles, NT, kJacSmem, b->st>>>(bd, 1, 2 * pair, 0);
-        }
-        {
-            Prof pr(b, K_JAC);
-            k_jac<<<bd.njtiles, NT, kJacSmem, b->st>>>(bd, 0, 2 * pair + 1, 1);
-        }
+        enq_mom_pair(b, bd);
         if (pair % 2 == 1 || pair == npairs - 1) {
             int m = 0;
             int rc = read_flag(b, 1, &m);
@@ -433,14 +466,7 @@ int one_step(cfd_batch* b) {
             if (m <= 0) break;
         }
     }
-    {
-        Prof pr(b, K_UPBC);
-        k_upbc<<<b->n, BC_THREADS, 0, b->st>>>(bd);
-    }
-    {
-        Prof pr(b, K_FACE_Q);
-        k_face_q<<<bd.njtiles, NT, kFaceQSmem, b->st>>>(bd);
-    }
+    enq_mid(b, bd);
     // pressure correction: the first iteration is launched without a check (a case whose
     // q vanished is flagged done by k_face_q and its CTAs leave at once)
     for (int it = 0; it < b->maxit_p; it++) {
@@ -450,30 +476,107 @@ int one_step(cfd_batch* b) {
             if (rc) return rc;
             if (a <= 0) break;
         }
-        { Prof pr(b, K_BICG_P); k_bicg_p<<<nf, NT, 0, b->st>>>(bd, it == 0); }
-        run_vcycle(b);
-        { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 0); }
-        { Prof pr(b, K_BICG_S); k_bicg_s<<<nf, NT, 0, b->st>>>(bd); }
-        run_vcycle(b);
-        { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 1); }
-        { Prof pr(b, K_BICG_X); k_bicg_x<<<nf, NT, 0, b->st>>>(bd, b->maxit_p, it == 0); }
+        enq_p_iter(b, bd);
     }
-    {
-        Prof pr(b, K_CORRECT);
-        k_correct<<<nf, NT, 0, b->st>>>(bd);
-    }
-    {
-        Prof pr(b, K_BC);
-        k_bc<<<b->n, BC_THREADS, 2 * (b->max_W + 1) * sizeof(double), b->st>>>(bd);
-    }
-    {
-        Prof pr(b, K_DIAG);
-        k_diag<<<nf, NT, 0, b->st>>>(bd);
-    }
+    enq_end(b, bd);
     CK(cudaGetLastError());
+    return CFD_OK;
+}
+
+// Build the step graph for state parity `cur`: child graphs for the straight segments and
+// two while-loops whose condition kernels read the device counters of still-iterating work.
+int build_step_graph(cfd_batch* b, int cur) {
+    const bool prof = b->prof;
+    b->prof = false;
+    const long long l0 = b->launches;
+    BatchDev bd = b->bd;
+    bd.cur = cur;
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphNode_t prev = nullptr;
+    auto child = [&](auto&& enqueue) -> int {
+        cudaGraph_t seg = nullptr;
+        CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+        enqueue();
+        CK(cudaStreamEndCapture(b->st, &seg));
+        cudaGraphNode_t n = nullptr;
+        CK(cudaGraphAddChildGraphNode(&n, g, prev ? &prev : nullptr, prev ? 1 : 0, seg));
+        cudaGraphDestroy(seg);
+        prev = n;
+        return CFD_OK;
+    };
+    auto loop = [&](auto&& enqueue, int* flag, int* counter, int maxc, int* total) -> int {
+        cudaGraphConditionalHandle h;
+        CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t n = nullptr;
+        CK(cudaGraphAddNode(&n, g, prev ? &prev : nullptr, prev ? 1 : 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CK(cudaStreamBeginCaptureToGraph(b->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        enqueue();
+        k_loop_cond<<<1, 32, 0, b->st>>>(h, flag, counter, maxc, total);
+        cudaGraph_t out = nullptr;
+        CK(cudaStreamEndCapture(b->st, &out));
+        prev = n;
+        return CFD_OK;
+    };
+    int rc = child([&] { enq_begin(b, bd); });
+    const long long la = b->launches;
+    if (!rc) rc = loop([&] { enq_mom_pair(b, bd); }, b->flags + 1, b->flags + 2,
+                       std::max(1, b->maxit_mom / 2), b->flags + 5);
+    const long long lm = b->launches;
+    if (!rc) rc = child([&] { enq_mid(b, bd); });
+    const long long lp0 = b->launches;
+    if (!rc) rc = loop([&] { enq_p_iter(b, bd); }, b->flags + 0, b->flags + 3, b->maxit_p, b->flags + 6);
+    const long long lp1 = b->launches;
+    if (!rc) rc = child([&] { enq_end(b, bd); });
+    if (!rc) {
+        // kernels per straight segment, per loop iteration (+1: the condition kernel)
+        b->launches_per_pair = (int)(lm - la) + 1;
+        b->launches_per_iter = (int)(lp1 - lp0) + 1;
+        b->launches_fixed = (int)((la - l0) + (lp0 - lm) + (b->launches - lp1));
+        if (cudaGraphInstantiate(&b->gexec[cur], g, 0) != cudaSuccess) rc = fail(CFD_E_CUDA, "graph instantiation failed");
+    }
+    cudaGraphDestroy(g);
+    b->launches = l0;
+    b->prof = prof;
+    return rc;
+}
+
+int one_step(cfd_batch* b) {
+    int rc;
+    if (b->use_graph && !b->prof) {
+        if (!b->gexec[b->cur]) {
+            rc = build_step_graph(b, b->cur);
+            if (rc) return rc;
+        }
+        CK(cudaGraphLaunch(b->gexec[b->cur], b->st));
+        b->launches += b->launches_fixed;  // the loops' share is added from the device counters
+    } else {
+        rc = one_step_direct(b);
+        if (rc) return rc;
+    }
     b->cur ^= 1;
     b->steps_done++;
     if (b->prof) return flush_profile(b);
+    return CFD_OK;
+}
+
+// adds the loop launches of graph steps (from the cumulative device counters) to the count
+int account_graph_launches(cfd_batch* b) {
+    if (!b->use_graph) return CFD_OK;
+    int dummy = 0;
+    int rc = read_flag(b, 0, &dummy);
+    if (rc) return rc;
+    const int tp = b->h_flags[5], ti = b->h_flags[6];
+    b->launches += (long long)(tp - b->flags_total0[0]) * b->launches_per_pair +
+                   (long long)(ti - b->flags_total0[1]) * b->launches_per_iter;
+    b->flags_total0[0] = tp;
+    b->flags_total0[1] = ti;
     return CFD_OK;
 }
 
@@ -676,13 +779,13 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     ALLOC(b->iscal, sizeof(int) * NISCAL * ncases);
     ALLOC(b->partial, sizeof(double) * PSTRIDE * std::max<size_t>(ftiles.size(), 1));
     ALLOC(b->counter, sizeof(unsigned) * ncases);
-    ALLOC(b->flags, sizeof(int) * 4);
+    ALLOC(b->flags, sizeof(int) * 8);
     ALLOC(b->work, sizeof(unsigned long long) * 4);
     ALLOC(b->dtmaps, (size_t)256 * ncases);
     ALLOC(b->dtiles, sizeof(Tile) * std::max<size_t>(ntl, 1));
     ALLOC(b->dcc, sizeof(int) * std::max<size_t>(ncc, 1));
 #undef ALLOC
-    if (cudaHostAlloc((void**)&b->h_flags, sizeof(int) * 4, cudaHostAllocDefault) != cudaSuccess)
+    if (cudaHostAlloc((void**)&b->h_flags, sizeof(int) * 8, cudaHostAllocDefault) != cudaSuccess)
         return cleanup(fail(CFD_E_CUDA, "pinned allocation failed"));
     cudaMemsetAsync(b->f64, 0, (size_t)b->n64 * sizeof(double), b->st);
     cudaMemsetAsync(b->f32, 0, (size_t)b->n32 * sizeof(float), b->st);
@@ -690,6 +793,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     cudaMemsetAsync(b->iscal, 0, sizeof(int) * NISCAL * ncases, b->st);
     cudaMemsetAsync(b->counter, 0, sizeof(unsigned) * ncases, b->st);
     cudaMemsetAsync(b->work, 0, sizeof(unsigned long long) * 4, b->st);
+    cudaMemsetAsync(b->flags, 0, sizeof(int) * 8, b->st);
     CK(cudaStreamSynchronize(b->st));
     {
         const size_t smem = 2 * (size_t)(b->max_W + 1) * sizeof(double);
@@ -750,7 +854,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     }
     bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
     bd.jtiles = b->dtiles + pos_jt; bd.njtiles = (int)jtiles.size();
-    bd.error = b->flags + 2;
+    bd.error = b->flags + 4;
     for (int l = 0; l < MAXLEV; l++) {
         bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
         bd.mtiles[l] = b->dtiles + pos_mt[l]; bd.nmtiles[l] = (int)mt[l].size();
@@ -816,7 +920,7 @@ int cfd_batch_step(cfd_batch* b, int nsteps) {
         }
     }
     CK(cudaStreamSynchronize(b->st));
-    return CFD_OK;
+    return account_graph_launches(b);
 }
 
 int cfd_batch_stats(cfd_batch* b, int case_index, cfd_step_stats* out) {
@@ -848,6 +952,8 @@ int cfd_batch_get_plane(cfd_batch* b, int case_index, const char* name, double* 
 int cfd_batch_destroy(cfd_batch* b) {
     if (!b) return CFD_OK;
     if (b->st) cudaStreamSynchronize(b->st);
+    for (int k = 0; k < 2; k++)
+        if (b->gexec[k]) cudaGraphExecDestroy(b->gexec[k]);
     for (auto& l : b->pending) { cudaEventDestroy(l.e0); cudaEventDestroy(l.e1); }
     for (auto e : b->pool) cudaEventDestroy(e);
     cudaFree(b->f64); cudaFree(b->f32); cudaFree(b->dc); cudaFree(b->scal); cudaFree(b->iscal);

@@ -434,17 +434,21 @@ constexpr int JT_FIELD = JTW * JTH + 2 * TX * TYJ;
 constexpr size_t JAC_SMEM = (size_t)NFIELD * JT_FIELD * sizeof(double) + 128;
 const size_t kJacSmem = JAC_SMEM;
 
-__global__ void __launch_bounds__(NT, 3) k_jac(BatchDev b, int to_scratch, int sweep, int decide) {
+__global__ void __launch_bounds__(NT, 3) k_jac(BatchDev b) {
     extern __shared__ __align__(128) unsigned char jraw[];
     __shared__ __align__(8) uint64_t bar[NFIELD];
     double* jsm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(jraw) + 127) & ~uintptr_t(127));
     const Tile t = b.jtiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
     const int* isc = b.iscal + (long long)t.c * NISCAL;
-    int mask = 0;
+    int mask = 0, sweep = 0;
 #pragma unroll
     for (int f = 0; f < NFIELD; f++) mask |= (isc[I_MDONE0 + f] == 0) << f;
     if (mask == 0) return;  // uniform over the case's CTAs
+    // the case's sweep index: every still-active field has done the same number of sweeps;
+    // even sweeps go A -> B, odd sweeps B -> A and decide the stop
+    sweep = isc[I_MIT0 + (__ffs(mask) - 1)];
+    const int to_scratch = (sweep & 1) == 0, decide = sweep & 1;
     const int tid = threadIdx.x;
     const int ld = c.ld, n1 = c.n1;
     const int nxt = b.cur ^ 1;
@@ -692,9 +696,10 @@ __global__ void __launch_bounds__(NT, 3) k_face_q(BatchDev b) {
 
 // ---------------------------------------------------------------------------
 // BiCGStab, right-preconditioned, FP64 vectors; per-case scalars live on the device
-__global__ void __launch_bounds__(NT) k_bicg_p(BatchDev b, int first) {
+__global__ void __launch_bounds__(NT) k_bicg_p(BatchDev b) {
     const Tile t = b.ftiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const bool first = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
     const CaseDev& c = b.cases[t.c];
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
     if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
@@ -774,9 +779,10 @@ __global__ void __launch_bounds__(NT) k_bicg_s(BatchDev b) {
     store_mirrored(mplane(b, L, M_X), L.ld, i, j, L.W, c.periodic, 0.0f);
 }
 
-__global__ void __launch_bounds__(NT) k_bicg_x(BatchDev b, int maxit, int first) {
+__global__ void __launch_bounds__(NT) k_bicg_x(BatchDev b, int maxit) {
     const Tile t = b.ftiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const bool first = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
     const CaseDev& c = b.cases[t.c];
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
     const double* sc0 = b.scal + (long long)t.c * NSCAL;
@@ -1393,6 +1399,17 @@ __global__ void __launch_bounds__(BC_THREADS) k_si(BatchDev b) {
             s = s + (ca + cb) * 0.5 * c.d1;
             store_mirrored(SI, ld, i, j, c.W, c.periodic, s);
         }
+    }
+}
+
+// condition of a graph while-loop: keep looping while `*flag > 0` and fewer than `maxc`
+// iterations ran this step; `total` accumulates iterations over all steps
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, const int* flag, int* counter, int maxc,
+                            int* total) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const int n = ++(*counter);
+        atomicAdd(total, 1);
+        cudaGraphSetConditional(h, (*flag > 0 && n < maxc) ? 1u : 0u);
     }
 }
 

@@ -5,16 +5,16 @@
 namespace cfd {
 __global__ void k_assemble_p(BatchDev b);
 __global__ void k_rhs(BatchDev b);
-__global__ void k_jac(BatchDev b, int to_scratch, int sweep, int decide);
+__global__ void k_jac(BatchDev b);
 extern const size_t kJacSmem;  // dynamic shared memory of k_jac
 extern const size_t kRhsSmem;
 extern const size_t kFaceQSmem;
 __global__ void k_upbc(BatchDev b);
 __global__ void k_face_q(BatchDev b);
-__global__ void k_bicg_p(BatchDev b, int first);
+__global__ void k_bicg_p(BatchDev b);
 __global__ void k_spmv(BatchDev b, int mode);
 __global__ void k_bicg_s(BatchDev b);
-__global__ void k_bicg_x(BatchDev b, int maxit, int first);
+__global__ void k_bicg_x(BatchDev b, int maxit);
 __global__ void k_mg_smooth(BatchDev b, int l, int colour);
 __global__ void k_mg_smooth_blk(BatchDev b, int l, int reverse, int zero_init);
 __global__ void k_mg_resid(BatchDev b, int l);
@@ -26,4 +26,5 @@ __global__ void k_correct(BatchDev b);
 __global__ void k_bc(BatchDev b);
 __global__ void k_diag(BatchDev b);
 __global__ void k_si(BatchDev b);
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, const int* flag, int* counter, int maxc, int* total);
 }  // namespace cfd
