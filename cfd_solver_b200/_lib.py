@@ -27,7 +27,8 @@ SYMBOLS = ("cfd_params_default", "cfd_last_error", "cfd_device_count", "cfd_set_
            "cfd_batch_destroy", "cfd_case_bytes", "cfd_batch_profile", "cfd_batch_kernel_times",
            "cfd_batch_sync", "cfd_batch_stream", "cfd_batch_launches", "cfd_batch_work",
            "cfd_batch_state_bytes", "cfd_batch_get_state", "cfd_batch_set_state",
-           "cfd_gauss_solve", "cfd_gauss_solve_noalloc")
+           "cfd_gauss_solve", "cfd_gauss_solve_noalloc", "cfd_batch_fetch_stats", "cfd_batch_admit",
+           "cfd_batch_set_active", "cfd_serve")
 
 _D = ctypes.c_double
 _PD = ctypes.POINTER(ctypes.c_double)
@@ -61,6 +62,31 @@ class CfdStepStats(ctypes.Structure):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "it_mom"}
         d["it_mom"] = list(self.it_mom)
         return d
+
+
+class CfdRequest(ctypes.Structure):
+    _fields_ = [("arrival_s", _D), ("grid", ctypes.POINTER(CfdGrid)), ("params", CfdParams),
+                ("tol", _D), ("max_steps", ctypes.c_int)]
+
+
+class CfdResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("slot", ctypes.c_int), ("steps", ctypes.c_int),
+                ("arrival_s", _D), ("admit_s", _D), ("done_s", _D), ("latency_s", _D),
+                ("nu", _D), ("steady_res_rel", _D), ("mass_res_rel", _D)]
+
+
+class CfdServeConfig(ctypes.Structure):
+    _fields_ = [("nclasses", ctypes.c_int), ("class_grids", ctypes.POINTER(CfdGrid)),
+                ("class_profile", ctypes.POINTER(ctypes.c_int)),
+                ("class_slots", ctypes.POINTER(ctypes.c_int)), ("hbm_budget", ctypes.c_size_t),
+                ("steps_per_tick", ctypes.c_int)]
+
+
+class CfdServeStats(ctypes.Structure):
+    _fields_ = [("makespan_s", _D), ("cases_per_s", _D), ("p50_latency_s", _D),
+                ("p99_latency_s", _D), ("mean_latency_s", _D), ("steps", ctypes.c_longlong),
+                ("cell_updates", ctypes.c_longlong), ("converged", ctypes.c_int),
+                ("failed", ctypes.c_int), ("slots", ctypes.c_int)]
 
 
 class CfdError(RuntimeError):
@@ -116,6 +142,11 @@ def lib():
                                   ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p,
                                   _D, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]
     L.cfd_gauss_solve_noalloc.argtypes = L.cfd_gauss_solve.argtypes
+    L.cfd_batch_fetch_stats.argtypes = [vp, ctypes.POINTER(CfdStepStats), ctypes.c_int]
+    L.cfd_batch_admit.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CfdGrid), ctypes.POINTER(CfdParams)]
+    L.cfd_batch_set_active.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.cfd_serve.argtypes = [ctypes.POINTER(CfdServeConfig), ctypes.POINTER(CfdRequest), ctypes.c_int,
+                            ctypes.POINTER(CfdResult), ctypes.POINTER(CfdServeStats)]
     special = {"cfd_params_default", "cfd_last_error", "cfd_case_bytes", "cfd_batch_stream",
                "cfd_batch_launches", "cfd_batch_state_bytes"}
     for name in SYMBOLS:

@@ -147,7 +147,7 @@ struct cfd_batch {
     std::vector<CaseDev> hc;
     std::vector<cfd_params> prm;
     std::vector<CaseGeom> geom;
-    std::vector<double> q_l2_first, sr_first;
+    std::vector<double> q_l2_first, sr_first;  // unused (first-step references live on the device)
     CaseDev* dc = nullptr;
     double* f64 = nullptr;
     float* f32 = nullptr;
@@ -368,6 +368,23 @@ void cheb_bounds(const cfd_grid& g, const cfd_params& p, CaseDev& d) {
     }
 }
 
+// physics, numerics and Chebyshev bounds of one case into its descriptor
+void case_params_to_dev(CaseDev& d, const cfd_grid& g, const cfd_params& p) {
+    d.fix_T_annw = p.fix_T_annw; d.fix_circ_de = p.fix_circ_de; d.warm_up = p.warm_start;
+    d.d0 = g.dxi0; d.d1 = g.dxi1; d.dt = p.dt; d.Re = p.Re; d.Pr = p.Pr; d.Ri = p.Ri; d.F = p.F;
+    d.Pi = acos(-1.0);
+    const double thetamax = d.Pi / 12.0;
+    d.speed_amp = thetamax * 2.0 * d.Pi * p.F;
+    d.accn_amp = 2.0 * d.Pi * p.F * d.speed_amp;
+    d.uinf = sin(p.alpha_deg * d.Pi / 180.0);
+    d.vinf = cos(p.alpha_deg * d.Pi / 180.0);
+    d.sa = sin(p.alpha_deg * d.Pi / 180.0);
+    d.ca = cos(p.alpha_deg * d.Pi / 180.0);
+    d.ar = g.ar; d.omega_p = p.omega_p; d.lid_u = p.lid_u;
+    d.tol_mom = p.tol_mom; d.atol_mom = p.atol_mom; d.tol_p = p.tol_p; d.atol_p = p.atol_p;
+    cheb_bounds(g, p, d);
+}
+
 void make_tiles(int ilo, int ihi, int n1, int cid, std::vector<Tile>& out, int ty = TY) {
     int k = 0;
     for (int j0 = 1; j0 <= n1 - 2; j0 += ty)
@@ -580,26 +597,13 @@ int account_graph_launches(cfd_batch* b) {
     return CFD_OK;
 }
 
-// steady residual: mean |du| + |dv| + |dT| per unknown cell and unit time
-double steady_res(const cfd_batch* b, int c) {
-    const double* sc = b->hscal.data() + (size_t)c * NSCAL;
-    const CaseDev& d = b->hc[c];
-    const double ncell = (double)(d.ihi - d.ilo + 1) * (d.n1 - 2);
-    return (sc[S_DUL1] + sc[S_DTL1]) / (d.dt * ncell);
-}
-
 int fetch_scalars(cfd_batch* b) {
     b->hscal.resize((size_t)b->n * NSCAL);
     b->hiscal.resize((size_t)b->n * NISCAL);
     CK(cudaMemcpyAsync(b->hscal.data(), b->scal, b->hscal.size() * sizeof(double), cudaMemcpyDeviceToHost, b->st));
     CK(cudaMemcpyAsync(b->hiscal.data(), b->iscal, b->hiscal.size() * sizeof(int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
-    for (int c = 0; c < b->n; c++) {
-        if (b->q_l2_first[c] < 0 && b->steps_done > 0) {
-            b->q_l2_first[c] = b->hscal[(size_t)c * NSCAL + S_QL2];
-            b->sr_first[c] = steady_res(b, c);
-        }
-    }
+
     return CFD_OK;
 }
 
@@ -616,11 +620,12 @@ void fill_stats(cfd_batch* b, int c, cfd_step_stats* s) {
     s->q_l1 = sc[S_QL1]; s->q_l2 = sc[S_QL2]; s->q_max = sc[S_QMAX];
     s->dT_l1 = sc[S_DTL1]; s->dT_max = sc[S_DTMAX];
     s->p_res_rel = sc[S_NB1] > 0 ? sc[S_RL1] / sc[S_NB1] : 0.0;
-    const double q0 = b->q_l2_first[c];
+    const double q0 = sc[S_QL2_0];
     s->mass_res_rel = q0 > 0 ? sc[S_QL2] / q0 : (sc[S_QL2] == 0 ? 0.0 : 1.0);
-    s->steady_res = steady_res(b, c);
-    const double r0 = b->sr_first[c];
+    s->steady_res = sc[S_SR];
+    const double r0 = sc[S_SR0];
     s->steady_res_rel = r0 > 0 ? s->steady_res / r0 : (s->steady_res == 0 ? 0.0 : 1.0);
+    s->steps = is[I_NSTEP];
 }
 
 int plane_id(const char* name, int cur) {
@@ -638,6 +643,50 @@ int plane_id(const char* name, int cur) {
 }
 
 }  // namespace
+
+// Grid, normals, initial state, descriptor and per-case scalars of case `c` (a slot of the
+// batch); with `setup` also its pressure stencil and multigrid hierarchy.
+int upload_case(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, bool setup) {
+    CaseDev& d = b->hc[c];
+    case_params_to_dev(d, g, p);
+    b->prm[c] = p;
+    std::vector<double> pad;
+    auto put = [&](int plane_id, const double* src) -> int {
+        pad_plane(d, src, pad);
+        CK(cudaMemcpy(b->f64 + d.base + H - 16 + (long long)plane_id * d.ps, pad.data(), sizeof(double) * d.ps,
+                      cudaMemcpyHostToDevice));
+        return CFD_OK;
+    };
+    const double* gp[10] = {g.x, g.y, g.xix, g.xiy, g.etx, g.ety, g.alph, g.beta, g.gam, g.jac};
+    const int gid[10] = {P_X, P_Y, P_XIX, P_XIY, P_ETX, P_ETY, P_ALPH, P_BETA, P_GAM, P_JAC};
+    for (int m = 0; m < 10; m++)
+        if (int rc = put(gid[m], gp[m])) return rc;
+    std::vector<double> vec((size_t)g.n0 * g.n1, 0.0);  // normals as rows 0..3 of P_VEC
+    const double* nv[4] = {g.xnix, g.xniy, g.xnox, g.xnoy};
+    for (int r = 0; r < 4 && r < g.n1; r++)
+        for (int i = 0; i < g.n0; i++) vec[(size_t)r * g.n0 + i] = nv[r][i];
+    if (int rc = put(P_VEC, vec.data())) return rc;
+    std::vector<double> st[6];
+    initial_state(&g, &p, d, st);
+    const int sid[6] = {P_U, P_V, P_T0 + b->cur, P_UP0 + b->cur, P_VP0 + b->cur, P_P};
+    for (int m = 0; m < 6; m++)
+        if (int rc = put(sid[m], st[m].data())) return rc;
+    CK(cudaMemcpy(b->dc + c, &d, sizeof(CaseDev), cudaMemcpyHostToDevice));
+    std::vector<double> sc(NSCAL, 0.0);
+    std::vector<int> is(NISCAL, 0);
+    is[I_ACTIVE] = 1;
+    CK(cudaMemcpy(b->scal + (size_t)c * NSCAL, sc.data(), sizeof(double) * NSCAL, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->iscal + (size_t)c * NISCAL, is.data(), sizeof(int) * NISCAL, cudaMemcpyHostToDevice));
+    if (setup) {
+        BatchDev bd = b->bd;
+        k_assemble_p<<<d.tile_count, NT, 0, b->st>>>(bd, d.tile_begin);
+        for (int l = 0; l + 1 < d.nlev; l++)
+            k_mg_galerkin<<<d.lev[l + 1].tile_count, NT, 0, b->st>>>(bd, l, d.lev[l + 1].tile_begin);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(b->st));
+    }
+    return CFD_OK;
+}
 
 // ==========================================================================
 extern "C" {
@@ -717,19 +766,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         d.ps = G.ps;
         off64 += G.bytes64() - 16 + 16;
         off64 = rup(off64, 16);
-        d.fix_T_annw = p.fix_T_annw; d.fix_circ_de = p.fix_circ_de; d.warm_up = p.warm_start;
-        d.d0 = g.dxi0; d.d1 = g.dxi1; d.dt = p.dt; d.Re = p.Re; d.Pr = p.Pr; d.Ri = p.Ri; d.F = p.F;
-        d.Pi = acos(-1.0);
-        const double thetamax = d.Pi / 12.0;
-        d.speed_amp = thetamax * 2.0 * d.Pi * p.F;
-        d.accn_amp = 2.0 * d.Pi * p.F * d.speed_amp;
-        d.uinf = sin(p.alpha_deg * d.Pi / 180.0);
-        d.vinf = cos(p.alpha_deg * d.Pi / 180.0);
-        d.sa = sin(p.alpha_deg * d.Pi / 180.0);
-        d.ca = cos(p.alpha_deg * d.Pi / 180.0);
-        d.ar = g.ar; d.omega_p = p.omega_p; d.lid_u = p.lid_u;
-        d.tol_mom = p.tol_mom; d.atol_mom = p.atol_mom; d.tol_p = p.tol_p; d.atol_p = p.atol_p;
-        cheb_bounds(g, p, d);
+        case_params_to_dev(d, g, p);
         d.tile_begin = (int)ftiles.size();
         make_tiles(G.ilo, G.ihi, g.n1, c, ftiles);
         d.tile_count = (int)ftiles.size() - d.tile_begin;
@@ -862,45 +899,21 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     }
 
     // ---- upload grid + initial state (padded planes with halos)
-    std::vector<double> pad;
-    for (int c = 0; c < ncases; c++) {
-        const cfd_grid& g = grids[c];
-        const CaseDev& d = b->hc[c];
-        const double* gp[10] = {g.x, g.y, g.xix, g.xiy, g.etx, g.ety, g.alph, g.beta, g.gam, g.jac};
-        const int gid[10] = {P_X, P_Y, P_XIX, P_XIY, P_ETX, P_ETY, P_ALPH, P_BETA, P_GAM, P_JAC};
-        for (int m = 0; m < 10; m++) {
-            pad_plane(d, gp[m], pad);
-            CK(cudaMemcpy(b->f64 + d.base + H - 16 + (long long)gid[m] * d.ps, pad.data(),
-                          sizeof(double) * d.ps, cudaMemcpyHostToDevice));
-        }
-        // normals as rows 0..3 of P_VEC
-        std::vector<double> vec((size_t)g.n0 * g.n1, 0.0);
-        const double* nv[4] = {g.xnix, g.xniy, g.xnox, g.xnoy};
-        for (int r = 0; r < 4 && r < g.n1; r++)
-            for (int i = 0; i < g.n0; i++) vec[(size_t)r * g.n0 + i] = nv[r][i];
-        pad_plane(d, vec.data(), pad);
-        CK(cudaMemcpy(b->f64 + d.base + H - 16 + (long long)P_VEC * d.ps, pad.data(), sizeof(double) * d.ps,
-                      cudaMemcpyHostToDevice));
-        std::vector<double> st[6];
-        initial_state(&g, &params[c], d, st);
-        const int sid[6] = {P_U, P_V, P_T0, P_UP0, P_VP0, P_P};
-        for (int m = 0; m < 6; m++) {
-            pad_plane(d, st[m].data(), pad);
-            CK(cudaMemcpy(b->f64 + d.base + H - 16 + (long long)sid[m] * d.ps, pad.data(),
-                          sizeof(double) * d.ps, cudaMemcpyHostToDevice));
-        }
-    }
-    // ---- set-up kernels: pressure stencil, multigrid hierarchy
     b->cur = 0;
     bd.cur = 0;
+    for (int c = 0; c < ncases; c++) {
+        int rc = upload_case(b, c, grids[c], params[c], false);
+        if (rc) return cleanup(rc);
+    }
+    // ---- set-up kernels: pressure stencil, multigrid hierarchy
     {
         Prof pr(b, K_ASSEMBLE_P);
-        k_assemble_p<<<bd.nftiles, NT, 0, b->st>>>(bd);
+        k_assemble_p<<<bd.nftiles, NT, 0, b->st>>>(bd, 0);
     }
     for (int l = 0; l + 1 < b->nlev_max; l++) {
         if (bd.natiles[l + 1] == 0) continue;
         Prof pr(b, K_MG_GALERKIN);
-        k_mg_galerkin<<<bd.natiles[l + 1], NT, 0, b->st>>>(bd, l);
+        k_mg_galerkin<<<bd.natiles[l + 1], NT, 0, b->st>>>(bd, l, 0);
     }
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(b->st) != cudaSuccess)
         return cleanup(fail(CFD_E_CUDA, "set-up kernels failed"));
@@ -914,10 +927,6 @@ int cfd_batch_step(cfd_batch* b, int nsteps) {
     for (int s = 0; s < nsteps; s++) {
         int rc = one_step(b);
         if (rc) return rc;
-        if (s == 0 && b->steps_done == 1) {
-            rc = fetch_scalars(b);
-            if (rc) return rc;
-        }
     }
     CK(cudaStreamSynchronize(b->st));
     return account_graph_launches(b);
@@ -986,6 +995,33 @@ int cfd_batch_kernel_times(cfd_batch* b, const char** names, double* total_ms, l
 int cfd_batch_sync(cfd_batch* b) {
     if (!b) return fail(CFD_E_ARG, "null batch");
     CK(cudaStreamSynchronize(b->st));
+    return CFD_OK;
+}
+
+int cfd_batch_admit(cfd_batch* b, int slot, const cfd_grid* g, const cfd_params* p) {
+    if (!b || slot < 0 || slot >= b->n) return fail(CFD_E_ARG, "bad slot");
+    int rc = check_params(g, p);
+    if (rc) return rc;
+    const CaseDev& d = b->hc[slot];
+    if (g->n0 != d.n0 || g->n1 != d.n1 || p->profile != d.profile)
+        return fail(CFD_E_ARG, "case does not match the slot's geometry (n0, n1, profile)");
+    CK(cudaStreamSynchronize(b->st));
+    return upload_case(b, slot, *g, *p, true);
+}
+
+int cfd_batch_set_active(cfd_batch* b, int slot, int active) {
+    if (!b || slot < 0 || slot >= b->n) return fail(CFD_E_ARG, "bad slot");
+    const int v = active ? 1 : 0;
+    CK(cudaMemcpyAsync(b->iscal + (size_t)slot * NISCAL + I_ACTIVE, &v, sizeof(int), cudaMemcpyHostToDevice, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    return CFD_OK;
+}
+
+int cfd_batch_fetch_stats(cfd_batch* b, cfd_step_stats* out, int cap) {
+    if (!b || !out) return fail(CFD_E_ARG, "bad arguments");
+    int rc = fetch_scalars(b);
+    if (rc) return rc;
+    for (int c = 0; c < b->n && c < cap; c++) fill_stats(b, c, out + c);
     return CFD_OK;
 }
 

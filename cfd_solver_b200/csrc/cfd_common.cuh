@@ -55,7 +55,8 @@ enum Scalar {
     S_RHO, S_ALPHA, S_OMEGA, S_BETA, S_NB1, S_RL1, S_RL1_0,
     S_QL1, S_QL2, S_QMAX, S_DMAX, S_CL, S_CD, S_CM, S_NU, S_CIRC, S_CLP, S_CDP, S_CLV, S_CDV,
     S_DTL1, S_DTMAX, S_DUL1, S_CW0, S_CW1,  // Chebyshev weights of the u-type / T systems
-    S_MR0 = 26,           // 5 initial momentum residuals (L1)
+    S_QL2_0, S_SR, S_SR0,                   // first-step q_l2; steady residual (now, first step)
+    S_MR0 = 29,           // 5 initial momentum residuals (L1)
     S_MR = S_MR0 + NFIELD,  // 5 latest momentum residuals
     NSCAL = S_MR + NFIELD + 2
 };
@@ -66,6 +67,8 @@ enum IScalar {
     I_MDONE0,                 // 5 momentum done flags
     I_MIT0 = I_MDONE0 + NFIELD,  // 5 momentum sweep counts
     I_STATUS = I_MIT0 + NFIELD,
+    I_ACTIVE,                 // 0: an empty slot, skipped by every kernel
+    I_NSTEP,                  // steps taken since the case was admitted
     NISCAL
 };
 

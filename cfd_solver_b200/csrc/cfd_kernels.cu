@@ -36,8 +36,8 @@ __device__ __forceinline__ bool near_wall(const CaseDev& c, int i, int j) {
 
 // ---------------------------------------------------------------------------
 // pressure stencil assembly (PSolver.cpp:944-1040), also the set-up of MG level 0
-__global__ void __launch_bounds__(NT) k_assemble_p(BatchDev b) {
-    const Tile t = b.ftiles[blockIdx.x];
+__global__ void __launch_bounds__(NT) k_assemble_p(BatchDev b, int toff) {
+    const Tile t = b.ftiles[toff + blockIdx.x];
     const CaseDev& c = b.cases[t.c];
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
     if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
@@ -232,12 +232,15 @@ __global__ void __launch_bounds__(NT, 2) k_rhs(BatchDev b) {
     const int cur = b.cur, nxt = cur ^ 1;
     // halo tiles: u, v, T, p, up, vp; interior tiles: xix, xiy, etx, ety, alpha, gamma, beta
     double* SI = sm + RHS_HALO * JTW * JTH;
+    const bool active = b.iscal[(long long)t.c * NISCAL + I_ACTIVE] != 0;
+    if (tid == 0 && t.k == 0) {
+        int* is = b.iscal + (long long)t.c * NISCAL;
+        for (int f = 0; f < NFIELD; f++) { is[I_MDONE0 + f] = active ? 0 : 1; is[I_MIT0 + f] = 0; }
+        if (active) atomicAdd(b.mactive, NFIELD);
+        else is[I_PDONE] = 1;  // an empty slot takes no part in the step
+    }
+    if (!active) return;
     if (tid == 0) {
-        if (t.k == 0) {
-            int* is = b.iscal + (long long)t.c * NISCAL;
-            for (int f = 0; f < NFIELD; f++) { is[I_MDONE0 + f] = 0; is[I_MIT0 + f] = 0; }
-            atomicAdd(b.mactive, NFIELD);
-        }
         mbar_init(&bar, 1);
         fence_mbar_init();
         const char* maps = b.tmaps + (size_t)t.c * 256;
@@ -577,7 +580,7 @@ __global__ void __launch_bounds__(NT, 3) k_jac(BatchDev b) {
 // up/vp far-field condition (PSolver.cpp:1356-1382), one CTA per O-grid case
 __global__ void __launch_bounds__(BC_THREADS) k_upbc(BatchDev b) {
     const CaseDev& c = b.cases[blockIdx.x];
-    if (c.profile != OGRID) return;
+    if (c.profile != OGRID || !b.iscal[(long long)blockIdx.x * NISCAL + I_ACTIVE]) return;
     const int ld = c.ld, j = c.n1 - 1, nxt = b.cur ^ 1;
     double* UP = plane(b, c, P_UP0 + nxt);
     double* VP = plane(b, c, P_VP0 + nxt);
@@ -616,6 +619,7 @@ __global__ void __launch_bounds__(NT, 3) k_face_q(BatchDev b) {
     const CaseDev& c = b.cases[t.c];
     const int tid = threadIdx.x;
     const int nxt = b.cur ^ 1;
+    if (!b.iscal[(long long)t.c * NISCAL + I_ACTIVE]) return;  // uniform over the case
     if (tid == 0) {
         mbar_init(&bar, 1);
         fence_mbar_init();
@@ -675,6 +679,7 @@ __global__ void __launch_bounds__(NT, 3) k_face_q(BatchDev b) {
         int* is = b.iscal + (long long)t.c * NISCAL;
         sc[S_QL1] = red[0];
         sc[S_QL2] = sqrt(red[1]);
+        if (is[I_NSTEP] == 0) sc[S_QL2_0] = sqrt(red[1]);
         sc[S_QMAX] = red[2];
         sc[S_RHO] = red[1];
         sc[S_ALPHA] = 1.0;
@@ -992,8 +997,8 @@ __device__ __forceinline__ bool lev_unknown(const LevelDev& L, int periodic, int
     return i >= L.ilo && i <= L.ihi;
 }
 
-__global__ void __launch_bounds__(NT) k_mg_galerkin(BatchDev b, int l) {
-    const Tile t = b.atiles[l + 1][blockIdx.x];
+__global__ void __launch_bounds__(NT) k_mg_galerkin(BatchDev b, int l, int toff) {
+    const Tile t = b.atiles[l + 1][toff + blockIdx.x];
     const CaseDev& c = b.cases[t.c];
     const LevelDev& F = c.lev[l];
     const LevelDev& C = c.lev[l + 1];
@@ -1052,6 +1057,7 @@ __global__ void __launch_bounds__(NT) k_mg_galerkin(BatchDev b, int l) {
 __global__ void __launch_bounds__(NT) k_correct(BatchDev b) {
     const Tile t = b.ftiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
+    if (!b.iscal[(long long)t.c * NISCAL + I_ACTIVE]) return;  // uniform over the case
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
     // no pressure iteration ran (q vanished or broke down at once): pcor = 0
     const bool none = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
@@ -1112,6 +1118,7 @@ __global__ void __launch_bounds__(NT) k_correct(BatchDev b) {
 __global__ void __launch_bounds__(BC_THREADS) k_bc(BatchDev b) {
     const int cid = blockIdx.x;
     const CaseDev& c = b.cases[cid];
+    if (!b.iscal[(long long)cid * NISCAL + I_ACTIVE]) return;
     const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
     const int cur = b.cur, nxt = cur ^ 1;
     const bool cav = c.profile == CAVITY;
@@ -1346,6 +1353,7 @@ __global__ void __launch_bounds__(BC_THREADS) k_bc(BatchDev b) {
 __global__ void __launch_bounds__(NT) k_diag(BatchDev b) {
     const Tile t = b.ftiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
+    if (!b.iscal[(long long)t.c * NISCAL + I_ACTIVE]) return;  // uniform over the case
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
     double red[3] = {0.0, 0.0, 0.0};
     if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
@@ -1372,9 +1380,15 @@ __global__ void __launch_bounds__(NT) k_diag(BatchDev b) {
     }
     if (case_reduce<3, 0x5u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0) {
         double* sc = b.scal + (long long)t.c * NSCAL;
+        int* is = b.iscal + (long long)t.c * NISCAL;
         sc[S_DMAX] = fmax(red[0], 0.0);
         sc[S_DTL1] = red[1];
         sc[S_DTMAX] = red[2];
+        // steady residual: mean (|du| + |dv| + |dT|) / dt over the unknown cells
+        const double ncell = (double)(c.ihi - c.ilo + 1) * (c.n1 - 2);
+        sc[S_SR] = (sc[S_DUL1] + red[1]) / (c.dt * ncell);
+        if (is[I_NSTEP] == 0) sc[S_SR0] = sc[S_SR];
+        is[I_NSTEP] += 1;
     }
 }
 

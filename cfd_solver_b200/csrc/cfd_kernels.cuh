@@ -3,7 +3,7 @@
 #include "cfd_common.cuh"
 
 namespace cfd {
-__global__ void k_assemble_p(BatchDev b);
+__global__ void k_assemble_p(BatchDev b, int toff);
 __global__ void k_rhs(BatchDev b);
 __global__ void k_jac(BatchDev b);
 extern const size_t kJacSmem;  // dynamic shared memory of k_jac
@@ -21,7 +21,7 @@ __global__ void k_mg_resid(BatchDev b, int l);
 __global__ void k_mg_restrict(BatchDev b, int l);
 __global__ void k_mg_prolong(BatchDev b, int l);
 __global__ void k_mg_coarse(BatchDev b, int l, int sweeps);
-__global__ void k_mg_galerkin(BatchDev b, int l);
+__global__ void k_mg_galerkin(BatchDev b, int l, int toff);
 __global__ void k_correct(BatchDev b);
 __global__ void k_bc(BatchDev b);
 __global__ void k_diag(BatchDev b);

@@ -74,6 +74,23 @@ class Batch:
     def sync(self):
         _lib.check(_lib.lib().cfd_batch_sync(self.h), "cfd_batch_sync")
 
+    def admit(self, slot: int, grid, params):
+        """Write a new case into `slot` (same n0, n1, profile); the other slots keep running."""
+        s, keep = _lib.make_grid(grid)
+        self._keep.extend(keep)
+        self.grids[slot] = grid
+        _lib.check(_lib.lib().cfd_batch_admit(self.h, slot, ctypes.byref(s), ctypes.byref(params)),
+                   "cfd_batch_admit")
+
+    def set_active(self, slot: int, active: bool):
+        _lib.check(_lib.lib().cfd_batch_set_active(self.h, slot, int(active)), "cfd_batch_set_active")
+
+    def all_stats(self) -> list:
+        n = len(self.grids)
+        arr = (_lib.CfdStepStats * n)()
+        _lib.check(_lib.lib().cfd_batch_fetch_stats(self.h, arr, n), "cfd_batch_fetch_stats")
+        return [a.as_dict() for a in arr]
+
     def stream(self) -> int:
         return int(_lib.lib().cfd_batch_stream(self.h) or 0)
 
@@ -113,6 +130,44 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def serve(requests, classes, steps_per_tick: int = 50, slots=None, hbm_budget: int = 0):
+    """Run a real-time serving session (cfd_serve).
+
+    requests: list of (arrival_s, grid, params, tol, max_steps); classes: list of
+    (template grid, profile); slots: slots per class (or None with hbm_budget).
+    Returns (list of result dicts, stats dict).
+    """
+    keep = []
+    grids = []
+    for g, prof in classes:
+        s, k = _lib.make_grid(g)
+        keep.extend(k)
+        grids.append(s)
+    garr = (_lib.CfdGrid * len(grids))(*grids)
+    profs = (ctypes.c_int * len(classes))(*[p for _, p in classes])
+    sl = (ctypes.c_int * len(classes))(*slots) if slots is not None else None
+    cfg = _lib.CfdServeConfig(nclasses=len(classes), class_grids=garr, class_profile=profs,
+                              class_slots=sl, hbm_budget=int(hbm_budget), steps_per_tick=steps_per_tick)
+    rgrids = []
+    reqs = (_lib.CfdRequest * len(requests))()
+    for i, (t, g, prm, tol, mx) in enumerate(requests):
+        s, k = _lib.make_grid(g)
+        keep.extend(k)
+        rgrids.append(s)
+        reqs[i].arrival_s = t
+        reqs[i].grid = ctypes.pointer(rgrids[-1])
+        reqs[i].params = prm
+        reqs[i].tol = tol
+        reqs[i].max_steps = mx
+    res = (_lib.CfdResult * len(requests))()
+    st = _lib.CfdServeStats()
+    _lib.check(_lib.lib().cfd_serve(ctypes.byref(cfg), reqs, len(requests), res, ctypes.byref(st)),
+               "cfd_serve")
+    results = [{k: getattr(r, k) for k, _ in r._fields_} for r in res]
+    stats = {k: getattr(st, k) for k, _ in st._fields_}
+    return results, stats
 
 
 def _addr(buf) -> int:

@@ -120,6 +120,54 @@ int cfd_batch_get_plane(cfd_batch* b, int case_index, const char* name, double* 
 int cfd_batch_destroy(cfd_batch* b);
 /* device bytes a case of this size needs (admission by HBM budget) */
 size_t cfd_case_bytes(int n0, int n1, int profile);
+/* the stats of every case (cap entries at most), one device -> host copy */
+int cfd_batch_fetch_stats(cfd_batch* b, cfd_step_stats* out, int cap);
+
+/* ---- slots: continuous batching over a batch of fixed-geometry slots ----
+ * Every case of a batch is a slot. cfd_batch_admit() writes a new case into slot `slot`
+ * (same n0, n1 and profile as the slot): grid, initial state, parameters and its pressure
+ * stencil / multigrid set-up, while the other slots keep their resident state; the case
+ * then takes part in every cfd_batch_step(). cfd_batch_set_active(b, slot, 0) empties a
+ * slot (its kernels skip it), 1 re-activates it. */
+int cfd_batch_admit(cfd_batch* b, int slot, const cfd_grid* g, const cfd_params* p);
+int cfd_batch_set_active(cfd_batch* b, int slot, int active);
+
+/* ---- serving session: requests with arrival times over slot classes ---- */
+typedef struct cfd_request {
+    double arrival_s;     /* seconds after the session starts */
+    const cfd_grid* grid; /* must match a slot class (n0, n1, params.profile) */
+    cfd_params params;
+    double tol;           /* converged when steady_res_rel <= tol */
+    int max_steps;        /* step cap (result CFD_E_NOTCONV) */
+} cfd_request;
+
+typedef struct cfd_result {
+    int status; /* CFD_OK (converged), CFD_E_NOTCONV, CFD_E_DIVERGED */
+    int slot, steps;
+    double arrival_s, admit_s, done_s, latency_s;
+    double nu, steady_res_rel, mass_res_rel;
+} cfd_result;
+
+typedef struct cfd_serve_config {
+    int nclasses;
+    const cfd_grid* class_grids; /* one template grid per slot class (sets n0, n1) */
+    const int* class_profile;    /* CFD_PROFILE_* of each class */
+    const int* class_slots;      /* slots per class; NULL: an equal share of hbm_budget each */
+    size_t hbm_budget;           /* device bytes for all slots when class_slots is NULL */
+    int steps_per_tick;          /* steps between convergence checks / admissions */
+} cfd_serve_config;
+
+typedef struct cfd_serve_stats {
+    double makespan_s, cases_per_s, p50_latency_s, p99_latency_s, mean_latency_s;
+    long long steps, cell_updates;
+    int converged, failed, slots;
+} cfd_serve_stats;
+
+/* Runs a serving session in real time: requests are admitted into free slots of their
+ * class as they arrive, all active slots advance together, converged cases are retired
+ * and their slots back-filled. results[i] belongs to reqs[i]. */
+int cfd_serve(const cfd_serve_config* cfg, const cfd_request* reqs, int nreq, cfd_result* results,
+              cfd_serve_stats* stats);
 
 /* ---- timing: per-kernel CUDA-event durations accumulated on the batch's stream ---- */
 int cfd_batch_profile(cfd_batch* b, int enable);
