@@ -287,7 +287,7 @@ def main():
     # the traffic counters: per field-cell read x_k, rhs, x_{k-1} and write x_{k+1} (32 B; the
     # first sweep skips x_{k-1}); per cell read alpha, beta, gamma (24 B)
     dom = max(kt.items(), key=lambda kv: kv[1][0])
-    jac_ms, jac_n = kt.get("k_jac", (0.0, 0))
+    jac_ms, jac_n = kt.get("k_sweep", (0.0, 0))
     fc = work1[0] - work0[0]
     cc = work1[1] - work0[1]
     f0 = work1[2] - work0[2]
@@ -300,7 +300,7 @@ def main():
         peak, peak_src = 6650.0, "fallback"
     achieved = (jac_bytes / 1e9) / (jac_ms / 1e3) if jac_ms > 0 else 0.0
     traffic = None
-    tf = ROOT / "profiles" / "k_jac_traffic.json"
+    tf = ROOT / "profiles" / "k_sweep_traffic.json"
     if tf.exists() and jac_n:
         try:
             tj = json.loads(tf.read_text())
@@ -309,7 +309,7 @@ def main():
             traffic = tj["dram_over_algorithmic"] * jac_bytes / jac_n
         except Exception:
             traffic = None
-    roofline = {"kernel": "k_jac", "bound": "hbm", "achieved": achieved, "peak": peak,
+    roofline = {"kernel": "k_sweep", "bound": "hbm", "achieved": achieved, "peak": peak,
                 "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "algorithmic_bytes_per_launch": jac_bytes / max(jac_n, 1),
                 "avg_launch_us": jac_ms / max(jac_n, 1) * 1e3, "launches": jac_n,

@@ -18,6 +18,7 @@ OK = 0
 ERRORS = {-1: "CFD_E_ARG", -2: "CFD_E_CUDA", -3: "CFD_E_OOM", -4: "CFD_E_DIVERGED",
           -5: "CFD_E_MAXITER", -6: "CFD_E_BREAKDOWN", -7: "CFD_E_NOTCONV"}
 PROFILE_OGRID, PROFILE_CAVITY = 0, 1
+PRECISION_FP64, PRECISION_MIXED = 0, 1
 
 # exported symbols (kept in sync with include/cfd_b200.h; tests check both)
 SYMBOLS = ("cfd_params_default", "cfd_last_error", "cfd_device_count", "cfd_set_device",
@@ -47,7 +48,7 @@ class CfdParams(ctypes.Structure):
                 ("tol_mom", _D), ("atol_mom", _D), ("tol_p", _D), ("atol_p", _D),
                 ("maxit_mom", ctypes.c_int), ("maxit_p", ctypes.c_int), ("profile", ctypes.c_int),
                 ("fix_T_annw", ctypes.c_int), ("fix_circ_de", ctypes.c_int),
-                ("warm_start", ctypes.c_int), ("omega_p", _D), ("lid_u", _D)]
+                ("warm_start", ctypes.c_int), ("omega_p", _D), ("lid_u", _D), ("precision", ctypes.c_int)]
 
 
 class CfdStepStats(ctypes.Structure):

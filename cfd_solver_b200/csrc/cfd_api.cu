@@ -20,6 +20,7 @@
 #include "cfd_common.cuh"
 #include "cfd_kernels.cuh"
 #include "cfd_reduce.cuh"
+#include "cfd_sweep.cuh"
 
 using namespace cfd;
 
@@ -49,14 +50,14 @@ namespace {
 long long rup(long long x, long long a) { return (x + a - 1) / a * a; }
 
 enum KernelId {
-    K_ASSEMBLE_P, K_RHS, K_JAC, K_UPBC, K_FACE_Q, K_BICG_P, K_SPMV, K_BICG_S, K_BICG_X,
+    K_ASSEMBLE_P, K_RHS, K_SWEEP, K_UPBC, K_FACE_Q, K_BICG_P, K_SPMV, K_BICG_S, K_BICG_X,
     K_MG_SMOOTH, K_MG_RESID, K_MG_RESTRICT, K_MG_PROLONG, K_MG_COARSE, K_MG_GALERKIN,
-    K_CORRECT, K_BC, K_DIAG, K_SI, NKERNEL
+    K_CORRECT, K_BC, K_DIAG, K_SI, K_MOM_UPDATE, K_SWEEP_FIN, NKERNEL
 };
 const char* kKernelNames[NKERNEL] = {
-    "k_assemble_p", "k_rhs", "k_jac", "k_upbc", "k_face_q", "k_bicg_p", "k_spmv", "k_bicg_s",
+    "k_assemble_p", "k_rhs", "k_sweep", "k_upbc", "k_face_q", "k_bicg_p", "k_spmv", "k_bicg_s",
     "k_bicg_x", "k_mg_smooth", "k_mg_resid", "k_mg_restrict", "k_mg_prolong", "k_mg_coarse",
-    "k_mg_galerkin", "k_correct", "k_bc", "k_diag", "k_si"};
+    "k_mg_galerkin", "k_correct", "k_bc", "k_diag", "k_si", "k_mom_update", "k_sweep_fin"};
 
 struct LevelGeom {
     int W, n1, ld, ilo, ihi;
@@ -98,12 +99,14 @@ std::vector<LevelGeom> build_levels(int W, int n1, int periodic) {
 struct CaseGeom {
     int W, ld, ilo, ihi, periodic;
     long long ps;
+    int xld;         // FP32 precision-form planes: pitch (columns -4 .. W+1 and slack), stride
+    long long xps;
     std::vector<LevelGeom> lev;
     long long bytes64() const { return (long long)NPLANES * ps + 16; }
     long long words32() const {
         long long s = 0;
         for (auto& g : lev) s += (long long)NMG * g.ps + 32;
-        return s;
+        return s + (long long)NXPLANES * xps + 32;
     }
 };
 
@@ -116,6 +119,8 @@ CaseGeom case_geom(int n0, int n1, int profile) {
     g.ilo = g.periodic ? 0 : 1;
     g.ihi = g.periodic ? g.W - 1 : n0 - 2;
     g.lev = build_levels(g.W, n1, g.periodic);
+    g.xld = (int)rup(g.W + H32 + H + 2, 32);
+    g.xps = rup((long long)n1 * g.xld + 32, 32);
     return g;
 }
 
@@ -158,7 +163,8 @@ struct cfd_batch {
     unsigned int* counter = nullptr;
     // device flags: [0] cases still in the pressure solve, [1] (case, field) pairs still in
     // the momentum solves, [2] / [3] this step's momentum-pair / pressure-iteration counts,
-    // [4] kernel wait timeout, [5] / [6] cumulative pair / iteration counts (graph steps)
+    // [4] kernel wait timeout, [5] / [6] cumulative pair / iteration counts (graph steps),
+    // [7] this step's momentum sweep launches
     int* flags = nullptr;
     bool use_graph = true;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -174,6 +180,9 @@ struct cfd_batch {
     int nlev_max = 0;
     int ncol[MAXLEV] = {};
     int maxit_mom = 100, maxit_p = 200;
+    int precision = CFD_PRECISION_FP64;
+    int sw_grid = 0;      // CTAs of the persistent sweep kernel
+    size_t sw_smem = 0;
     int coarse_sweeps = 12;
     int max_W = 0;
     int cur = 0;
@@ -294,6 +303,8 @@ int check_params(const cfd_grid* g, const cfd_params* p) {
         return fail(CFD_E_ARG, "missing grid plane");
     if (!(p->dt > 0) || !(p->Re > 0) || !(p->Pr > 0)) return fail(CFD_E_ARG, "dt, Re, Pr must be > 0");
     if (p->maxit_mom < 2 || p->maxit_p < 1) return fail(CFD_E_ARG, "iteration caps too small");
+    if (p->precision != CFD_PRECISION_FP64 && p->precision != CFD_PRECISION_MIXED)
+        return fail(CFD_E_ARG, "unknown precision");
     const size_t N = (size_t)g->n0 * g->n1;
     for (size_t k = 0; k < N; k++) {
         if (!(g->alph[k] > 0) || !(g->gam[k] > 0) || !std::isfinite(g->beta[k]) || !std::isfinite(g->jac[k]))
@@ -432,16 +443,26 @@ int run_vcycle(cfd_batch* b) {
 // ---- the pieces of one step (also captured into the step graph)
 void enq_begin(cfd_batch* b, BatchDev& bd) {
     cudaMemsetAsync(b->flags, 0, 4 * sizeof(int), b->st);
+    cudaMemsetAsync(b->flags + 7, 0, sizeof(int), b->st);
     Prof pr(b, K_RHS);
     k_rhs<<<bd.njtiles, NT, kRhsSmem, b->st>>>(bd);
 }
 void enq_mom_pair(cfd_batch* b, BatchDev& bd) {
     for (int s = 0; s < 2; s++) {
-        Prof pr(b, K_JAC);
-        k_jac<<<bd.njtiles, NT, kJacSmem, b->st>>>(bd);
+        {
+            Prof pr(b, K_SWEEP);
+            if (b->precision == CFD_PRECISION_MIXED) k_sweep_mx<<<b->sw_grid, SW_THREADS, b->sw_smem, b->st>>>(bd);
+            else k_sweep_f64<<<b->sw_grid, SW_THREADS, b->sw_smem, b->st>>>(bd);
+        }
+        Prof pr(b, K_SWEEP_FIN);
+        k_sweep_fin<<<b->n, SWF_THREADS, 0, b->st>>>(bd);
     }
 }
 void enq_mid(cfd_batch* b, BatchDev& bd) {
+    if (b->precision == CFD_PRECISION_MIXED) {
+        Prof pr(b, K_MOM_UPDATE);
+        k_mom_update<<<bd.nftiles, NT, 0, b->st>>>(bd);
+    }
     {
         Prof pr(b, K_UPBC);
         k_upbc<<<b->n, BC_THREADS, 0, b->st>>>(bd);
@@ -700,6 +721,7 @@ void cfd_params_default(cfd_params* p) {
     p->profile = CFD_PROFILE_OGRID;
     p->fix_T_annw = 0; p->fix_circ_de = 0; p->warm_start = 1;
     p->omega_p = 1.0; p->lid_u = 1.0;
+    p->precision = CFD_PRECISION_FP64;
 }
 
 const char* cfd_last_error(void) { return g_err.c_str(); }
@@ -789,10 +811,18 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
             else cc[l].push_back(c);
             b->ncol[l] = std::max(b->ncol[l], (G.periodic && (lg.W & 1)) ? 6 : 4);
         }
+        d.xld = G.xld;
+        d.xps = G.xps;
+        d.xbase = off32 + 32 - H32;
+        off32 += (long long)NXPLANES * G.xps + 32;
+        off32 = rup(off32, 32);
         b->nlev_max = std::max(b->nlev_max, d.nlev);
         b->max_W = std::max(b->max_W, d.W);
         b->maxit_mom = std::max(b->maxit_mom, p.maxit_mom);
         b->maxit_p = std::max(b->maxit_p, p.maxit_p);
+        if (c == 0) b->precision = p.precision;
+        if (p.precision != b->precision)
+            return cleanup(fail(CFD_E_ARG, "all cases of a batch must use the same precision"));
     }
     if (b->max_W > 4096) return cleanup(fail(CFD_E_ARG, "grid width above 4096 columns"));
     b->n64 = off64 + 16;
@@ -814,11 +844,12 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     ALLOC(b->dc, sizeof(CaseDev) * ncases);
     ALLOC(b->scal, sizeof(double) * NSCAL * ncases);
     ALLOC(b->iscal, sizeof(int) * NISCAL * ncases);
-    ALLOC(b->partial, sizeof(double) * PSTRIDE * std::max<size_t>(ftiles.size(), 1));
+    ALLOC(b->partial, sizeof(double) * PSTRIDE *
+                          std::max<size_t>(std::max(ftiles.size(), jtiles.size() * SW_WARPS), 1));
     ALLOC(b->counter, sizeof(unsigned) * ncases);
     ALLOC(b->flags, sizeof(int) * 8);
     ALLOC(b->work, sizeof(unsigned long long) * 4);
-    ALLOC(b->dtmaps, (size_t)256 * ncases);
+    ALLOC(b->dtmaps, (size_t)TMAP_STRIDE * ncases);
     ALLOC(b->dtiles, sizeof(Tile) * std::max<size_t>(ntl, 1));
     ALLOC(b->dcc, sizeof(int) * std::max<size_t>(ncc, 1));
 #undef ALLOC
@@ -836,7 +867,11 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         const size_t smem = 2 * (size_t)(b->max_W + 1) * sizeof(double);
         if (smem > 48 * 1024)
             CK(cudaFuncSetAttribute(k_bc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        CK(cudaFuncSetAttribute(k_jac, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kJacSmem));
+        b->sw_smem = b->precision == CFD_PRECISION_MIXED ? sweep_smem_mx() : sweep_smem_f64();
+        const void* swk = b->precision == CFD_PRECISION_MIXED ? (const void*)k_sweep_mx : (const void*)k_sweep_f64;
+        CK(cudaFuncSetAttribute(swk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->sw_smem));
+        CK(cudaFuncSetAttribute(swk, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        b->sw_grid = (int)jtiles.size();  // one CTA per 32 x 16 tile
         CK(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem));
         CK(cudaFuncSetAttribute(k_face_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFaceQSmem));
     }
@@ -867,31 +902,45 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     bd.work = b->work;
     bd.tmaps = b->dtmaps;
     {
-        // 3-D tensor maps over each case's FP64 planes: x = column + 2 (from the halo column
-        // -2), y = row, z = plane; boxes 36 x 20 (tile + halo) and 32 x 16 (tile)
+        // 3-D tensor maps per case (x, y = row, z = plane): over the FP64 planes from the halo
+        // column -2 (x = column + 2), boxes 36 x 20 (tile + halo), 32 x 16 (tile) and
+        // 32 x 16 x 3 (three consecutive planes); over the FP32 correction planes from column
+        // -4 (x = column + 4, so both boxes start on 16-byte boundaries), 40 x 20 and 32 x 16
         EncodeTiledFn enc = tensor_map_encoder();
         if (!enc) return cleanup(fail(CFD_E_CUDA, "cuTensorMapEncodeTiled unavailable"));
-        std::vector<unsigned char> maps((size_t)256 * ncases);
+        std::vector<unsigned char> maps((size_t)TMAP_STRIDE * ncases);
         for (int c = 0; c < ncases; c++) {
             const CaseDev& d = b->hc[c];
-            void* gaddr = b->f64 + d.base + H - 2;
-            const cuuint64_t dims[3] = {(cuuint64_t)d.ld, (cuuint64_t)d.n1, (cuuint64_t)NPLANES};
-            const cuuint64_t strides[2] = {(cuuint64_t)d.ld * 8, (cuuint64_t)d.ps * 8};
-            const cuuint32_t box0[3] = {TX + 4, TYJ + 4, 1}, box1[3] = {TX, TYJ, 1}, es[3] = {1, 1, 1};
-            CUtensorMap* m = reinterpret_cast<CUtensorMap*>(maps.data() + (size_t)256 * c);
-            for (int k = 0; k < 2; k++) {
-                CUresult r = enc(m + k, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, gaddr, dims, strides, k ? box1 : box0, es,
-                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-                if (r != CUDA_SUCCESS)
-                    return cleanup(fail(CFD_E_CUDA, "cuTensorMapEncodeTiled failed for case " + std::to_string(c)));
-            }
+            unsigned char* mc = maps.data() + (size_t)TMAP_STRIDE * c;
+            const cuuint32_t es[3] = {1, 1, 1};
+            auto make = [&](int off, CUtensorMapDataType ty, void* gaddr, const cuuint64_t* dims,
+                            const cuuint64_t* strides, const cuuint32_t* box) {
+                return enc(reinterpret_cast<CUtensorMap*>(mc + off), ty, 3, gaddr, dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            };
+            const cuuint64_t d64[3] = {(cuuint64_t)d.ld, (cuuint64_t)d.n1, (cuuint64_t)NPLANES};
+            const cuuint64_t s64[2] = {(cuuint64_t)d.ld * 8, (cuuint64_t)d.ps * 8};
+            const cuuint32_t bh[3] = {TX + 4, TYJ + 4, 1}, bt[3] = {TX, TYJ, 1}, bt3[3] = {TX, TYJ, 3};
+            const cuuint64_t d32[3] = {(cuuint64_t)d.xld, (cuuint64_t)d.n1, (cuuint64_t)NXPLANES};
+            const cuuint64_t s32[2] = {(cuuint64_t)d.xld * 4, (cuuint64_t)d.xps * 4};
+            const cuuint32_t xh[3] = {TX + 8, TYJ + 4, 1};
+            void* g64 = b->f64 + d.base + H - 2;
+            void* g32 = b->f32 + d.xbase;
+            CUresult r = make(TMAP_F64_HALO, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, g64, d64, s64, bh);
+            if (r == CUDA_SUCCESS) r = make(TMAP_F64_TILE, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, g64, d64, s64, bt);
+            if (r == CUDA_SUCCESS) r = make(TMAP_F64_TILE3, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, g64, d64, s64, bt3);
+            if (r == CUDA_SUCCESS) r = make(TMAP_X32_HALO, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g32, d32, s32, xh);
+            if (r == CUDA_SUCCESS) r = make(TMAP_X32_TILE, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g32, d32, s32, bt);
+            if (r != CUDA_SUCCESS)
+                return cleanup(fail(CFD_E_CUDA, "cuTensorMapEncodeTiled failed for case " + std::to_string(c)));
         }
         CK(cudaMemcpy(b->dtmaps, maps.data(), maps.size(), cudaMemcpyHostToDevice));
     }
     bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
     bd.jtiles = b->dtiles + pos_jt; bd.njtiles = (int)jtiles.size();
     bd.error = b->flags + 4;
+    bd.sweep_no = b->flags + 7;
     for (int l = 0; l < MAXLEV; l++) {
         bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
         bd.mtiles[l] = b->dtiles + pos_mt[l]; bd.nmtiles[l] = (int)mt[l].size();
@@ -1005,6 +1054,7 @@ int cfd_batch_admit(cfd_batch* b, int slot, const cfd_grid* g, const cfd_params*
     const CaseDev& d = b->hc[slot];
     if (g->n0 != d.n0 || g->n1 != d.n1 || p->profile != d.profile)
         return fail(CFD_E_ARG, "case does not match the slot's geometry (n0, n1, profile)");
+    if (p->precision != b->precision) return fail(CFD_E_ARG, "case precision differs from the batch's");
     CK(cudaStreamSynchronize(b->st));
     return upload_case(b, slot, *g, *p, true);
 }

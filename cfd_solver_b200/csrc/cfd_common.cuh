@@ -50,6 +50,19 @@ enum MgPlane { M_AP, M_AE, M_AW, M_AN, M_AS, M_ANE, M_ANW, M_ASE, M_ASW, M_X, M_
 // momentum / energy systems solved each step
 enum Field { F_U, F_V, F_T, F_UP, F_VP, NFIELD };
 
+// FP32 planes of the precision form (per case, after its multigrid levels): the two
+// correction buffers and the FP32 residual of each of the five systems. Column i of
+// row j of plane k sits at f32[c.xbase + k * c.xps + j * c.xld + H32 + i]; the 4
+// columns left of column 0 keep every tensor box of these planes 16-byte aligned.
+enum MxPlane { X_DA = 0, X_DB = NFIELD, X_R = 2 * NFIELD, NXPLANES = 3 * NFIELD };
+constexpr int H32 = 4;
+
+// per-case CUtensorMaps (128 bytes each) in BatchDev::tmaps, TMAP_STRIDE bytes per case:
+// FP64 planes with x = column + 2: box 36 x 20 (tile + 2-cell halo), box 32 x 16 (tile),
+// box 32 x 16 x 3 planes; FP32 correction planes with x = column + 4: box 40 x 20, 32 x 16
+constexpr int TMAP_F64_HALO = 0, TMAP_F64_TILE = 128, TMAP_F64_TILE3 = 256, TMAP_X32_HALO = 384,
+              TMAP_X32_TILE = 512, TMAP_STRIDE = 640;
+
 // per-case scalar slots (FP64) of the pressure solve and step statistics
 enum Scalar {
     S_RHO, S_ALPHA, S_OMEGA, S_BETA, S_NB1, S_RL1, S_RL1_0,
@@ -89,6 +102,8 @@ struct CaseDev {
     int tile_begin, tile_count;     // fine-grid tiles of this case
     int jt_begin, jt_count;         // 32 x 16 tiles of this case (u/v/T sweeps)
     int nlev;
+    int xld;                        // FP32 precision-form planes: pitch, base, stride
+    long long xbase, xps;
     int fix_T_annw, fix_circ_de, warm_up;
     double d0, d1, dt, Re, Pr, Ri, F;
     double uinf, vinf, speed_amp, accn_amp, Pi, ar, omega_p, lid_u, sa, ca;
@@ -114,6 +129,7 @@ struct BatchDev {
     int* active;           // global count of cases still iterating (pressure)
     int* mactive;          // global count of (case, field) pairs still iterating (momentum)
     int* error;            // set when a bounded wait in a kernel gives up
+    int* sweep_no;         // momentum sweep launches of the current step (k_sweep_fin counts)
     const Tile* ftiles;    // fine-grid tiles of every case (FP64 kernels, multigrid level 0)
     int nftiles;
     const Tile* jtiles;    // 32 x 16 tiles of every case (u/v/T sweeps)
@@ -125,8 +141,7 @@ struct BatchDev {
     const int* ccases[MAXLEV];    // cases whose coarsest level is l
     int nccases[MAXLEV];
     unsigned long long* work;  // [0] field-cells and [1] cells swept by k_jac, [2] field-cells of sweep 0
-    const char* tmaps;     // per case two 128-byte CUtensorMaps over its FP64 planes (x, y, plane):
-                           // [0] box 36 x 20 (tile + 2-cell halo), [1] box 32 x 16 (tile)
+    const char* tmaps;     // per case TMAP_STRIDE bytes of CUtensorMaps (TMAP_* offsets)
     int cur;               // which of T0/T1 (up0/up1, vp0/vp1) holds the current state
 };
 
@@ -136,6 +151,9 @@ __device__ __forceinline__ double* plane(const BatchDev& b, const CaseDev& c, in
 }
 __device__ __forceinline__ float* mplane(const BatchDev& b, const LevelDev& L, int k) {
     return b.f32 + L.base + (long long)k * L.ps + H;
+}
+__device__ __forceinline__ float* xplane(const BatchDev& b, const CaseDev& c, int k) {
+    return b.f32 + c.xbase + (long long)k * c.xps + H32;
 }
 
 // periodic halo mirror of column i (or -1 if none)

@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(NT, 2) k_rhs(BatchDev b) {
     if (tid == 0) {
         mbar_init(&bar, 1);
         fence_mbar_init();
-        const char* maps = b.tmaps + (size_t)t.c * 256;
+        const char* maps = b.tmaps + (size_t)t.c * TMAP_STRIDE;
         mbar_arrive_expect_tx(&bar, (RHS_HALO * JTW * JTH + RHS_INT * TX * TYJ) * sizeof(double));
         const int hp[RHS_HALO] = {P_U, P_V, P_T0 + cur, P_P, P_UP0 + cur, P_VP0 + cur};
         const int ip[RHS_INT] = {P_XIX, P_XIY, P_ETX, P_ETY, P_ALPH, P_GAM, P_BETA};
@@ -371,212 +371,6 @@ __global__ void __launch_bounds__(NT, 2) k_rhs(BatchDev b) {
 }
 
 // ---------------------------------------------------------------------------
-// one Chebyshev-accelerated Jacobi sweep of the five momentum / energy systems
-// (replaces gauss(), PSolver.cpp:2280-2446). With the Jacobi value
-// xJ = (rhs - sum_nb a_nb x_k) / ap the three-term recurrence is
-//     x_{k+1} = w_{k+1} (x_k + g (xJ - x_k) - x_{k-1}) + x_{k-1},  g = 2 / (a + b),
-// w_1 = 1, w_2 = 1 / (1 - 1 / (2 s^2)), w_{k+1} = 1 / (1 - w_k / (4 s^2)), s = (b + a) / (b - a),
-// for eigenvalues of D^-1 A in [a, b] (bounds computed per case on the host).
-// x_{k+1} overwrites x_{k-1} in place, so the iterates ping-pong between the
-// solution buffer A and the scratch B; sweeps come in pairs and end in A. The stop
-// rule is the reference's: the relative L1 residual before a sweep below tol_mom (or
-// the absolute floor atol_mom) ends the solve after that sweep.
-//
-// A CTA owns a 32 x 16 tile (two cells per thread). For each active field the tile of
-// x_k plus its 2-cell halo is brought into shared memory by bulk asynchronous copies
-// (one per row, completed on an mbarrier), double-buffered so the next field's tile
-// streams in while this one is swept. The 25-point operator has 10 distinct
-// coefficients (PSolver.cpp:791-848), built in registers from alpha, beta, gamma.
-
-// Per cell the operator is fixed by E = dt alpha/(Re dxi0^2), G = dt gamma/(Re dxi1^2) and
-// B = dt beta/(Re dxi0 dxi1): 4th-order rows (PSolver.cpp:791-821) have
-//   ae = aw = -4/3 E, aee = aww = E/12, an = as = -4/3 G, ann = ass = G/12,
-//   ane = asw = 8/9 B, anw = ase = -8/9 B, annee = assww = B/72, annww = assee = -B/72,
-//   anne = assw = anee = asww = -B/9, annw = asse = anww = asee = B/9, ap = 1 + 5/2 (E + G);
-// 9-point rows (PSolver.cpp:766-775): ae = aw = -E, an = as = -G, ane = asw = B/2,
-// anw = ase = -B/2, ap = 1 + 2 (E + G), with the wall-row couplings folded out on the
-// O-grid (PSolver.cpp:851-882). The T system divides E, G, B by Pr.
-struct CellOp {
-    double E, G, B;
-    unsigned char nearw, drop_s, drop_n;
-};
-
-__device__ __forceinline__ void cell_op(const CaseDev& c, double al, double be, double ga, int i, int j,
-                                        CellOp& o) {
-    const double dt = c.dt, Re = c.Re;
-    o.E = dt * al / (Re * c.d0 * c.d0);
-    o.G = dt * ga / (Re * c.d1 * c.d1);
-    o.B = dt * be / (Re * c.d0 * c.d1);
-    o.nearw = near_wall(c, i, j);
-    o.drop_s = c.profile == OGRID && j == 1;
-    o.drop_n = c.profile == OGRID && j == c.n1 - 2;
-}
-
-// off-centre sum of the operator on the shared-memory tile, u-type scaling
-__device__ __forceinline__ double tile_sum(const double* S, int o, const CellOp& a) {
-    constexpr int R = JTW, R2 = 2 * JTW;
-    if (a.nearw) {
-        double s = -a.E * (S[o + 1] + S[o - 1]);
-        double n = -a.G * S[o + R] + 0.5 * a.B * (S[o + R + 1] - S[o + R - 1]);
-        double so = -a.G * S[o - R] + 0.5 * a.B * (S[o - R - 1] - S[o - R + 1]);
-        if (!a.drop_n) s += n;
-        if (!a.drop_s) s += so;
-        return s;
-    }
-    const double ex = (-4.0 / 3.0) * (S[o + 1] + S[o - 1]) + (1.0 / 12.0) * (S[o + 2] + S[o - 2]);
-    const double gy = (-4.0 / 3.0) * (S[o + R] + S[o - R]) + (1.0 / 12.0) * (S[o + R2] + S[o - R2]);
-    const double bx = (8.0 / 9.0) * (S[o + R + 1] + S[o - R - 1] - S[o + R - 1] - S[o - R + 1]) +
-                      (1.0 / 72.0) * (S[o + R2 + 2] + S[o - R2 - 2] - S[o + R2 - 2] - S[o - R2 + 2]) +
-                      (1.0 / 9.0) * (S[o + R2 - 1] + S[o - R2 + 1] + S[o + R - 2] + S[o - R + 2] -
-                                     S[o + R2 + 1] - S[o - R2 - 1] - S[o + R + 2] - S[o - R - 2]);
-    return a.E * ex + a.G * gy + a.B * bx;
-}
-
-// shared memory per field: x_k tile with halo, rhs tile, x_{k-1} tile (each 128-byte aligned)
-constexpr int JT_FIELD = JTW * JTH + 2 * TX * TYJ;
-constexpr size_t JAC_SMEM = (size_t)NFIELD * JT_FIELD * sizeof(double) + 128;
-const size_t kJacSmem = JAC_SMEM;
-
-__global__ void __launch_bounds__(NT, 3) k_jac(BatchDev b) {
-    extern __shared__ __align__(128) unsigned char jraw[];
-    __shared__ __align__(8) uint64_t bar[NFIELD];
-    double* jsm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(jraw) + 127) & ~uintptr_t(127));
-    const Tile t = b.jtiles[blockIdx.x];
-    const CaseDev& c = b.cases[t.c];
-    const int* isc = b.iscal + (long long)t.c * NISCAL;
-    int mask = 0, sweep = 0;
-#pragma unroll
-    for (int f = 0; f < NFIELD; f++) mask |= (isc[I_MDONE0 + f] == 0) << f;
-    if (mask == 0) return;  // uniform over the case's CTAs
-    // the case's sweep index: every still-active field has done the same number of sweeps;
-    // even sweeps go A -> B, odd sweeps B -> A and decide the stop
-    sweep = isc[I_MIT0 + (__ffs(mask) - 1)];
-    const int to_scratch = (sweep & 1) == 0, decide = sweep & 1;
-    const int tid = threadIdx.x;
-    const int ld = c.ld, n1 = c.n1;
-    const int nxt = b.cur ^ 1;
-    const bool need_prev = sweep > 0;
-    if (tid == 0) {
-#pragma unroll
-        for (int f = 0; f < NFIELD; f++) mbar_init(&bar[f], 1);
-        fence_mbar_init();
-        // every active field's tiles in flight at once: three tensor loads per field
-        // (x_k with halo, rhs, x_{k-1}); tensor x coordinate = column + 2, y = row, z = plane
-        const char* maps = b.tmaps + (size_t)t.c * 256;
-        const unsigned bytes = (JTW * JTH + TX * TYJ * (need_prev ? 2 : 1)) * sizeof(double);
-        for (int f = 0; f < NFIELD; f++) {
-            if (!(mask & (1 << f))) continue;
-            const int pa = f < 2 ? P_US + f : P_T0 + 2 * (f - 2) + nxt;
-            double* sm = jsm + f * JT_FIELD;
-            mbar_arrive_expect_tx(&bar[f], bytes);
-            tma_load_3d(sm, maps, t.i0, t.j0 - 2, to_scratch ? pa : P_BU + f, &bar[f]);
-            tma_load_3d(sm + JTW * JTH, maps + 128, t.i0 + 2, t.j0, P_RU + f, &bar[f]);
-            if (need_prev)
-                tma_load_3d(sm + JTW * JTH + TX * TYJ, maps + 128, t.i0 + 2, t.j0, to_scratch ? P_BU + f : pa,
-                            &bar[f]);
-        }
-    }
-    __syncthreads();
-
-    const int li = tid % TX, lj = tid / TX;
-    const int i = t.i0 + li;
-    const int jA = t.j0 + lj, jB = jA + TY;
-    const bool inA = i >= c.ilo && i <= c.ihi && jA <= n1 - 2;
-    const bool inB = i >= c.ilo && i <= c.ihi && jB <= n1 - 2;
-    // operators of the two cells
-    CellOp A0, A1;
-    const long long kA = (long long)jA * ld + i, kB = (long long)jB * ld + i;
-    const double* AL = plane(b, c, P_ALPH);
-    const double* BE = plane(b, c, P_BETA);
-    const double* GA = plane(b, c, P_GAM);
-    if (inA) cell_op(c, AL[kA], BE[kA], GA[kA], i, jA, A0);
-    if (inB) cell_op(c, AL[kB], BE[kB], GA[kB], i, jB, A1);
-    const double* sc = b.scal + (long long)t.c * NSCAL;
-    const double g0 = 2.0 / (c.cheb_a[0] + c.cheb_b[0]), g1 = 2.0 / (c.cheb_a[1] + c.cheb_b[1]);
-    const double w0 = sweep == 0 ? 1.0 : sc[S_CW0], w1 = sweep == 0 ? 1.0 : sc[S_CW1];
-    const double rPr = 1.0 / c.Pr;
-    const bool tbug = !c.fix_T_annw;
-    const int oA = (lj + 2) * JTW + (li + 2), oB = oA + TY * JTW;
-
-    double r[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    bool ok = true;
-#pragma unroll
-    for (int f = 0; f < NFIELD; f++) {
-        if (!(mask & (1 << f))) continue;
-        ok = __syncthreads_and(mbar_wait_bounded(&bar[f], 0)) && ok;
-        if (!ok) continue;
-        const double* S = jsm + f * JT_FIELD;
-        const double* Rs = S + JTW * JTH;
-        const double* Ps = Rs + TX * TYJ;
-        const int pa = f < 2 ? P_US + f : P_T0 + 2 * (f - 2) + nxt;
-        double* dst = plane(b, c, to_scratch ? P_BU + f : pa);
-        const bool isT = f == F_T;
-        const double g = isT ? g1 : g0, w = isT ? w1 : w0;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const bool in = h ? inB : inA;
-            if (!in) continue;
-            const CellOp& a = h ? A1 : A0;
-            const int o = h ? oB : oA;
-            const int oi = (lj + h * TY) * TX + li;
-            double sum = tile_sum(S, o, a);
-            const double ratio = a.nearw ? 2.0 : 2.5;
-            double ap = 1.0 + ratio * (a.E + a.G);
-            if (isT) {
-                // the reference's T solve passes atnw in the annw slot (PSolver.cpp:1290):
-                // the (i-1, j+2) coefficient becomes anw = -8/9 B instead of B/9
-                if (tbug && !a.nearw) sum -= a.B * S[o + 2 * JTW - 1];
-                sum *= rPr;
-                ap = 1.0 + ratio * (a.E + a.G) * rPr;
-            }
-            const double rhs = Rs[oi], xk = S[o];
-            const double xj = (rhs - sum) / ap;
-            double xn = xk + g * (xj - xk);
-            if (need_prev) {
-                const double xm = Ps[oi];
-                xn = w * (xk + g * (xj - xk) - xm) + xm;
-            }
-            store_mirrored(dst, ld, i, h ? jB : jA, c.W, c.periodic, xn);
-            r[f] += fabs(rhs - ap * xk - sum);
-        }
-    }
-    if (!ok) {
-        if (tid == 0) atomicExch(b.error, 1);
-        // let copies still in flight land before the CTA leaves
-        for (int f = 0; f < NFIELD; f++)
-            if (mask & (1 << f)) mbar_wait_bounded(&bar[f], 0);
-    }
-    const int ncell = __syncthreads_count(inA) + __syncthreads_count(inB);
-    if (tid == 0) {  // algorithmic-traffic counters (cells and field-cells swept)
-        const unsigned long long nf = (unsigned long long)__popc(mask) * ncell;
-        atomicAdd(&b.work[0], nf);
-        atomicAdd(&b.work[1], (unsigned long long)ncell);
-        if (sweep == 0) atomicAdd(&b.work[2], nf);
-    }
-    if (case_reduce<NFIELD, 0u>(b, t.c, blockIdx.x, c.jt_begin, c.jt_count, r) && tid == 0) {
-        double* scw = b.scal + (long long)t.c * NSCAL;
-        int* is = b.iscal + (long long)t.c * NISCAL;
-        for (int f = 0; f < NFIELD; f++) {
-            if (!(mask & (1 << f))) continue;
-            if (sweep == 0) scw[S_MR0 + f] = (r[f] != 0.0) ? r[f] : 1.0;
-            scw[S_MR + f] = r[f];
-            is[I_MIT0 + f] += 1;
-            if (decide) {
-                bool done = (r[f] / scw[S_MR0 + f] < c.tol_mom) || (r[f] <= c.atol_mom);
-                if (!isfinite(r[f])) { is[I_STATUS] |= ST_NAN; done = true; }
-                if (done) { is[I_MDONE0 + f] = 1; atomicSub(b.mactive, 1); }
-            }
-        }
-        for (int ty = 0; ty < 2; ty++) {  // Chebyshev weight of the next sweep
-            const double a = c.cheb_a[ty], bb = c.cheb_b[ty];
-            const double s2 = ((bb + a) / (bb - a)) * ((bb + a) / (bb - a));
-            scw[S_CW0 + ty] = (sweep == 0) ? 1.0 / (1.0 - 1.0 / (2.0 * s2))
-                                           : 1.0 / (1.0 - scw[S_CW0 + ty] / (4.0 * s2));
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // up/vp far-field condition (PSolver.cpp:1356-1382), one CTA per O-grid case
 __global__ void __launch_bounds__(BC_THREADS) k_upbc(BatchDev b) {
     const CaseDev& c = b.cases[blockIdx.x];
@@ -623,7 +417,7 @@ __global__ void __launch_bounds__(NT, 3) k_face_q(BatchDev b) {
     if (tid == 0) {
         mbar_init(&bar, 1);
         fence_mbar_init();
-        const char* maps = b.tmaps + (size_t)t.c * 256;
+        const char* maps = b.tmaps + (size_t)t.c * TMAP_STRIDE;
         mbar_arrive_expect_tx(&bar, FQ_HALO * JTW * JTH * sizeof(double));
         const int hp[FQ_HALO] = {P_P, P_UP0 + nxt, P_VP0 + nxt, P_XIX, P_XIY, P_ETX, P_ETY};
         for (int m = 0; m < FQ_HALO; m++) tma_load_3d(sm + m * JTW * JTH, maps, t.i0, t.j0 - 2, hp[m], &bar);

@@ -5,8 +5,6 @@
 namespace cfd {
 __global__ void k_assemble_p(BatchDev b, int toff);
 __global__ void k_rhs(BatchDev b);
-__global__ void k_jac(BatchDev b);
-extern const size_t kJacSmem;  // dynamic shared memory of k_jac
 extern const size_t kRhsSmem;
 extern const size_t kFaceQSmem;
 __global__ void k_upbc(BatchDev b);

@@ -1,0 +1,441 @@
+// cfd_sweep.cu -- the Chebyshev-Jacobi sweeps of the five u/v/T/up/vp systems
+// (replacing gauss(), PSolver.cpp:2280-2446) as one persistent, pipelined kernel.
+//
+// One CTA sweeps one 32 x 16 tile of one case for all of its still-iterating fields.
+// The fields stream through two shared-memory buffers: each field's x tile with its
+// 2-cell halo, its right-hand side and (after the first sweep) the previous iterate
+// arrive by tensor copies completed on the buffer's mbarrier, and the copies of field
+// k+2 are issued as soon as field k has been read into registers, so they overlap the
+// arithmetic of field k and the wait for field k+1. The first field also brings alpha,
+// beta, gamma; every thread turns its own cells' values into the operator (E, G, B and
+// the two inverse diagonals) in place, in a thread-private part of shared memory that
+// needs no barrier and costs no registers.
+//
+// A warp owns four consecutive rows of the tile, a lane one column: the thread reads its
+// eight-row x five-column window once into registers, so its four cells cost ten
+// shared-memory loads each instead of twenty-five. The per-tile L1 residuals go to
+// per-warp partials that k_sweep_fin sums per case in a fixed order after the launch.
+//
+// Three modes share the code:
+//   SW_F64    FP64 iterates x_k (the plain path);
+//   SW_MX0    first sweep of the precision form: the residual r = rhs - A x0 in FP64
+//             from the FP64 iterate, stored as FP32 together with the first FP32
+//             correction d_1 = g D^-1 r;
+//   SW_MX     later sweeps of the precision form on the FP32 correction d_k for
+//             A d = r (x = x0 + d is formed by k_mom_update after the last sweep).
+// The stop rule is the reference's (relative L1 residual of the system before the
+// sweep, PSolver.cpp:2318-2330), evaluated with deterministic per-case reductions.
+//
+// Chebyshev acceleration: with the Jacobi value xJ = (rhs - sum_nb a_nb x_k) / ap the
+// three-term recurrence is
+//     x_{k+1} = w_{k+1} (x_k + g (xJ - x_k) - x_{k-1}) + x_{k-1},  g = 2 / (a + b),
+// w_1 = 1, w_2 = 1 / (1 - 1 / (2 s^2)), w_{k+1} = 1 / (1 - w_k / (4 s^2)), s = (b + a) / (b - a),
+// for eigenvalues of D^-1 A in [a, b] (bounds computed per case on the host).
+// x_{k+1} overwrites x_{k-1} in place, so the iterates ping-pong between the solution
+// buffer and the scratch; sweeps come in pairs and end in the solution buffer.
+//
+// Per cell the operator is fixed by E = dt alpha/(Re dxi0^2), G = dt gamma/(Re dxi1^2) and
+// B = dt beta/(Re dxi0 dxi1): 4th-order rows (PSolver.cpp:791-821) have
+//   ae = aw = -4/3 E, aee = aww = E/12, an = as = -4/3 G, ann = ass = G/12,
+//   ane = asw = 8/9 B, anw = ase = -8/9 B, annee = assww = B/72, annww = assee = -B/72,
+//   anne = assw = anee = asww = -B/9, annw = asse = anww = asee = B/9, ap = 1 + 5/2 (E + G);
+// 9-point rows (PSolver.cpp:766-775): ae = aw = -E, an = as = -G, ane = asw = B/2,
+// anw = ase = -B/2, ap = 1 + 2 (E + G), with the wall-row couplings folded out on the
+// O-grid (PSolver.cpp:851-882). The T system divides E, G, B by Pr.
+#include "cfd_bulk.cuh"
+#include "cfd_common.cuh"
+#include "cfd_reduce.cuh"
+#include "cfd_sweep.cuh"
+
+namespace cfd {
+
+namespace {
+
+template <int MODE>
+struct SwCfg;
+template <>
+struct SwCfg<SW_F64> {
+    using XT = double;  // x tile (with halo)
+    using RT = double;  // right-hand side / residual tile
+    using ST = double;  // arithmetic of the sweep
+    static constexpr int XW = TX + 4, XO = 2;  // halo tile row length, column of cell 0 in it
+    static constexpr bool PREV = true;
+};
+template <>
+struct SwCfg<SW_MX0> {
+    using XT = double;
+    using RT = double;
+    using ST = double;
+    static constexpr int XW = TX + 4, XO = 2;
+    static constexpr bool PREV = false;
+};
+template <>
+struct SwCfg<SW_MX> {
+    using XT = float;
+    using RT = float;
+    using ST = float;
+    static constexpr int XW = TX + 8, XO = 4;  // FP32 boxes start 4 columns left (16-byte x)
+    static constexpr bool PREV = true;
+};
+
+constexpr int SW_HALO_ROWS = TYJ + 4;
+constexpr int SW_CELLS = TX * TYJ;
+constexpr int align128(int x) { return (x + 127) / 128 * 128; }
+
+// shared-memory layout: two field buffers, then alpha/beta/gamma (FP64, 3 planes) which
+// every thread overwrites with its cells' operator (5 planes of ST: E, G, B, 1/ap_u,
+// 1/ap_T) -- in place for FP64, behind them for FP32 (4-byte slots would overlap other
+// threads' unread 8-byte inputs)
+template <int MODE>
+struct SwLayout {
+    using C = SwCfg<MODE>;
+    static constexpr unsigned XBYTES = C::XW * SW_HALO_ROWS * sizeof(typename C::XT);
+    static constexpr unsigned RBYTES = SW_CELLS * sizeof(typename C::RT);
+    static constexpr unsigned PBYTES = SW_CELLS * sizeof(typename C::XT);
+    static constexpr unsigned MBYTES = 3 * SW_CELLS * sizeof(double);
+    static constexpr int X = 0;
+    static constexpr int RHS = align128(XBYTES);
+    static constexpr int PREV = RHS + align128(RBYTES);
+    static constexpr int BUF = PREV + (C::PREV ? align128(PBYTES) : 0);
+    static constexpr int MET = 2 * BUF;
+    static constexpr int OPS = sizeof(typename C::ST) == 8 ? MET : MET + (int)MBYTES;
+    static constexpr int TOTAL = OPS + 5 * SW_CELLS * (int)sizeof(typename C::ST);
+};
+
+// FP64 plane of field f's iterate for state parity nxt (u*, v*, T, up, vp)
+__device__ __forceinline__ int sw_iter_plane(int f, int nxt) { return f < 2 ? P_US + f : P_T0 + 2 * (f - 2) + nxt; }
+
+// issue the tensor copies of field f of tile t into buffer `sm` (with alpha, beta, gamma)
+template <int MODE>
+__device__ __forceinline__ void sw_issue(const Tile& t, int f, int sweep, int nxt, const char* maps,
+                                         unsigned char* sm, unsigned char* met, uint64_t* bar) {
+    using L = SwLayout<MODE>;
+    const int pa = sw_iter_plane(f, nxt);
+    unsigned bytes = L::XBYTES + L::RBYTES + (met ? L::MBYTES : 0u);
+    bool prev = false;
+    int xs = 0, ps = 0;
+    if (MODE == SW_F64) {
+        const int to_scratch = (sweep & 1) == 0;
+        xs = to_scratch ? pa : P_BU + f;
+        ps = to_scratch ? P_BU + f : pa;
+        prev = sweep > 0;
+    } else if (MODE == SW_MX0) {
+        xs = pa;
+    } else {
+        const int to_scratch = (sweep & 1) == 0;
+        xs = to_scratch ? X_DA + f : X_DB + f;
+        ps = to_scratch ? X_DB + f : X_DA + f;
+        prev = sweep > 1;
+    }
+    if (prev) bytes += L::PBYTES;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, bytes);
+    if (MODE == SW_MX) {
+        tma_load_3d(sm + L::X, maps + TMAP_X32_HALO, t.i0, t.j0 - 2, xs, bar);
+        tma_load_3d(sm + L::RHS, maps + TMAP_X32_TILE, t.i0 + 4, t.j0, X_R + f, bar);
+        if (prev) tma_load_3d(sm + L::PREV, maps + TMAP_X32_TILE, t.i0 + 4, t.j0, ps, bar);
+    } else {
+        tma_load_3d(sm + L::X, maps + TMAP_F64_HALO, t.i0, t.j0 - 2, xs, bar);
+        tma_load_3d(sm + L::RHS, maps + TMAP_F64_TILE, t.i0 + 2, t.j0, P_RU + f, bar);
+        if (prev) tma_load_3d(sm + L::PREV, maps + TMAP_F64_TILE, t.i0 + 2, t.j0, ps, bar);
+    }
+    // alpha, beta, gamma: three consecutive planes in one box
+    if (met) tma_load_3d(met, maps + TMAP_F64_TILE3, t.i0 + 2, t.j0, P_ALPH, bar);
+}
+
+// off-centre sum of the u-type operator for the cell whose window centre row is `r0 + 2`
+template <typename ST>
+__device__ __forceinline__ ST sw_sum(const ST (&w)[8][5], int r0, ST E, ST G, ST B, bool nearw, bool drop_s,
+                                     bool drop_n) {
+#define WX(dy, dx) w[r0 + 2 + (dy)][2 + (dx)]
+    if (nearw) {
+        ST s = -E * (WX(0, 1) + WX(0, -1));
+        const ST n = -G * WX(1, 0) + ST(0.5) * B * (WX(1, 1) - WX(1, -1));
+        const ST so = -G * WX(-1, 0) + ST(0.5) * B * (WX(-1, -1) - WX(-1, 1));
+        if (!drop_n) s += n;
+        if (!drop_s) s += so;
+        return s;
+    }
+    const ST ex = ST(-4.0 / 3.0) * (WX(0, 1) + WX(0, -1)) + ST(1.0 / 12.0) * (WX(0, 2) + WX(0, -2));
+    const ST gy = ST(-4.0 / 3.0) * (WX(1, 0) + WX(-1, 0)) + ST(1.0 / 12.0) * (WX(2, 0) + WX(-2, 0));
+    const ST bx = ST(8.0 / 9.0) * (WX(1, 1) + WX(-1, -1) - WX(1, -1) - WX(-1, 1)) +
+                  ST(1.0 / 72.0) * (WX(2, 2) + WX(-2, -2) - WX(2, -2) - WX(-2, 2)) +
+                  ST(1.0 / 9.0) * (WX(2, -1) + WX(-2, 1) + WX(1, -2) + WX(-1, 2) - WX(2, 1) - WX(-2, -1) -
+                                   WX(1, 2) - WX(-1, -2));
+    return E * ex + G * gy + B * bx;
+#undef WX
+}
+
+template <int MODE>
+__device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm, uint64_t* bar) {
+    using C = SwCfg<MODE>;
+    using L = SwLayout<MODE>;
+    using XT = typename C::XT;
+    using RT = typename C::RT;
+    using ST = typename C::ST;
+    const Tile t = b.jtiles[blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    const int* isc = b.iscal + (long long)t.c * NISCAL;
+    int mask = 0;
+#pragma unroll
+    for (int f = 0; f < NFIELD; f++) mask |= (isc[I_MDONE0 + f] == 0) << f;
+    if (mask == 0) return;  // uniform over the case's CTAs
+    // every still-active field of the case has done the same number of sweeps
+    const int sweep = isc[I_MIT0 + (__ffs(mask) - 1)];
+    const int tid = threadIdx.x, lane = tid & 31, wrp = tid >> 5;
+    const int nxt = b.cur ^ 1;
+    int fl[NFIELD];
+    int nf = 0;
+#pragma unroll
+    for (int f = 0; f < NFIELD; f++)
+        if (mask & (1 << f)) fl[nf++] = f;
+    const char* maps = b.tmaps + (size_t)t.c * TMAP_STRIDE;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+        sw_issue<MODE>(t, fl[0], sweep, nxt, maps, sm, sm + L::MET, &bar[0]);
+        if (nf > 1) sw_issue<MODE>(t, fl[1], sweep, nxt, maps, sm + L::BUF, nullptr, &bar[1]);
+    }
+    // per-case constants (uniform)
+    const double* sc = b.scal + (long long)t.c * NSCAL;
+    const bool weighted = MODE == SW_MX ? true : sweep > 0;
+    const bool has_prev = MODE == SW_MX ? sweep > 1 : (MODE == SW_F64 && sweep > 0);
+    const ST gU = (ST)(2.0 / (c.cheb_a[0] + c.cheb_b[0])), gT = (ST)(2.0 / (c.cheb_a[1] + c.cheb_b[1]));
+    const ST wU = weighted ? (ST)sc[S_CW0] : ST(1), wT = weighted ? (ST)sc[S_CW1] : ST(1);
+    const double rPr64 = 1.0 / c.Pr;
+    const ST rPr = (ST)rPr64;
+    const int ld = c.ld, xld = c.xld, W = c.W, per = c.periodic;
+    const int i = t.i0 + lane;
+    bool inq[SW_ROWS], nearw[SW_ROWS], drop_s[SW_ROWS], drop_n[SW_ROWS];
+#pragma unroll
+    for (int q = 0; q < SW_ROWS; q++) {
+        const int j = t.j0 + wrp * SW_ROWS + q;
+        inq[q] = i >= c.ilo && i <= c.ihi && j <= c.n1 - 2;
+        nearw[q] = j == 1 || j == c.n1 - 2 || (c.profile == CAVITY && (i == 1 || i == c.n0 - 2));
+        drop_s[q] = c.profile == OGRID && j == 1;
+        drop_n[q] = c.profile == OGRID && j == c.n1 - 2;
+    }
+    __syncthreads();
+
+    ST* OPS = reinterpret_cast<ST*>(sm + L::OPS);
+    double r[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    bool ok = true;
+    int k = 0;
+    for (; k < nf; k++) {
+        const int bi = k & 1;
+        ok = __syncthreads_and(mbar_wait_bounded(&bar[bi], (k >> 1) & 1)) && ok;
+        if (!ok) break;
+        const unsigned char* buf = sm + bi * L::BUF;
+        if (k == 0) {
+            // alpha, beta, gamma of the thread's own cells -> E, G, B, 1/ap_u, 1/ap_T
+            const double* MET = reinterpret_cast<const double*>(sm + L::MET);
+            const double kE = c.dt / (c.Re * c.d0 * c.d0), kG = c.dt / (c.Re * c.d1 * c.d1),
+                         kB = c.dt / (c.Re * c.d0 * c.d1);
+#pragma unroll
+            for (int q = 0; q < SW_ROWS; q++) {
+                const int o = (wrp * SW_ROWS + q) * TX + lane;
+                const double E = kE * MET[o], B = kB * MET[SW_CELLS + o], G = kG * MET[2 * SW_CELLS + o];
+                const double D = (nearw[q] ? 2.0 : 2.5) * (E + G);
+                OPS[o] = (ST)E;
+                OPS[SW_CELLS + o] = (ST)G;
+                OPS[2 * SW_CELLS + o] = (ST)B;
+                OPS[3 * SW_CELLS + o] = (ST)(1.0 / (1.0 + D));
+                OPS[4 * SW_CELLS + o] = (ST)(1.0 / (1.0 + D * rPr64));
+            }
+        }
+        const int f = fl[k];
+        const bool isT = f == F_T;
+        const XT* X = reinterpret_cast<const XT*>(buf + L::X);
+        const RT* R = reinterpret_cast<const RT*>(buf + L::RHS);
+        const XT* P = reinterpret_cast<const XT*>(buf + L::PREV);
+        // the thread's window: rows wrp*4 - 2 .. wrp*4 + 5, columns lane - 2 .. lane + 2
+        ST w[8][5];
+        ST rhs[SW_ROWS], xm[SW_ROWS];
+#pragma unroll
+        for (int q = 0; q < SW_ROWS; q++) {
+            const int o = (wrp * SW_ROWS + q) * TX + lane;
+            rhs[q] = (ST)R[o];
+            xm[q] = has_prev ? (ST)P[o] : ST(0);
+        }
+#pragma unroll
+        for (int rr = 0; rr < 8; rr++)
+#pragma unroll
+            for (int cl = 0; cl < 5; cl++) w[rr][cl] = (ST)X[(wrp * SW_ROWS + rr) * C::XW + lane + cl + C::XO - 2];
+        __syncthreads();  // the buffer has been read: refill it with field k+2
+        if (tid == 0 && k + 2 < nf) sw_issue<MODE>(t, fl[k + 2], sweep, nxt, maps, sm + bi * L::BUF, nullptr, &bar[bi]);
+
+        const ST g = isT ? gT : gU, wgt = isT ? wT : wU;
+        const bool tbug = isT && !c.fix_T_annw;
+        double* dst64 = nullptr;
+        float* dst32 = nullptr;
+        float* res32 = nullptr;
+        if (MODE == SW_F64) {
+            dst64 = plane(b, c, (sweep & 1) == 0 ? P_BU + f : sw_iter_plane(f, nxt));
+        } else if (MODE == SW_MX0) {
+            dst32 = xplane(b, c, X_DB + f);
+            res32 = xplane(b, c, X_R + f);
+        } else {
+            dst32 = xplane(b, c, (sweep & 1) == 0 ? X_DB + f : X_DA + f);
+        }
+        double racc = 0.0;
+#pragma unroll
+        for (int q = 0; q < SW_ROWS; q++) {
+            if (!inq[q]) continue;
+            const int o = (wrp * SW_ROWS + q) * TX + lane;
+            const ST E = OPS[o], G = OPS[SW_CELLS + o], B = OPS[2 * SW_CELLS + o];
+            ST sum = sw_sum<ST>(w, q, E, G, B, nearw[q], drop_s[q], drop_n[q]);
+            const ST D = (nearw[q] ? ST(2) : ST(2.5)) * (E + G);
+            ST ap, rap;
+            if (isT) {
+                // the reference's T solve passes atnw in the annw slot (PSolver.cpp:1290):
+                // the (i-1, j+2) coefficient becomes anw = -8/9 B instead of B/9
+                if (tbug && !nearw[q]) sum -= B * w[q + 4][1];
+                sum *= rPr;
+                ap = ST(1) + D * rPr;
+                rap = OPS[4 * SW_CELLS + o];
+            } else {
+                ap = ST(1) + D;
+                rap = OPS[3 * SW_CELLS + o];
+            }
+            const ST xk = w[q + 2][2];
+            const ST res = rhs[q] - ap * xk - sum;
+            racc += fabs((double)res);
+            const int j = t.j0 + wrp * SW_ROWS + q;
+            if (MODE == SW_MX0) {
+                store_mirrored(dst32, xld, i, j, W, per, (float)(g * res * rap));
+                store_mirrored(res32, xld, i, j, W, per, (float)res);
+            } else {
+                ST xn = xk + g * res * rap;
+                if (weighted) xn = wgt * (xn - xm[q]) + xm[q];
+                if (MODE == SW_F64) store_mirrored(dst64, ld, i, j, W, per, (double)xn);
+                else store_mirrored(dst32, xld, i, j, W, per, (float)xn);
+            }
+        }
+#pragma unroll
+        for (int ff = 0; ff < NFIELD; ff++)
+            if (ff == f) r[ff] += racc;
+    }
+    if (!ok) {
+        if (tid == 0) {
+            atomicExch(b.error, 1);
+            // let the copies still in flight land before the CTA leaves
+            for (int m = k; m < nf && m < k + 2; m++) mbar_wait_bounded(&bar[m & 1], (m >> 1) & 1);
+        }
+        return;
+    }
+    // the warp's partial L1 residuals of this tile (summed per case by k_sweep_fin)
+#pragma unroll
+    for (int ff = 0; ff < NFIELD; ff++) {
+        double x = r[ff];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        r[ff] = x;
+    }
+    if (lane == 0) {
+        double* dstp = b.partial + ((long long)blockIdx.x * SW_WARPS + wrp) * PSTRIDE;
+#pragma unroll
+        for (int ff = 0; ff < NFIELD; ff++) dstp[ff] = r[ff];
+    }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(SW_THREADS, 4) k_sweep_f64(BatchDev b) {
+    extern __shared__ __align__(128) unsigned char swraw[];
+    __shared__ __align__(8) uint64_t bar[2];
+    unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(swraw) + 127) & ~uintptr_t(127));
+    sweep_tile<SW_F64>(b, sm, bar);
+}
+
+// precision form: every still-iterating field of every case is at the same sweep index
+// within one launch (all start at 0 together, one sweep per launch), so the launch runs
+// either the FP64 residual sweep (the step's first launch) or the FP32 correction sweeps
+__global__ void __launch_bounds__(SW_THREADS, 4) k_sweep_mx(BatchDev b) {
+    extern __shared__ __align__(128) unsigned char swraw[];
+    __shared__ __align__(8) uint64_t bar[2];
+    unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(swraw) + 127) & ~uintptr_t(127));
+    if (*b.sweep_no == 0) sweep_tile<SW_MX0>(b, sm, bar);
+    else sweep_tile<SW_MX>(b, sm, bar);
+}
+
+// per case after every sweep launch: sum the tile partials in a fixed order, count the
+// sweep, decide the stop (after odd sweeps) and advance the Chebyshev weights
+__global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
+    __shared__ double red[NFIELD * 32];
+    const int cid = blockIdx.x;
+    const CaseDev& c = b.cases[cid];
+    int* is = b.iscal + (long long)cid * NISCAL;
+    int mask = 0;
+#pragma unroll
+    for (int f = 0; f < NFIELD; f++) mask |= (is[I_MDONE0 + f] == 0) << f;
+    if (cid == 0 && threadIdx.x == 0) atomicAdd(b.sweep_no, 1);  // read by the next sweep launch
+    if (!mask) return;
+    const int tid = threadIdx.x;
+    double v[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const int np = c.jt_count * SW_WARPS;
+    for (int e = tid; e < np; e += SWF_THREADS) {
+        const double* src = b.partial + ((long long)c.jt_begin * SW_WARPS + e) * PSTRIDE;
+#pragma unroll
+        for (int f = 0; f < NFIELD; f++) v[f] += src[f];
+    }
+    block_sum<NFIELD>(v, red);
+    if (tid != 0) return;
+    double* scw = b.scal + (long long)cid * NSCAL;
+    const int sweep = is[I_MIT0 + (__ffs(mask) - 1)];
+    const int decide = sweep & 1;
+    for (int f = 0; f < NFIELD; f++) {
+        if (!(mask & (1 << f))) continue;
+        if (sweep == 0) scw[S_MR0 + f] = (v[f] != 0.0) ? v[f] : 1.0;
+        scw[S_MR + f] = v[f];
+        is[I_MIT0 + f] += 1;
+        if (decide) {
+            bool done = (v[f] / scw[S_MR0 + f] < c.tol_mom) || (v[f] <= c.atol_mom);
+            if (!isfinite(v[f])) {
+                is[I_STATUS] |= ST_NAN;
+                done = true;
+            }
+            if (done) {
+                is[I_MDONE0 + f] = 1;
+                atomicSub(b.mactive, 1);
+            }
+        }
+    }
+    for (int ty = 0; ty < 2; ty++) {  // Chebyshev weight of the next sweep
+        const double ca = c.cheb_a[ty], cb = c.cheb_b[ty];
+        const double s2 = ((cb + ca) / (cb - ca)) * ((cb + ca) / (cb - ca));
+        scw[S_CW0 + ty] = (sweep == 0) ? 1.0 / (1.0 - 1.0 / (2.0 * s2)) : 1.0 / (1.0 - scw[S_CW0 + ty] / (4.0 * s2));
+    }
+    // algorithmic-traffic counters (cells and field-cells swept)
+    const unsigned long long ncell = (unsigned long long)(c.ihi - c.ilo + 1) * (c.n1 - 2);
+    const unsigned long long nf = (unsigned long long)__popc(mask) * ncell;
+    atomicAdd(&b.work[0], nf);
+    atomicAdd(&b.work[1], ncell);
+    if (sweep == 0) atomicAdd(&b.work[2], nf);
+}
+
+size_t sweep_smem_f64() { return (size_t)SwLayout<SW_F64>::TOTAL + 128; }
+size_t sweep_smem_mx() { return (size_t)max(SwLayout<SW_MX0>::TOTAL, SwLayout<SW_MX>::TOTAL) + 128; }
+
+// x0 += d for every field of the precision form (after the last sweep, d_final in X_DA)
+__global__ void __launch_bounds__(NT) k_mom_update(BatchDev b) {
+    const Tile t = b.ftiles[blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    if (!b.iscal[(long long)t.c * NISCAL + I_ACTIVE]) return;  // uniform over the case
+    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
+    const int nxt = b.cur ^ 1;
+    const long long k = (long long)j * c.ld + i, kx = (long long)j * c.xld + i;
+    double x[NFIELD];
+    float d[NFIELD];
+#pragma unroll
+    for (int f = 0; f < NFIELD; f++) {
+        x[f] = plane(b, c, sw_iter_plane(f, nxt))[k];
+        d[f] = xplane(b, c, X_DA + f)[kx];
+    }
+#pragma unroll
+    for (int f = 0; f < NFIELD; f++)
+        store_mirrored(plane(b, c, sw_iter_plane(f, nxt)), c.ld, i, j, c.W, c.periodic, x[f] + (double)d[f]);
+}
+
+}  // namespace cfd

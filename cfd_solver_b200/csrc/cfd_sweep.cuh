@@ -1,0 +1,18 @@
+// cfd_sweep.cuh -- the persistent momentum / energy sweep kernels (cfd_sweep.cu).
+#pragma once
+#include "cfd_common.cuh"
+
+namespace cfd {
+enum SweepMode { SW_F64 = 0, SW_MX0 = 1, SW_MX = 2 };
+constexpr int SW_WARPS = 4;                       // warps per CTA (one 32 x 16 tile)
+constexpr int SW_THREADS = 32 * SW_WARPS;
+constexpr int SW_ROWS = TYJ / SW_WARPS;           // rows of the tile per thread
+constexpr int SWF_THREADS = 128;                  // per-case finalisation
+
+__global__ void k_sweep_f64(BatchDev b);
+__global__ void k_sweep_mx(BatchDev b);
+__global__ void k_sweep_fin(BatchDev b);
+__global__ void k_mom_update(BatchDev b);
+size_t sweep_smem_f64();
+size_t sweep_smem_mx();
+}  // namespace cfd

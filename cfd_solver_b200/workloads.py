@@ -33,17 +33,24 @@ def sweep_draws(ncases: int = 256, seed: int = SWEEP_SEED):
     return out
 
 
-def cavity_dt(N: int, Ri: float, cfl: float = 0.4) -> float:
-    """Convective time step of the cavity form: CFL on the lid speed or the buoyant
-    velocity scale sqrt(Ri), whichever is larger."""
-    return cfl / (N - 1) / max(1.0, math.sqrt(Ri))
+def cavity_dt(N: int, Ri: float, Re: float = 0.0, Pr: float = 1.0, cfl: float = 0.4) -> float:
+    """Time step of the cavity form, velocity scale U = max(1, sqrt(Ri)) (lid speed or
+    buoyant velocity). Two limits: CFL `cfl` on U, and the stability of explicit
+    (forward-Euler) convection with implicit diffusion, whose low-wavenumber modes grow
+    unless dt <= 2 / (Re Pr_eff U^2) with Pr_eff = max(1, Pr) (u, v: 1/Re; T: 1/(Re Pr));
+    half of that bound is used."""
+    U = max(1.0, math.sqrt(Ri))
+    dt = cfl / (N - 1) / U
+    if Re > 0.0:
+        dt = min(dt, 1.0 / (Re * max(1.0, Pr) * U * U))
+    return dt
 
 
 def make_case(d: dict, form: str):
     """(grid, params-dict) of one draw in the given form."""
     if form == "cavity":
         g = cavity(d["N"], d["N"], skew=d["skew"])
-        prm = dict(Re=d["Re"], Ri=d["Ri"], Pr=d["Pr"], dt=cavity_dt(d["N"], d["Ri"]))
+        prm = dict(Re=d["Re"], Ri=d["Ri"], Pr=d["Pr"], dt=cavity_dt(d["N"], d["Ri"], d["Re"], d["Pr"]))
     elif form == "twin":
         g = ogrid(d["N"], d["N"], ar=2.0, r_outer=20.0, skew=d["skew"])
         # the reference's own time step and flow angle (PSolver.cpp:169-174)

@@ -44,6 +44,9 @@ extern "C" {
 #define CFD_PROFILE_OGRID 0  /* the reference's O-grid (periodic xi, body + far field) */
 #define CFD_PROFILE_CAVITY 1 /* lid-driven unit square on a curvilinear grid */
 
+#define CFD_PRECISION_FP64 0  /* every sweep and Krylov vector in FP64 (the plain path) */
+#define CFD_PRECISION_MIXED 1 /* FP32 inner sweeps / Krylov work inside FP64 defect correction */
+
 /* One INP.DAT grid (PSolver.cpp:517-547); planes are n1*n0 host float64, [j][i]. */
 typedef struct cfd_grid {
     int n0, n1;
@@ -68,6 +71,7 @@ typedef struct cfd_params {
     int warm_start;            /* 1: up/vp solves start from the previous step; 0: from zero */
     double omega_p;            /* p += omega_p * pcor (reference: 1) */
     double lid_u;              /* cavity lid velocity */
+    int precision;             /* CFD_PRECISION_FP64 (plain) or CFD_PRECISION_MIXED; one per batch */
 } cfd_params;
 
 /* Statistics of the last completed step of a case. */
