@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--form", choices=["twin", "cavity"], default="twin")
     ap.add_argument("--ncases", type=int, default=256)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="plain FP64 path or the precision form (FP32 corrections in FP64 defect correction)")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -142,6 +144,7 @@ def workload_config(args):
             "params": "skew U[0,0.2], Re logU[50,1000], Ri logU[0.1,10], Pr {0.71,7}, seed 1234+rank",
             "dt": "1e-4 (reference)" if args.form == "twin" else "CFL 0.4 / max(1, sqrt(Ri))",
             "inner_tolerances": "reference: relative L1 0.75e-2 (momentum and pressure)",
+            "precision": args.precision,
             "l2_flush": "inputs larger than L2 (>= 2.4 GB resident per step)",
             "parallelism": f"case-sharded, dp{args.gpus}"}
 
@@ -239,7 +242,7 @@ def main():
     for d in draws:
         g, prm = make_case(d, args.form)
         grids.append(g)
-        params.append(case_params(g, **prm))
+        params.append(case_params(g, precision=1 if args.precision == "mixed" else 0, **prm))
     cells = sum(g.n0 * g.n1 for g in grids)
     b = Batch(grids, params)
     stream = torch.cuda.ExternalStream(b.stream())
@@ -284,14 +287,21 @@ def main():
     value = cells * args.steps * world / (ms_max / 1e3)
 
     # roofline of the dominant kernel (the u/v/T sweeps): algorithmic bytes per launch from
-    # the traffic counters: per field-cell read x_k, rhs, x_{k-1} and write x_{k+1} (32 B; the
-    # first sweep skips x_{k-1}); per cell read alpha, beta, gamma (24 B)
+    # the traffic counters (field-cells of all sweeps, of sweep 0, of sweep 1; cells).
+    # FP64: per field-cell read x_k, rhs, x_{k-1}, write x_{k+1} (32 B; sweep 0 has no x_{k-1}).
+    # Precision form: sweep 0 reads x0 and rhs (FP64), writes r and d_1 (FP32): 24 B; later
+    # sweeps read d_k, r, d_{k-1}, write d_{k+1} in FP32: 16 B (12 B at sweep 1, d_0 = 0).
+    # Every sweep reads alpha, beta, gamma (24 B per cell).
     dom = max(kt.items(), key=lambda kv: kv[1][0])
     jac_ms, jac_n = kt.get("k_sweep", (0.0, 0))
     fc = work1[0] - work0[0]
     cc = work1[1] - work0[1]
     f0 = work1[2] - work0[2]
-    jac_bytes = 32 * fc - 8 * f0 + 24 * cc
+    f1 = work1[3] - work0[3]
+    if args.precision == "mixed":
+        jac_bytes = 24 * f0 + 12 * f1 + 16 * (fc - f0 - f1) + 24 * cc
+    else:
+        jac_bytes = 32 * fc - 8 * f0 + 24 * cc
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -350,7 +360,8 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f64+f32",
                 "data": "synthetic (seeded sweep draws; grids generated in INP.DAT format)",
                 "config": workload_config(args),
                 "cells_per_step": cells * world,

@@ -1079,9 +1079,9 @@ void* cfd_batch_stream(cfd_batch* b) { return b ? (void*)b->st : nullptr; }
 
 long long cfd_batch_launches(cfd_batch* b) { return b ? b->launches : -1; }
 
-int cfd_batch_work(cfd_batch* b, unsigned long long* out3) {
-    if (!b || !out3) return fail(CFD_E_ARG, "bad arguments");
-    CK(cudaMemcpyAsync(out3, b->work, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->st));
+int cfd_batch_work(cfd_batch* b, unsigned long long* out4) {
+    if (!b || !out4) return fail(CFD_E_ARG, "bad arguments");
+    CK(cudaMemcpyAsync(out4, b->work, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
     return CFD_OK;
 }

@@ -143,19 +143,11 @@ __device__ __forceinline__ void sw_issue(const Tile& t, int f, int sweep, int nx
     if (met) tma_load_3d(met, maps + TMAP_F64_TILE3, t.i0 + 2, t.j0, P_ALPH, bar);
 }
 
-// off-centre sum of the u-type operator for the cell whose window centre row is `r0 + 2`
-template <typename ST>
-__device__ __forceinline__ ST sw_sum(const ST (&w)[8][5], int r0, ST E, ST G, ST B, bool nearw, bool drop_s,
-                                     bool drop_n) {
+// off-centre sums of the u-type operator for the cell whose window centre row is `r0 + 2`:
+// the 25-point (4th-order) rows and the 9-point near-wall rows
 #define WX(dy, dx) w[r0 + 2 + (dy)][2 + (dx)]
-    if (nearw) {
-        ST s = -E * (WX(0, 1) + WX(0, -1));
-        const ST n = -G * WX(1, 0) + ST(0.5) * B * (WX(1, 1) - WX(1, -1));
-        const ST so = -G * WX(-1, 0) + ST(0.5) * B * (WX(-1, -1) - WX(-1, 1));
-        if (!drop_n) s += n;
-        if (!drop_s) s += so;
-        return s;
-    }
+template <typename ST>
+__device__ __forceinline__ ST sw_sum25(const ST (&w)[8][5], int r0, ST E, ST G, ST B) {
     const ST ex = ST(-4.0 / 3.0) * (WX(0, 1) + WX(0, -1)) + ST(1.0 / 12.0) * (WX(0, 2) + WX(0, -2));
     const ST gy = ST(-4.0 / 3.0) * (WX(1, 0) + WX(-1, 0)) + ST(1.0 / 12.0) * (WX(2, 0) + WX(-2, 0));
     const ST bx = ST(8.0 / 9.0) * (WX(1, 1) + WX(-1, -1) - WX(1, -1) - WX(-1, 1)) +
@@ -163,8 +155,17 @@ __device__ __forceinline__ ST sw_sum(const ST (&w)[8][5], int r0, ST E, ST G, ST
                   ST(1.0 / 9.0) * (WX(2, -1) + WX(-2, 1) + WX(1, -2) + WX(-1, 2) - WX(2, 1) - WX(-2, -1) -
                                    WX(1, 2) - WX(-1, -2));
     return E * ex + G * gy + B * bx;
-#undef WX
 }
+template <typename ST>
+__device__ __forceinline__ ST sw_sum9(const ST (&w)[8][5], int r0, ST E, ST G, ST B, bool drop_s, bool drop_n) {
+    ST s = -E * (WX(0, 1) + WX(0, -1));
+    const ST n = -G * WX(1, 0) + ST(0.5) * B * (WX(1, 1) - WX(1, -1));
+    const ST so = -G * WX(-1, 0) + ST(0.5) * B * (WX(-1, -1) - WX(-1, 1));
+    if (!drop_n) s += n;
+    if (!drop_s) s += so;
+    return s;
+}
+#undef WX
 
 template <int MODE>
 __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm, uint64_t* bar) {
@@ -184,18 +185,15 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
     const int sweep = isc[I_MIT0 + (__ffs(mask) - 1)];
     const int tid = threadIdx.x, lane = tid & 31, wrp = tid >> 5;
     const int nxt = b.cur ^ 1;
-    int fl[NFIELD];
-    int nf = 0;
-#pragma unroll
-    for (int f = 0; f < NFIELD; f++)
-        if (mask & (1 << f)) fl[nf++] = f;
+    const int nf = __popc(mask);
     const char* maps = b.tmaps + (size_t)t.c * TMAP_STRIDE;
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         fence_mbar_init();
-        sw_issue<MODE>(t, fl[0], sweep, nxt, maps, sm, sm + L::MET, &bar[0]);
-        if (nf > 1) sw_issue<MODE>(t, fl[1], sweep, nxt, maps, sm + L::BUF, nullptr, &bar[1]);
+        const int m1 = mask & (mask - 1);
+        sw_issue<MODE>(t, __ffs(mask) - 1, sweep, nxt, maps, sm, sm + L::MET, &bar[0]);
+        if (m1) sw_issue<MODE>(t, __ffs(m1) - 1, sweep, nxt, maps, sm + L::BUF, nullptr, &bar[1]);
     }
     // per-case constants (uniform)
     const double* sc = b.scal + (long long)t.c * NSCAL;
@@ -219,10 +217,16 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
     __syncthreads();
 
     ST* OPS = reinterpret_cast<ST*>(sm + L::OPS);
+    bool any_nearw = false;
+#pragma unroll
+    for (int q = 0; q < SW_ROWS; q++) any_nearw |= nearw[q];
+    // the thread's periodic mirror column (written alongside column i), or none
+    const int mcol = mirror_col(i, W, per);
     double r[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
     bool ok = true;
     int k = 0;
-    for (; k < nf; k++) {
+    for (int fm = mask; fm; fm &= fm - 1, k++) {
+        const int f = __ffs(fm) - 1;
         const int bi = k & 1;
         ok = __syncthreads_and(mbar_wait_bounded(&bar[bi], (k >> 1) & 1)) && ok;
         if (!ok) break;
@@ -244,7 +248,6 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
                 OPS[4 * SW_CELLS + o] = (ST)(1.0 / (1.0 + D * rPr64));
             }
         }
-        const int f = fl[k];
         const bool isT = f == F_T;
         const XT* X = reinterpret_cast<const XT*>(buf + L::X);
         const RT* R = reinterpret_cast<const RT*>(buf + L::RHS);
@@ -262,54 +265,85 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
         for (int rr = 0; rr < 8; rr++)
 #pragma unroll
             for (int cl = 0; cl < 5; cl++) w[rr][cl] = (ST)X[(wrp * SW_ROWS + rr) * C::XW + lane + cl + C::XO - 2];
-        __syncthreads();  // the buffer has been read: refill it with field k+2
-        if (tid == 0 && k + 2 < nf) sw_issue<MODE>(t, fl[k + 2], sweep, nxt, maps, sm + bi * L::BUF, nullptr, &bar[bi]);
+        __syncthreads();  // the buffer has been read: refill it with the field after next
+        if (tid == 0) {
+            int nx = fm & (fm - 1);
+            nx &= nx - 1;
+            if (nx) sw_issue<MODE>(t, __ffs(nx) - 1, sweep, nxt, maps, sm + bi * L::BUF, nullptr, &bar[bi]);
+        }
 
+        // off-centre sums: the 25-point form for every cell, then the few near-wall cells
+        ST sum[SW_ROWS];
+#pragma unroll
+        for (int q = 0; q < SW_ROWS; q++) {
+            const int o = (wrp * SW_ROWS + q) * TX + lane;
+            sum[q] = sw_sum25<ST>(w, q, OPS[o], OPS[SW_CELLS + o], OPS[2 * SW_CELLS + o]);
+        }
+        if (any_nearw) {
+#pragma unroll
+            for (int q = 0; q < SW_ROWS; q++) {
+                if (!nearw[q]) continue;
+                const int o = (wrp * SW_ROWS + q) * TX + lane;
+                sum[q] = sw_sum9<ST>(w, q, OPS[o], OPS[SW_CELLS + o], OPS[2 * SW_CELLS + o], drop_s[q], drop_n[q]);
+            }
+        }
         const ST g = isT ? gT : gU, wgt = isT ? wT : wU;
+        const ST scale = isT ? rPr : ST(1);
+        // the reference's T solve passes atnw in the annw slot (PSolver.cpp:1290): the
+        // (i-1, j+2) coefficient of the 25-point T rows becomes anw = -8/9 B instead of B/9
         const bool tbug = isT && !c.fix_T_annw;
+        const int rapoff = (isT ? 4 : 3) * SW_CELLS;
         double* dst64 = nullptr;
         float* dst32 = nullptr;
         float* res32 = nullptr;
+        int dld = ld;
         if (MODE == SW_F64) {
             dst64 = plane(b, c, (sweep & 1) == 0 ? P_BU + f : sw_iter_plane(f, nxt));
         } else if (MODE == SW_MX0) {
             dst32 = xplane(b, c, X_DB + f);
             res32 = xplane(b, c, X_R + f);
+            dld = xld;
         } else {
             dst32 = xplane(b, c, (sweep & 1) == 0 ? X_DB + f : X_DA + f);
+            dld = xld;
         }
         double racc = 0.0;
 #pragma unroll
         for (int q = 0; q < SW_ROWS; q++) {
-            if (!inq[q]) continue;
             const int o = (wrp * SW_ROWS + q) * TX + lane;
             const ST E = OPS[o], G = OPS[SW_CELLS + o], B = OPS[2 * SW_CELLS + o];
-            ST sum = sw_sum<ST>(w, q, E, G, B, nearw[q], drop_s[q], drop_n[q]);
+            ST sm_ = sum[q];
+            if (tbug && !nearw[q]) sm_ -= B * w[q + 4][1];
+            sm_ *= scale;
             const ST D = (nearw[q] ? ST(2) : ST(2.5)) * (E + G);
-            ST ap, rap;
-            if (isT) {
-                // the reference's T solve passes atnw in the annw slot (PSolver.cpp:1290):
-                // the (i-1, j+2) coefficient becomes anw = -8/9 B instead of B/9
-                if (tbug && !nearw[q]) sum -= B * w[q + 4][1];
-                sum *= rPr;
-                ap = ST(1) + D * rPr;
-                rap = OPS[4 * SW_CELLS + o];
-            } else {
-                ap = ST(1) + D;
-                rap = OPS[3 * SW_CELLS + o];
-            }
+            const ST ap = ST(1) + D * scale;
+            const ST rap = OPS[rapoff + o];
             const ST xk = w[q + 2][2];
-            const ST res = rhs[q] - ap * xk - sum;
-            racc += fabs((double)res);
-            const int j = t.j0 + wrp * SW_ROWS + q;
+            const ST res = rhs[q] - ap * xk - sm_;
+            racc += inq[q] ? fabs((double)res) : 0.0;
+            const long long kk = (long long)(t.j0 + wrp * SW_ROWS + q) * dld;
             if (MODE == SW_MX0) {
-                store_mirrored(dst32, xld, i, j, W, per, (float)(g * res * rap));
-                store_mirrored(res32, xld, i, j, W, per, (float)res);
+                const float d1 = (float)(g * res * rap), rr = (float)res;
+                if (inq[q]) {
+                    dst32[kk + i] = d1;
+                    res32[kk + i] = rr;
+                    if (mcol > -1000000) {
+                        dst32[kk + mcol] = d1;
+                        res32[kk + mcol] = rr;
+                    }
+                }
             } else {
                 ST xn = xk + g * res * rap;
                 if (weighted) xn = wgt * (xn - xm[q]) + xm[q];
-                if (MODE == SW_F64) store_mirrored(dst64, ld, i, j, W, per, (double)xn);
-                else store_mirrored(dst32, xld, i, j, W, per, (float)xn);
+                if (inq[q]) {
+                    if (MODE == SW_F64) {
+                        dst64[kk + i] = (double)xn;
+                        if (mcol > -1000000) dst64[kk + mcol] = (double)xn;
+                    } else {
+                        dst32[kk + i] = (float)xn;
+                        if (mcol > -1000000) dst32[kk + mcol] = (float)xn;
+                    }
+                }
             }
         }
 #pragma unroll
@@ -412,6 +446,7 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
     atomicAdd(&b.work[0], nf);
     atomicAdd(&b.work[1], ncell);
     if (sweep == 0) atomicAdd(&b.work[2], nf);
+    if (sweep == 1) atomicAdd(&b.work[3], nf);
 }
 
 size_t sweep_smem_f64() { return (size_t)SwLayout<SW_F64>::TOTAL + 128; }

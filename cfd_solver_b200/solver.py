@@ -98,7 +98,7 @@ class Batch:
         return int(_lib.lib().cfd_batch_launches(self.h))
 
     def work(self) -> tuple:
-        w = (ctypes.c_ulonglong * 3)()
+        w = (ctypes.c_ulonglong * 4)()
         _lib.check(_lib.lib().cfd_batch_work(self.h, w), "cfd_batch_work")
         return tuple(int(x) for x in w)
 

@@ -184,8 +184,9 @@ void* cfd_batch_stream(cfd_batch* b);
 /* kernels launched by the batch since creation */
 long long cfd_batch_launches(cfd_batch* b);
 /* algorithmic-traffic counters of the u/v/T sweeps: [0] field-cells swept, [1] cells swept,
- * [2] field-cells of first sweeps (which read one array less) */
-int cfd_batch_work(cfd_batch* b, unsigned long long* out3);
+ * [2] field-cells of first sweeps, [3] field-cells of second sweeps (the sweeps that read
+ * one array less in the FP64 path and in the precision form respectively) */
+int cfd_batch_work(cfd_batch* b, unsigned long long* out4);
 
 /* ---- the gauss() seam on device arrays (replaces PSolver.cpp:2280-2446) ----
  * Solves one momentum / energy system given its 25 stored coefficient planes in
