@@ -47,6 +47,16 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["step", "converged", "serve"], default="step",
+                    help="step: outer-step throughput of the sweep (default); converged: every case of "
+                         "the sweep to its steady tolerance or the step cap, batched vs the plain "
+                         "single-case FP64 path; serve: Poisson request stream through cfd_serve")
+    ap.add_argument("--tol", type=float, default=1e-8, help="steady-residual tolerance (converged/serve)")
+    ap.add_argument("--cap", type=int, default=30000, help="step cap per case (converged)")
+    ap.add_argument("--chunk", type=int, default=100, help="steps between retirement checks")
+    ap.add_argument("--requests", type=int, default=512, help="requests of the serve workload")
+    ap.add_argument("--rate", type=float, default=4.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--max-steps", type=int, default=1000, help="step cap per request (serve)")
     return ap.parse_args()
 
 
@@ -212,11 +222,176 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ------------------------------------------------------------------ plain single-case path
+def plain_step_ms(grid, prm, warm: int, timed: int) -> float:
+    """Device time per step of one case alone on the plain FP64 path (a batch of one), after
+    `warm` untimed steps past the start-up transient."""
+    import torch
+    from cfd_solver_b200.solver import Batch, case_params
+    with Batch([grid], [case_params(grid, precision=0, **prm)]) as b:
+        b.step(warm)
+        b.sync()
+        stream = torch.cuda.ExternalStream(b.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.step(timed)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / timed
+
+
+def plain_times_by_size(cases, warm=1500, timed=500):
+    """Per-step time of the plain path for each grid size, on the first case of that size."""
+    out = {}
+    for g, prm in cases:
+        if g.n0 not in out:
+            out[g.n0] = plain_step_ms(g, prm, warm, timed)
+    return out
+
+
+def run_converged(args):
+    """Every case of the sweep to steady_res_rel <= tol (or the step cap), batched with
+    retirement, against the plain FP64 single-case path on the same cases."""
+    import torch
+    from cfd_solver_b200.solver import Batch, case_params
+    from cfd_solver_b200.workloads import SWEEP_SEED, make_case, sweep_draws
+    draws = sweep_draws(args.ncases, seed=SWEEP_SEED)
+    cases = [make_case(d, args.form) for d in draws]
+    prec = 1 if args.precision == "mixed" else 0
+    b = Batch([g for g, _ in cases], [case_params(g, precision=prec, **p) for g, p in cases])
+    n = len(cases)
+    active = [True] * n
+    steps_at, outcome, nu = [0] * n, [""] * n, [0.0] * n
+    clocks = ClockSampler(0)
+    torch.cuda.synchronize()
+    clocks.mark_start()
+    t0 = time.perf_counter()
+    total = 0
+    while any(active):
+        b.step(args.chunk)
+        total += args.chunk
+        st = b.all_stats()
+        for i in range(n):
+            if not active[i]:
+                continue
+            s = st[i]
+            bad = bool(s["status"] & 4) or s["steady_res_rel"] != s["steady_res_rel"]
+            conv = s["steps"] >= 2 and s["steady_res_rel"] <= args.tol
+            if bad or conv or s["steps"] >= args.cap:
+                active[i] = False
+                b.set_active(i, False)
+                steps_at[i], nu[i] = s["steps"], s["nu"]
+                outcome[i] = "diverged" if bad else ("converged" if conv else "capped")
+    b.sync()
+    makespan = time.perf_counter() - t0
+    clocks.mark_end()
+    clk = clocks.stop()
+    b.close()
+    nconv = outcome.count("converged")
+    # plain path: per-size step time of one case alone (FP64), times each case's steps
+    pt = plain_times_by_size(cases)
+    plain_s = sum(steps_at[i] * pt[cases[i][0].n0] for i in range(n)) / 1e3
+    # cross-check: the quickest-converging case run alone to its retirement step
+    qi = min((i for i in range(n) if outcome[i] == "converged"), key=lambda i: steps_at[i], default=None)
+    check = None
+    if qi is not None:
+        g, prm = cases[qi]
+        with Batch([g], [case_params(g, precision=0, **prm)]) as one:
+            stream = torch.cuda.ExternalStream(one.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            one.step(steps_at[qi])
+            e1.record(stream)
+            e1.synchronize()
+            s1 = one.stats(0)
+        check = {"case": qi, "N": g.n0, "steps": steps_at[qi], "measured_s": e0.elapsed_time(e1) / 1e3,
+                 "predicted_s": steps_at[qi] * pt[g.n0] / 1e3, "steady_res_rel": s1["steady_res_rel"],
+                 "nu_plain": s1["nu"], "nu_batched": nu[qi]}
+    cells = sum(g.n0 * g.n1 * steps_at[i] for i, (g, _) in enumerate(cases))
+    line = {"metric": "converged cases/s", "value": nconv / makespan, "unit": "cases/s", "n_gpus": 1,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+            "data": "synthetic (seeded sweep draws)",
+            "config": {**workload_config(args), "tol": args.tol, "step_cap": args.cap,
+                       "retire_check_every": args.chunk},
+            "makespan_s": makespan, "converged": nconv, "capped": outcome.count("capped"),
+            "diverged": outcome.count("diverged"), "cell_updates_per_s": cells / makespan,
+            "plain": {"value": nconv / plain_s, "makespan_s": plain_s, "path": "single case, FP64",
+                      "ms_per_step_by_N": pt, "cross_check": check},
+            "speedup_vs_plain": plain_s / makespan, "clocks": clk,
+            "timing": "host wall clock around the whole run (retirement needs the host each chunk)"}
+    print(json.dumps(line))
+
+
+def run_serve(args):
+    """A Poisson request stream (sizes N in {129,257,513,1025} w.p. {.4,.3,.2,.1}, physics as
+    the sweep) through the native serving loop, against a plain single-case FP64 server
+    (FIFO, one case at a time) whose service times are measured per size."""
+    import math as _m
+    import numpy as np
+    from cfd_solver_b200.grid import cavity
+    from cfd_solver_b200.solver import case_params, serve
+    from cfd_solver_b200.workloads import SWEEP_SEED, make_case, sweep_draws
+    rng = np.random.default_rng(SWEEP_SEED + 7)
+    sizes, probs = [129, 257, 513, 1025], [0.4, 0.3, 0.2, 0.1]
+    base = sweep_draws(args.requests, seed=SWEEP_SEED + 7)
+    prec = 1 if args.precision == "mixed" else 0
+    reqs, cases = [], []
+    t = 0.0
+    for d in base:
+        d = dict(d, N=int(rng.choice(sizes, p=probs)))
+        t += float(rng.exponential(1.0 / args.rate))
+        g, prm = make_case(d, "cavity")
+        cases.append((g, prm))
+        reqs.append((t, g, case_params(g, precision=prec, **prm), args.tol, args.max_steps))
+    classes = [(cavity(N, N), 1) for N in sizes]
+    slots = [64, 32, 16, 8]
+    results, st = serve(reqs, classes, steps_per_tick=args.chunk, slots=slots, precision=prec)
+    # plain server: FIFO, one case at a time, service = steps x plain step time of its size
+    pt = plain_times_by_size([cases[i] for i in range(len(cases))], warm=300, timed=200)
+    free, lat = 0.0, []
+    for (ta, g, *_), r in zip(reqs, results):
+        start = max(free, ta)
+        free = start + r["steps"] * pt[g.n0] / 1e3
+        lat.append(free - ta)
+    lat_s = sorted(lat)
+    pct = lambda q: lat_s[min(len(lat_s) - 1, max(0, _m.ceil(q * len(lat_s)) - 1))]
+    finished = len(results)
+    line = {"metric": "served cases/s", "value": finished / max(st["makespan_s"], 1e-9), "unit": "cases/s",
+            "n_gpus": 1, "value_counts": "finished requests (converged or at their step cap) per second",
+            "higher_is_better": True, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+            "data": "synthetic (seeded Poisson stream)",
+            "config": {"workload": f"{args.requests} requests, Poisson rate {args.rate}/s, N in {sizes} "
+                                   f"w.p. {probs}, cavity form", "tol": args.tol,
+                       "max_steps": args.max_steps, "slots": dict(zip(sizes, slots)),
+                       "steps_per_tick": args.chunk, "precision": args.precision},
+            "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
+            "mean_latency_s": st["mean_latency_s"], "makespan_s": st["makespan_s"],
+            "converged": st["converged"], "finished_at_cap": args.requests - st["converged"],
+            "cell_updates_per_s": st["cell_updates"] / max(st["makespan_s"], 1e-9),
+            "plain": {"cases_per_s": len(lat) / max(free - reqs[0][0], 1e-9), "p50_latency_s": pct(0.5),
+                      "p99_latency_s": pct(0.99), "ms_per_step_by_N": pt,
+                      "path": "single case, FP64, FIFO (service times measured per size)"}}
+    print(json.dumps(line))
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.workload == "converged":
+        if args.form == "twin" and "--form" not in sys.argv:
+            args.form = "cavity"
+        if "--precision" not in sys.argv:
+            args.precision = "mixed"
+        run_converged(args)
+        return
+    if args.workload == "serve":
+        if "--precision" not in sys.argv:
+            args.precision = "mixed"
+        run_serve(args)
         return
     import torch
     import torch.distributed as dist

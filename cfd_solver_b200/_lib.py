@@ -80,7 +80,7 @@ class CfdServeConfig(ctypes.Structure):
     _fields_ = [("nclasses", ctypes.c_int), ("class_grids", ctypes.POINTER(CfdGrid)),
                 ("class_profile", ctypes.POINTER(ctypes.c_int)),
                 ("class_slots", ctypes.POINTER(ctypes.c_int)), ("hbm_budget", ctypes.c_size_t),
-                ("steps_per_tick", ctypes.c_int)]
+                ("steps_per_tick", ctypes.c_int), ("precision", ctypes.c_int)]
 
 
 class CfdServeStats(ctypes.Structure):

@@ -55,6 +55,7 @@ extern "C" int cfd_serve(const cfd_serve_config* cfg, const cfd_request* reqs, i
             cfd_params p;
             cfd_params_default(&p);
             p.profile = cfg->class_profile[k];
+            p.precision = cfg->precision;
             tp.push_back(p);
             slot_class.push_back(k);
         }

@@ -132,11 +132,13 @@ class Batch:
             pass
 
 
-def serve(requests, classes, steps_per_tick: int = 50, slots=None, hbm_budget: int = 0):
+def serve(requests, classes, steps_per_tick: int = 50, slots=None, hbm_budget: int = 0,
+          precision: int = _lib.PRECISION_FP64):
     """Run a real-time serving session (cfd_serve).
 
     requests: list of (arrival_s, grid, params, tol, max_steps); classes: list of
-    (template grid, profile); slots: slots per class (or None with hbm_budget).
+    (template grid, profile); slots: slots per class (or None with hbm_budget); precision:
+    CFD_PRECISION_* of the slots (every request's params must match).
     Returns (list of result dicts, stats dict).
     """
     keep = []
@@ -149,7 +151,8 @@ def serve(requests, classes, steps_per_tick: int = 50, slots=None, hbm_budget: i
     profs = (ctypes.c_int * len(classes))(*[p for _, p in classes])
     sl = (ctypes.c_int * len(classes))(*slots) if slots is not None else None
     cfg = _lib.CfdServeConfig(nclasses=len(classes), class_grids=garr, class_profile=profs,
-                              class_slots=sl, hbm_budget=int(hbm_budget), steps_per_tick=steps_per_tick)
+                              class_slots=sl, hbm_budget=int(hbm_budget), steps_per_tick=steps_per_tick,
+                              precision=precision)
     rgrids = []
     reqs = (_lib.CfdRequest * len(requests))()
     for i, (t, g, prm, tol, mx) in enumerate(requests):

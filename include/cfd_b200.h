@@ -159,6 +159,7 @@ typedef struct cfd_serve_config {
     const int* class_slots;      /* slots per class; NULL: an equal share of hbm_budget each */
     size_t hbm_budget;           /* device bytes for all slots when class_slots is NULL */
     int steps_per_tick;          /* steps between convergence checks / admissions */
+    int precision;               /* CFD_PRECISION_* of every slot (requests must match) */
 } cfd_serve_config;
 
 typedef struct cfd_serve_stats {
