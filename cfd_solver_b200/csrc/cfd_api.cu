@@ -481,10 +481,9 @@ void enq_p_iter(cfd_batch* b, BatchDev& bd) {
     { Prof pr(b, K_BICG_X); k_bicg_x<<<nf, NT, 0, b->st>>>(bd, b->maxit_p); }
 }
 void enq_end(cfd_batch* b, BatchDev& bd) {
-    const int nf = bd.nftiles;
-    { Prof pr(b, K_CORRECT); k_correct<<<nf, NT, 0, b->st>>>(bd); }
+    { Prof pr(b, K_CORRECT); k_correct<<<bd.njtiles, NT, 0, b->st>>>(bd); }
     { Prof pr(b, K_BC); k_bc<<<b->n, BC_THREADS, 2 * (b->max_W + 1) * sizeof(double), b->st>>>(bd); }
-    { Prof pr(b, K_DIAG); k_diag<<<nf, NT, 0, b->st>>>(bd); }
+    { Prof pr(b, K_DIAG); k_diag<<<bd.njtiles, NT, 0, b->st>>>(bd); }
 }
 
 // one step with host-side loop control (per-kernel profiling works on this path)

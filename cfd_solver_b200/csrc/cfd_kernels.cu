@@ -848,46 +848,67 @@ __global__ void __launch_bounds__(NT) k_mg_galerkin(BatchDev b, int l, int toff)
 // ---------------------------------------------------------------------------
 // pcor boundary conditions + velocity / pressure correction (PSolver.cpp:1471-1542);
 // also the momentum part of the steady residual, sum |u^{n+1} - u^n| + |v^{n+1} - v^n|
-__global__ void __launch_bounds__(NT) k_correct(BatchDev b) {
-    const Tile t = b.ftiles[blockIdx.x];
+__global__ void __launch_bounds__(NT, 3) k_correct(BatchDev b) {
+    // a 32 x 16 tile, two cells per thread (rows lj and lj + 8): every load of both cells
+    // is issued before any arithmetic
+    const Tile t = b.jtiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
-    if (!b.iscal[(long long)t.c * NISCAL + I_ACTIVE]) return;  // uniform over the case
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    const int* isc = b.iscal + (long long)t.c * NISCAL;
+    if (!isc[I_ACTIVE]) return;  // uniform over the case
     // no pressure iteration ran (q vanished or broke down at once): pcor = 0
-    const bool none = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
+    const bool none = isc[I_PIT] == 0;
+    const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
+    const bool cav = c.profile == CAVITY;
+    double* PC = plane(b, c, P_PCOR);
+    double* U = plane(b, c, P_U);
+    double* V = plane(b, c, P_V);
+    double* P = plane(b, c, P_P);
+    const double* US = plane(b, c, P_US);
+    const double* VS = plane(b, c, P_VS);
+    const double* XIX = plane(b, c, P_XIX);
+    const double* XIY = plane(b, c, P_XIY);
+    const double* ETX = plane(b, c, P_ETX);
+    const double* ETY = plane(b, c, P_ETY);
+    const double* VEC = plane(b, c, P_VEC);
+    const int i = t.i0 + (int)(threadIdx.x % TX);
+    bool in[2];
+    long long kk[2];
+    double pc0[2], pn0[2], ps0[2], pe0[2], pw0[2], us[2], vs[2], xix[2], etx[2], xiy[2], ety[2], u0[2], v0[2],
+        p0[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int j = t.j0 + (int)(threadIdx.x / TX) + h * TY;
+        in[h] = i >= c.ilo && i <= c.ihi && j <= n1 - 2;
+        const long long k = in[h] ? (long long)j * ld + i : (long long)ld + c.ilo;  // a safe cell when out
+        kk[h] = k;
+        pc0[h] = PC[k]; pn0[h] = PC[k + ld]; ps0[h] = PC[k - ld]; pe0[h] = PC[k + 1]; pw0[h] = PC[k - 1];
+        us[h] = US[k]; vs[h] = VS[k];
+        xix[h] = XIX[k]; etx[h] = ETX[k]; xiy[h] = XIY[k]; ety[h] = ETY[k];
+        u0[h] = U[k]; v0[h] = V[k]; p0[h] = P[k];
+    }
+    const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
+    const double d0 = c.d0, d1 = c.d1, dt = c.dt;
     double red[1] = {0.0};
-    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
-        const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
-        const bool cav = c.profile == CAVITY;
-        double* PC = plane(b, c, P_PCOR);
-        double* U = plane(b, c, P_U);
-        double* V = plane(b, c, P_V);
-        double* P = plane(b, c, P_P);
-        const long long k = (long long)j * ld + i;
-        // every load first (independent), the boundary conditions as selects afterwards
-        const double pc0 = PC[k], pn0 = PC[k + ld], ps0 = PC[k - ld], pe0 = PC[k + 1], pw0 = PC[k - 1];
-        const double us = plane(b, c, P_US)[k], vs = plane(b, c, P_VS)[k];
-        const double xix = plane(b, c, P_XIX)[k], etx = plane(b, c, P_ETX)[k];
-        const double xiy = plane(b, c, P_XIY)[k], ety = plane(b, c, P_ETY)[k];
-        const double u0 = U[k], v0 = V[k], p0 = P[k];
-        const double* VEC = plane(b, c, P_VEC);
-        const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
-        const double pc = none ? 0.0 : pc0;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        if (!in[h]) continue;
+        const int j = t.j0 + (int)(threadIdx.x / TX) + h * TY;
+        const long long k = kk[h];
+        const double pc = none ? 0.0 : pc0[h];
         // pcor on the boundary after its conditions: wall copy, far field 0 / copy at inflow
         const double far = (!cav && vnn >= 0) ? pc : 0.0;
-        const double pN = none ? 0.0 : (j == n1 - 2) ? (cav ? pc : far) : pn0;
-        const double pS = none ? 0.0 : (j == 1) ? pc : ps0;
-        const double pE = none ? 0.0 : (cav && i == n0 - 2) ? pc : pe0;
-        const double pW = none ? 0.0 : (cav && i == 1) ? pc : pw0;
-        const double d0 = c.d0, d1 = c.d1, dt = c.dt;
+        const double pN = none ? 0.0 : (j == n1 - 2) ? (cav ? pc : far) : pn0[h];
+        const double pS = none ? 0.0 : (j == 1) ? pc : ps0[h];
+        const double pE = none ? 0.0 : (cav && i == n0 - 2) ? pc : pe0[h];
+        const double pW = none ? 0.0 : (cav && i == 1) ? pc : pw0[h];
         const double dpcor_dxi = 0.5 * (pE - pW) / d0;
         const double dpcor_de = 0.5 * (pN - pS) / d1;
-        const double un = us - dt * (xix * dpcor_dxi + etx * dpcor_de);
-        const double vn = vs - dt * (xiy * dpcor_dxi + ety * dpcor_de);
-        red[0] = fabs(un - u0) + fabs(vn - v0);
+        const double un = us[h] - dt * (xix[h] * dpcor_dxi + etx[h] * dpcor_de);
+        const double vn = vs[h] - dt * (xiy[h] * dpcor_dxi + ety[h] * dpcor_de);
+        red[0] += fabs(un - u0[h]) + fabs(vn - v0[h]);
         store_mirrored(U, ld, i, j, W, per, un);
         store_mirrored(V, ld, i, j, W, per, vn);
-        const double pn = (c.omega_p == 1.0) ? p0 + pc : p0 + c.omega_p * pc;
+        const double pn = (c.omega_p == 1.0) ? p0[h] + pc : p0[h] + c.omega_p * pc;
         store_mirrored(P, ld, i, j, W, per, pn);
         if (none) store_mirrored(PC, ld, i, j, W, per, 0.0);
         // record the boundary pcor (output only)
@@ -902,7 +923,7 @@ __global__ void __launch_bounds__(NT) k_correct(BatchDev b) {
             if (i == n0 - 2 && j == n1 - 2) PC[(long long)(n1 - 1) * ld + n0 - 1] = pc;
         }
     }
-    if (case_reduce<1, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0)
+    if (case_reduce<1, 0u>(b, t.c, blockIdx.x, c.jt_begin, c.jt_count, red) && threadIdx.x == 0)
         b.scal[(long long)t.c * NSCAL + S_DUL1] = red[0];
 }
 
@@ -1144,35 +1165,54 @@ __global__ void __launch_bounds__(BC_THREADS) k_bc(BatchDev b) {
 
 // ---------------------------------------------------------------------------
 // dilatation, interior vorticity, dmax and the energy residual (PSolver.cpp:1807-1853)
-__global__ void __launch_bounds__(NT) k_diag(BatchDev b) {
-    const Tile t = b.ftiles[blockIdx.x];
+__global__ void __launch_bounds__(NT, 3) k_diag(BatchDev b) {
+    // a 32 x 16 tile, two cells per thread; all loads of both cells first
+    const Tile t = b.jtiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
     if (!b.iscal[(long long)t.c * NISCAL + I_ACTIVE]) return;  // uniform over the case
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
-    double red[3] = {0.0, 0.0, 0.0};
-    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
-        const int ld = c.ld;
-        const long long k = (long long)j * ld + i;
-        const double* U = plane(b, c, P_U);
-        const double* V = plane(b, c, P_V);
-        const double d0 = c.d0, d1 = c.d1;
-        const double xix = plane(b, c, P_XIX)[k], xiy = plane(b, c, P_XIY)[k];
-        const double etx = plane(b, c, P_ETX)[k], ety = plane(b, c, P_ETY)[k];
-        const double dil = xix * (U[k + 1] - U[k - 1]) / (2 * d0) + etx * (U[k + ld] - U[k - ld]) / (2 * d1) +
-                           ety * (V[k + ld] - V[k - ld]) / (2 * d1) + xiy * (V[k + 1] - V[k - 1]) / (2 * d0);
-        const double dv_dxi = 0.5 / d0 * (V[k + 1] - V[k - 1]);
-        const double dv_det = 0.5 / d1 * (V[k + ld] - V[k - ld]);
-        const double du_dxi = 0.5 / d0 * (U[k + 1] - U[k - 1]);
-        const double du_det = 0.5 / d1 * (U[k + ld] - U[k - ld]);
-        const double vort = (xix * dv_dxi + etx * dv_det) - (xiy * du_dxi + ety * du_det);
-        store_mirrored(plane(b, c, P_VORT), ld, i, j, c.W, c.periodic, vort);
-        store_mirrored(plane(b, c, P_DIL), ld, i, j, c.W, c.periodic, dil);
-        const double dT = fabs(plane(b, c, P_T0 + (b.cur ^ 1))[k] - plane(b, c, P_T0 + b.cur)[k]);
-        red[0] = dil;
-        red[1] = dT;
-        red[2] = dT;
+    const int ld = c.ld, W = c.W, per = c.periodic;
+    const int i = t.i0 + (int)(threadIdx.x % TX);
+    const double* U = plane(b, c, P_U);
+    const double* V = plane(b, c, P_V);
+    const double* XIX = plane(b, c, P_XIX);
+    const double* XIY = plane(b, c, P_XIY);
+    const double* ETX = plane(b, c, P_ETX);
+    const double* ETY = plane(b, c, P_ETY);
+    const double* TN = plane(b, c, P_T0 + (b.cur ^ 1));
+    const double* TO = plane(b, c, P_T0 + b.cur);
+    bool in[2];
+    double ue[2], uw[2], un[2], us[2], ve[2], vw[2], vn[2], vs[2], xix[2], xiy[2], etx[2], ety[2], tn[2], to[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int j = t.j0 + (int)(threadIdx.x / TX) + h * TY;
+        in[h] = i >= c.ilo && i <= c.ihi && j <= c.n1 - 2;
+        const long long k = in[h] ? (long long)j * ld + i : (long long)ld + c.ilo;  // a safe cell when out
+        ue[h] = U[k + 1]; uw[h] = U[k - 1]; un[h] = U[k + ld]; us[h] = U[k - ld];
+        ve[h] = V[k + 1]; vw[h] = V[k - 1]; vn[h] = V[k + ld]; vs[h] = V[k - ld];
+        xix[h] = XIX[k]; xiy[h] = XIY[k]; etx[h] = ETX[k]; ety[h] = ETY[k];
+        tn[h] = TN[k]; to[h] = TO[k];
     }
-    if (case_reduce<3, 0x5u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0) {
+    const double d0 = c.d0, d1 = c.d1;
+    double red[3] = {-1.0e300, 0.0, 0.0};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        if (!in[h]) continue;
+        const int j = t.j0 + (int)(threadIdx.x / TX) + h * TY;
+        const double dil = xix[h] * (ue[h] - uw[h]) / (2 * d0) + etx[h] * (un[h] - us[h]) / (2 * d1) +
+                           ety[h] * (vn[h] - vs[h]) / (2 * d1) + xiy[h] * (ve[h] - vw[h]) / (2 * d0);
+        const double dv_dxi = 0.5 / d0 * (ve[h] - vw[h]);
+        const double dv_det = 0.5 / d1 * (vn[h] - vs[h]);
+        const double du_dxi = 0.5 / d0 * (ue[h] - uw[h]);
+        const double du_det = 0.5 / d1 * (un[h] - us[h]);
+        const double vort = (xix[h] * dv_dxi + etx[h] * dv_det) - (xiy[h] * du_dxi + ety[h] * du_det);
+        store_mirrored(plane(b, c, P_VORT), ld, i, j, W, per, vort);
+        store_mirrored(plane(b, c, P_DIL), ld, i, j, W, per, dil);
+        const double dT = fabs(tn[h] - to[h]);
+        red[0] = fmax(red[0], dil);
+        red[1] += dT;
+        red[2] = fmax(red[2], dT);
+    }
+    if (case_reduce<3, 0x5u>(b, t.c, blockIdx.x, c.jt_begin, c.jt_count, red) && threadIdx.x == 0) {
         double* sc = b.scal + (long long)t.c * NSCAL;
         int* is = b.iscal + (long long)t.c * NISCAL;
         sc[S_DMAX] = fmax(red[0], 0.0);
