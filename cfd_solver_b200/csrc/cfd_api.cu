@@ -51,12 +51,12 @@ long long rup(long long x, long long a) { return (x + a - 1) / a * a; }
 
 enum KernelId {
     K_ASSEMBLE_P, K_RHS, K_SWEEP, K_UPBC, K_FACE_Q, K_BICG_P, K_SPMV, K_BICG_S, K_BICG_X,
-    K_MG_SMOOTH, K_MG_RESID, K_MG_RESTRICT, K_MG_PROLONG, K_MG_COARSE, K_MG_GALERKIN,
+    K_MG_SMOOTH, K_MG_RR, K_MG_POST, K_MG_COARSE, K_MG_GALERKIN,
     K_CORRECT, K_BC, K_DIAG, K_SI, K_MOM_UPDATE, K_SWEEP_FIN, NKERNEL
 };
 const char* kKernelNames[NKERNEL] = {
     "k_assemble_p", "k_rhs", "k_sweep", "k_upbc", "k_face_q", "k_bicg_p", "k_spmv", "k_bicg_s",
-    "k_bicg_x", "k_mg_smooth", "k_mg_resid", "k_mg_restrict", "k_mg_prolong", "k_mg_coarse",
+    "k_bicg_x", "k_mg_presmooth", "k_mg_rr", "k_mg_postsmooth", "k_mg_coarse",
     "k_mg_galerkin", "k_correct", "k_bc", "k_diag", "k_si", "k_mom_update", "k_sweep_fin"};
 
 struct LevelGeom {
@@ -184,6 +184,7 @@ struct cfd_batch {
     int sw_grid = 0;      // CTAs of the persistent sweep kernel
     size_t sw_smem = 0;
     int coarse_sweeps = 12;
+    int mg_pre = 1, mg_post = 2;  // multigrid sweeps before / after the coarse correction
     int max_W = 0;
     int cur = 0;
     long long steps_done = 0;
@@ -404,37 +405,40 @@ void make_tiles(int ilo, int ihi, int n1, int cid, std::vector<Tile>& out, int t
 
 // --------------------------------------------------------------------------
 // one time step of every case in the batch
+// planes of the pre-smoothed x and of the V-cycle result of a non-coarsest level: sweeps
+// alternate between x and r, starting in x
+int mg_pre_plane(int nu_pre) { return (nu_pre & 1) ? M_X : M_R; }
+int mg_res_plane(int nu_pre, int nu_post) {
+    const int p = mg_pre_plane(nu_pre);
+    return (nu_post & 1) ? (p == M_X ? M_R : M_X) : p;
+}
+
 int run_vcycle(cfd_batch* b) {
     BatchDev& bd = b->bd;
+    const int pre = mg_pre_plane(b->mg_pre);
     for (int l = 0; l < b->nlev_max; l++) {
         if (bd.nccases[l] > 0) {
             Prof pr(b, K_MG_COARSE);
             k_mg_coarse<<<bd.nccases[l], 1024, 0, b->st>>>(bd, l, b->coarse_sweeps);
         }
         if (bd.nmtiles[l] > 0) {
-            {   // pre-smoothing from the zero guess the restriction (or the Krylov step) left
+            for (int s = 0; s < b->mg_pre; s++) {  // pre-smoothing from zero
                 Prof pr(b, K_MG_SMOOTH);
-                k_mg_smooth_blk<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l, 0, 1);
+                const int dst = (s & 1) ? M_R : M_X;
+                k_mg_gs<<<bd.nmtiles[l], NT, kMgGsSmem, b->st>>>(bd, l, s == 0 ? 0 : 1, dst == M_X ? M_R : M_X, dst);
             }
-            {
-                Prof pr(b, K_MG_RESID);
-                k_mg_resid<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l);
-            }
-            {
-                Prof pr(b, K_MG_RESTRICT);
-                k_mg_restrict<<<bd.natiles[l + 1], NT, 0, b->st>>>(bd, l);
-            }
+            Prof pr(b, K_MG_RR);
+            k_mg_rr<<<bd.natiles[l + 1], NT, 0, b->st>>>(bd, l, pre);
         }
     }
     for (int l = b->nlev_max - 2; l >= 0; l--) {
         if (bd.nmtiles[l] == 0) continue;
-        {
-            Prof pr(b, K_MG_PROLONG);
-            k_mg_prolong<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l);
-        }
-        {
-            Prof pr(b, K_MG_SMOOTH);
-            k_mg_smooth_blk<<<bd.nmtiles[l], NT, 0, b->st>>>(bd, l, 1, 0);
+        int src = pre;
+        for (int s = 0; s < b->mg_post; s++) {
+            Prof pr(b, K_MG_POST);
+            const int dst = src == M_X ? M_R : M_X;
+            k_mg_gs<<<bd.nmtiles[l], NT, kMgGsSmem, b->st>>>(bd, l, s == 0 ? 2 : 3, src, dst);
+            src = dst;
         }
     }
     return CFD_OK;
@@ -604,6 +608,14 @@ int one_step(cfd_batch* b) {
 }
 
 // adds the loop launches of graph steps (from the cumulative device counters) to the count
+void drop_graphs(cfd_batch* b) {
+    for (int k = 0; k < 2; k++)
+        if (b->gexec[k]) {
+            cudaGraphExecDestroy(b->gexec[k]);
+            b->gexec[k] = nullptr;
+        }
+}
+
 int account_graph_launches(cfd_batch* b) {
     if (!b->use_graph) return CFD_OK;
     int dummy = 0;
@@ -806,7 +818,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
             L.tile_begin = (int)at[l].size();
             make_tiles(lg.ilo, lg.ihi, lg.n1, c, at[l]);
             L.tile_count = (int)at[l].size() - L.tile_begin;
-            if (l < d.nlev - 1) make_tiles(lg.ilo, lg.ihi, lg.n1, c, mt[l]);
+            if (l < d.nlev - 1) make_tiles(lg.ilo, lg.ihi, lg.n1, c, mt[l], TYJ);
             else cc[l].push_back(c);
             b->ncol[l] = std::max(b->ncol[l], (G.periodic && (lg.W & 1)) ? 6 : 4);
         }
@@ -873,6 +885,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         b->sw_grid = (int)jtiles.size();  // one CTA per 32 x 16 tile
         CK(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem));
         CK(cudaFuncSetAttribute(k_face_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFaceQSmem));
+        CK(cudaFuncSetAttribute(k_mg_gs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgGsSmem));
     }
 
     // ---- tile tables
@@ -939,6 +952,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
     bd.jtiles = b->dtiles + pos_jt; bd.njtiles = (int)jtiles.size();
     bd.error = b->flags + 4;
+    bd.mg_res = mg_res_plane(b->mg_pre, b->mg_post);
     bd.sweep_no = b->flags + 7;
     for (int l = 0; l < MAXLEV; l++) {
         bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
@@ -1009,8 +1023,7 @@ int cfd_batch_get_plane(cfd_batch* b, int case_index, const char* name, double* 
 int cfd_batch_destroy(cfd_batch* b) {
     if (!b) return CFD_OK;
     if (b->st) cudaStreamSynchronize(b->st);
-    for (int k = 0; k < 2; k++)
-        if (b->gexec[k]) cudaGraphExecDestroy(b->gexec[k]);
+    drop_graphs(b);
     for (auto& l : b->pending) { cudaEventDestroy(l.e0); cudaEventDestroy(l.e1); }
     for (auto e : b->pool) cudaEventDestroy(e);
     cudaFree(b->f64); cudaFree(b->f32); cudaFree(b->dc); cudaFree(b->scal); cudaFree(b->iscal);
@@ -1018,6 +1031,100 @@ int cfd_batch_destroy(cfd_batch* b) {
     if (b->h_flags) cudaFreeHost(b->h_flags);
     if (b->st) cudaStreamDestroy(b->st);
     delete b;
+    return CFD_OK;
+}
+
+int cfd_batch_set_mg(cfd_batch* b, int nu_pre, int nu_post, int coarse_sweeps) {
+    if (!b) return fail(CFD_E_ARG, "null batch");
+    if (nu_pre < 1 || nu_pre > 8 || nu_post < 1 || nu_post > 8 || coarse_sweeps < 1 || coarse_sweeps > 256)
+        return fail(CFD_E_ARG, "multigrid schedule out of range (sweeps 1..8, coarse sweeps 1..256)");
+    CK(cudaStreamSynchronize(b->st));
+    b->mg_pre = nu_pre;
+    b->mg_post = nu_post;
+    b->coarse_sweeps = coarse_sweeps;
+    b->bd.mg_res = mg_res_plane(nu_pre, nu_post);
+    drop_graphs(b);  // the step graphs hold the old schedule
+    return CFD_OK;
+}
+
+int cfd_batch_get_mg(cfd_batch* b, int* nu_pre, int* nu_post, int* coarse_sweeps) {
+    if (!b) return fail(CFD_E_ARG, "null batch");
+    if (nu_pre) *nu_pre = b->mg_pre;
+    if (nu_post) *nu_post = b->mg_post;
+    if (coarse_sweeps) *coarse_sweeps = b->coarse_sweeps;
+    return CFD_OK;
+}
+
+// Times each candidate multigrid schedule over `steps` steps from the batch's current state
+// (saved on the device and restored before every candidate and at the end), keeps the
+// fastest and reports its time per step. The batch's state is unchanged on return.
+int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule, double* out_ms_per_step) {
+    if (!b || steps < 1) return fail(CFD_E_ARG, "bad arguments");
+    static const int cand[][3] = {{1, 1, 12}, {1, 2, 12}, {2, 1, 12}, {2, 2, 12}, {1, 1, 24}, {1, 1, 6}, {2, 2, 24}};
+    const int ncand = (int)(sizeof(cand) / sizeof(cand[0]));
+    const size_t n64 = (size_t)b->n64 * sizeof(double), nsc = sizeof(double) * NSCAL * b->n,
+                 nis = sizeof(int) * NISCAL * b->n;
+    char* snap = nullptr;
+    CK(cudaStreamSynchronize(b->st));
+    if (cudaMalloc((void**)&snap, n64 + nsc + nis) != cudaSuccess)
+        return fail(CFD_E_OOM, "autotune: no device memory for the state snapshot");
+    const int cur0 = b->cur;
+    const long long steps0 = b->steps_done, launches0 = b->launches;
+    auto copy = [&](bool save) -> int {
+        char* p = snap;
+        const void* src[3] = {b->f64, b->scal, b->iscal};
+        void* dst[3] = {b->f64, b->scal, b->iscal};
+        const size_t nb[3] = {n64, nsc, nis};
+        for (int k = 0; k < 3; k++) {
+            cudaError_t e = save ? cudaMemcpyAsync(p, src[k], nb[k], cudaMemcpyDeviceToDevice, b->st)
+                                 : cudaMemcpyAsync(dst[k], p, nb[k], cudaMemcpyDeviceToDevice, b->st);
+            if (e != cudaSuccess) return fail(CFD_E_CUDA, "autotune: snapshot copy failed");
+            p += nb[k];
+        }
+        b->cur = cur0;
+        b->steps_done = steps0;
+        return CFD_OK;
+    };
+    const int mp = b->mg_pre, mq = b->mg_post, mc = b->coarse_sweeps;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int rc = copy(true), best = -1;
+    float best_ms = 0.f;
+    for (int k = 0; k < ncand && !rc; k++) {
+        rc = cfd_batch_set_mg(b, cand[k][0], cand[k][1], cand[k][2]);
+        if (!rc) rc = copy(false);
+        if (!rc) rc = cfd_batch_step(b, 1);  // builds the step graphs of this schedule
+        if (!rc) rc = copy(false);
+        if (rc) break;
+        cudaEventRecord(e0, b->st);
+        rc = cfd_batch_step(b, steps);
+        cudaEventRecord(e1, b->st);
+        if (rc) break;
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (best < 0 || ms < best_ms) {
+            best = k;
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int rc2 = rc ? cfd_batch_set_mg(b, mp, mq, mc) : cfd_batch_set_mg(b, cand[best][0], cand[best][1], cand[best][2]);
+    int rc3 = copy(false);
+    if (!rc3) rc3 = cudaStreamSynchronize(b->st) == cudaSuccess ? CFD_OK : fail(CFD_E_CUDA, "autotune sync");
+    cudaFree(snap);
+    b->launches = launches0;
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if (rc3) return rc3;
+    if (out_schedule) {
+        out_schedule[0] = cand[best][0];
+        out_schedule[1] = cand[best][1];
+        out_schedule[2] = cand[best][2];
+    }
+    if (out_ms_per_step) *out_ms_per_step = best_ms / steps;
     return CFD_OK;
 }
 

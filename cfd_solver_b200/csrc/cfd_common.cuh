@@ -134,7 +134,7 @@ struct BatchDev {
     int nftiles;
     const Tile* jtiles;    // 32 x 16 tiles of every case (u/v/T sweeps)
     int njtiles;
-    const Tile* mtiles[MAXLEV];   // level-l tiles of the cases for which l is not the coarsest level
+    const Tile* mtiles[MAXLEV];   // level-l 32 x 16 tiles of the cases for which l is not the coarsest level
     int nmtiles[MAXLEV];
     const Tile* atiles[MAXLEV];   // level-l tiles of every case that has level l (set-up)
     int natiles[MAXLEV];
@@ -143,6 +143,7 @@ struct BatchDev {
     unsigned long long* work;  // [0] field-cells and [1] cells swept by k_jac, [2] field-cells of sweep 0
     const char* tmaps;     // per case TMAP_STRIDE bytes of CUtensorMaps (TMAP_* offsets)
     int cur;               // which of T0/T1 (up0/up1, vp0/vp1) holds the current state
+    int mg_res;            // multigrid plane (M_X or M_R) holding a non-coarsest level's V-cycle result
 };
 
 // ------------------------------------------------------------------------

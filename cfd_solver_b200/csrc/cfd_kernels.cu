@@ -29,6 +29,12 @@ namespace cfd {
 constexpr int JTW = TX + 4;   // 32 x 16 tile columns incl. a 2-cell halo
 constexpr int JTH = TYJ + 4;  // 32 x 16 tile rows incl. a 2-cell halo
 
+// plane that holds the final multigrid V-cycle result of level l of case c (x on the
+// case's coarsest level; otherwise fixed by the numbers of pre- and post-sweeps)
+__device__ __forceinline__ int mg_result_plane(const BatchDev& b, const CaseDev& c, int l) {
+    return l == c.nlev - 1 ? M_X : b.mg_res;
+}
+
 __device__ __forceinline__ bool near_wall(const CaseDev& c, int i, int j) {
     if (j == 1 || j == c.n1 - 2) return true;
     return c.profile == CAVITY && (i == 1 || i == c.n0 - 2);
@@ -527,7 +533,7 @@ __global__ void __launch_bounds__(NT) k_spmv(BatchDev b, int mode) {
         const int ld = c.ld;
         const LevelDev& L = c.lev[0];
         const int l0 = L.ld;
-        const float* X = mplane(b, L, M_X);
+        const float* X = mplane(b, L, mg_result_plane(b, c, 0));
         const long long k = (long long)j * ld + i, q = (long long)j * l0 + i;
         const double xc = (double)X[q];
         const double y = plane(b, c, P_AP)[k] * xc + plane(b, c, P_AE)[k] * (double)X[q + 1] +
@@ -563,25 +569,47 @@ __global__ void __launch_bounds__(NT) k_spmv(BatchDev b, int mode) {
     }
 }
 
+// s = r - alpha v, and the half step x += alpha p_hat; when |s| already meets the stop rule
+// the solve ends here (the standard early exit: x + alpha p_hat is the iterate whose
+// residual is s) and the second preconditioner application of the iteration is skipped
 __global__ void __launch_bounds__(NT) k_bicg_s(BatchDev b) {
     const Tile t = b.ftiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const bool first = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
     const CaseDev& c = b.cases[t.c];
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
-    if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
     const double alpha = b.scal[(long long)t.c * NSCAL + S_ALPHA];
-    const long long k = (long long)j * c.ld + i;
-    const double s = plane(b, c, P_KR)[k] - alpha * plane(b, c, P_KV)[k];
-    plane(b, c, P_KS)[k] = s;
-    const LevelDev& L = c.lev[0];
-    mplane(b, L, M_B)[(long long)j * L.ld + i] = (float)s;
-    store_mirrored(mplane(b, L, M_X), L.ld, i, j, L.W, c.periodic, 0.0f);
+    double red[1] = {0.0};
+    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
+        const long long k = (long long)j * c.ld + i;
+        double* X = plane(b, c, P_PCOR);
+        const double x0 = first ? 0.0 : X[k];
+        const double s = plane(b, c, P_KR)[k] - alpha * plane(b, c, P_KV)[k];
+        const double x = x0 + alpha * plane(b, c, P_KPH)[k];
+        plane(b, c, P_KS)[k] = s;
+        store_mirrored(X, c.ld, i, j, c.W, c.periodic, x);
+        const LevelDev& L = c.lev[0];
+        mplane(b, L, M_B)[(long long)j * L.ld + i] = (float)s;
+        store_mirrored(mplane(b, L, M_X), L.ld, i, j, L.W, c.periodic, 0.0f);
+        red[0] = fabs(s);
+    }
+    if (case_reduce<1, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0) {
+        double* sc = b.scal + (long long)t.c * NSCAL;
+        int* is = b.iscal + (long long)t.c * NISCAL;
+        const bool conv = red[0] <= c.tol_p * sc[S_NB1] || red[0] <= c.atol_p;
+        if (conv || !isfinite(red[0])) {
+            is[I_PIT] += 1;
+            sc[S_RL1] = red[0];
+            if (!isfinite(red[0])) is[I_STATUS] |= ST_NAN;
+            is[I_PDONE] = 1;
+            atomicSub(b.active, 1);
+        }
+    }
 }
 
 __global__ void __launch_bounds__(NT) k_bicg_x(BatchDev b, int maxit) {
     const Tile t = b.ftiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
-    const bool first = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
     const CaseDev& c = b.cases[t.c];
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
     const double* sc0 = b.scal + (long long)t.c * NSCAL;
@@ -591,7 +619,8 @@ __global__ void __launch_bounds__(NT) k_bicg_x(BatchDev b, int maxit) {
         const int ld = c.ld;
         const long long k = (long long)j * ld + i;
         double* X = plane(b, c, P_PCOR);
-        const double x = (first ? 0.0 : X[k]) + alpha * plane(b, c, P_KPH)[k] + omega * plane(b, c, P_KSH)[k];
+        // x already carries the half step alpha p_hat (k_bicg_s)
+        const double x = X[k] + omega * plane(b, c, P_KSH)[k];
         store_mirrored(X, ld, i, j, c.W, c.periodic, x);
         const double r = plane(b, c, P_KS)[k] - omega * plane(b, c, P_KT)[k];
         plane(b, c, P_KR)[k] = r;
@@ -620,164 +649,235 @@ __global__ void __launch_bounds__(NT) k_bicg_x(BatchDev b, int maxit) {
 }
 
 // ---------------------------------------------------------------------------
-// multigrid preconditioner, FP32, level tiles
+// multigrid preconditioner, FP32, level tiles.
+//
+// One V-cycle: on the way down, level l is pre-smoothed from zero (k_mg_gs, post = 0:
+// writes x_l), then its residual is formed and restricted in one pass (k_mg_rr: writes
+// b_{l+1}); the coarsest level of each case is smoothed by one CTA (k_mg_coarse, in place
+// in x); on the way up, k_mg_gs (post = 1) adds the prolonged coarse result and
+// post-smooths in one pass, writing the level's result into its r plane. No kernel reads a
+// plane that another CTA of the same launch writes, so the V-cycle is a fixed linear map
+// (the same bits whatever the CTA schedule), as the Krylov method needs. The level's
+// final result lives in r (x for a case whose coarsest level it is).
 __device__ __forceinline__ int mg_colour(int i, int j, int W, int periodic) {
     // 4 colours by parity; an odd periodic width gets 2 extra colours for its last column
     if (periodic && (W & 1) && i == W - 1) return 4 + (j & 1);
     return (i & 1) | ((j & 1) << 1);
 }
 
-__global__ void __launch_bounds__(NT) k_mg_smooth(BatchDev b, int l, int colour) {
-    const Tile t = b.mtiles[l][blockIdx.x];
-    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
-    const CaseDev& c = b.cases[t.c];
-    const LevelDev& L = c.lev[l];
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
-    if (i < L.ilo || i > L.ihi || j > L.n1 - 2) return;
-    if (mg_colour(i, j, L.W, c.periodic) != colour) return;
-    const int ld = L.ld;
-    const long long k = (long long)j * ld + i;
-    float* X = mplane(b, L, M_X);
-    const float s = mplane(b, L, M_AE)[k] * X[k + 1] + mplane(b, L, M_AW)[k] * X[k - 1] +
-                    mplane(b, L, M_AN)[k] * X[k + ld] + mplane(b, L, M_AS)[k] * X[k - ld] +
-                    mplane(b, L, M_ANE)[k] * X[k + ld + 1] + mplane(b, L, M_ANW)[k] * X[k + ld - 1] +
-                    mplane(b, L, M_ASE)[k] * X[k - ld + 1] + mplane(b, L, M_ASW)[k] * X[k - ld - 1];
-    store_mirrored(X, ld, i, j, L.W, c.periodic, (mplane(b, L, M_B)[k] - s) / mplane(b, L, M_AP)[k]);
-}
 
-// One full multicolour Gauss-Seidel sweep per launch: the CTA keeps its tile of x plus a
-// one-cell halo in shared memory and sweeps the colours in order (reverse when `reverse`),
-// with a barrier between colours. Neighbouring tiles' values stay as they were at the start
-// of the sweep (block Gauss-Seidel at tile edges), so the smoother is a fixed linear map.
-// zero_init: the level's x is zero on entry (first smoothing after a restriction).
-__global__ void __launch_bounds__(NT) k_mg_smooth_blk(BatchDev b, int l, int reverse, int zero_init) {
-    __shared__ float xs[(TY + 2) * (TX + 2)];
-    const Tile t = b.mtiles[l][blockIdx.x];
-    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
-    const CaseDev& c = b.cases[t.c];
-    const LevelDev& L = c.lev[l];
-    const int tid = threadIdx.x, li = tid % TX, lj = tid / TX;
-    const int i = t.i0 + li, j = t.j0 + lj;
-    const int ld = L.ld;
-    float* X = mplane(b, L, M_X);
-    constexpr int SW = TX + 2;
-    // load the tile + halo (rows j0-1 .. j0+TY, columns i0-1 .. i0+TX), clamped to the plane
-    for (int e = tid; e < (TY + 2) * SW; e += NT) {
-        const int r = e / SW, q = e % SW;
-        const int gj = t.j0 - 1 + r, gi = t.i0 - 1 + q;
-        float v = 0.0f;
-        if (!zero_init && gj >= 0 && gj < L.n1 && gi >= -H && gi < L.W + H) v = X[(long long)gj * ld + gi];
-        xs[e] = v;
-    }
-    const bool in = i >= L.ilo && i <= L.ihi && j <= L.n1 - 2;
-    float ap = 1.f, ae = 0.f, aw = 0.f, an = 0.f, as = 0.f, ane = 0.f, anw = 0.f, ase = 0.f, asw = 0.f, bv = 0.f;
-    int col = -1;
-    if (in) {
-        const long long k = (long long)j * ld + i;
-        ap = mplane(b, L, M_AP)[k]; ae = mplane(b, L, M_AE)[k]; aw = mplane(b, L, M_AW)[k];
-        an = mplane(b, L, M_AN)[k]; as = mplane(b, L, M_AS)[k]; ane = mplane(b, L, M_ANE)[k];
-        anw = mplane(b, L, M_ANW)[k]; ase = mplane(b, L, M_ASE)[k]; asw = mplane(b, L, M_ASW)[k];
-        bv = mplane(b, L, M_B)[k];
-        col = mg_colour(i, j, L.W, c.periodic);
-    }
-    __syncthreads();
-    const int ncol = (c.periodic && (L.W & 1)) ? 6 : 4;
-    const int o = (lj + 1) * SW + (li + 1);
-    for (int n = 0; n < ncol; n++) {
-        const int cc = reverse ? ncol - 1 - n : n;
-        if (col == cc) {
-            const float s = ae * xs[o + 1] + aw * xs[o - 1] + an * xs[o + SW] + as * xs[o - SW] +
-                            ane * xs[o + SW + 1] + anw * xs[o + SW - 1] + ase * xs[o - SW + 1] +
-                            asw * xs[o - SW - 1];
-            xs[o] = (bv - s) / ap;
-        }
-        __syncthreads();
-    }
-    if (in) store_mirrored(X, ld, i, j, L.W, c.periodic, xs[o]);
-}
-
-__global__ void __launch_bounds__(NT) k_mg_resid(BatchDev b, int l) {
-    const Tile t = b.mtiles[l][blockIdx.x];
-    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
-    const CaseDev& c = b.cases[t.c];
-    const LevelDev& L = c.lev[l];
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
-    if (i < L.ilo || i > L.ihi || j > L.n1 - 2) return;
-    const int ld = L.ld;
-    const long long k = (long long)j * ld + i;
-    const float* X = mplane(b, L, M_X);
-    const float ax = mplane(b, L, M_AP)[k] * X[k] + mplane(b, L, M_AE)[k] * X[k + 1] +
-                     mplane(b, L, M_AW)[k] * X[k - 1] + mplane(b, L, M_AN)[k] * X[k + ld] +
-                     mplane(b, L, M_AS)[k] * X[k - ld] + mplane(b, L, M_ANE)[k] * X[k + ld + 1] +
-                     mplane(b, L, M_ANW)[k] * X[k + ld - 1] + mplane(b, L, M_ASE)[k] * X[k - ld + 1] +
-                     mplane(b, L, M_ASW)[k] * X[k - ld - 1];
-    store_mirrored(mplane(b, L, M_R), ld, i, j, L.W, c.periodic, mplane(b, L, M_B)[k] - ax);
-}
-
-// full-weighting restriction of level l's residual into level l+1 (tiles of level l+1)
-__global__ void __launch_bounds__(NT) k_mg_restrict(BatchDev b, int l) {
+// Residual r = b - A x of level l on the fine points a coarse tile of level l + 1 needs,
+// in shared memory, then full-weighting restriction into b_{l+1} (tiles of level l + 1;
+// x_{l+1} is zeroed for the coarse solve). Fine points that are not unknowns contribute 0.
+__global__ void __launch_bounds__(NT) k_mg_rr(BatchDev b, int l, int src) {
+    constexpr int RW = 2 * TX + 1, RH = 2 * TY + 1;  // fine residual region
+    constexpr int XW = RW + 2, XH = RH + 2;          // fine x region (one-cell halo)
+    __shared__ float xs[XH * XW];
+    __shared__ float rs[RH * RW];
     const Tile t = b.atiles[l + 1][blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
     const LevelDev& F = c.lev[l];
     const LevelDev& C = c.lev[l + 1];
-    const int I = t.i0 + (int)(threadIdx.x % TX), J = t.j0 + (int)(threadIdx.x / TX);
+    const int tid = threadIdx.x;
+    const int fl = F.ld, per = c.periodic;
+    const int fi0 = 2 * t.i0 - 1, fj0 = 2 * t.j0 - 1;
+    const float* X = mplane(b, F, src);
+    for (int e = tid; e < XH * XW; e += NT) {
+        const int gj = fj0 - 1 + e / XW, gi = fi0 - 1 + e % XW;
+        float v = 0.0f;
+        if (gj >= 0 && gj < F.n1 && gi >= -H && gi < F.W + H) v = X[(long long)gj * fl + gi];
+        xs[e] = v;
+    }
+    __syncthreads();
+    // fine unknown columns in stored form: periodic -1 .. W (halo mirrors), else ilo .. ihi
+    const int clo = per ? -1 : F.ilo, chi = per ? F.W : F.ihi;
+    for (int e = tid; e < RH * RW; e += NT) {
+        const int rj = e / RW, ri = e % RW;
+        const int gj = fj0 + rj, gi = fi0 + ri;
+        float r = 0.0f;
+        if (gj >= 1 && gj <= F.n1 - 2 && gi >= clo && gi <= chi) {
+            const long long k = (long long)gj * fl + gi;
+            const int o = (rj + 1) * XW + (ri + 1);
+            const float ax = mplane(b, F, M_AP)[k] * xs[o] + mplane(b, F, M_AE)[k] * xs[o + 1] +
+                             mplane(b, F, M_AW)[k] * xs[o - 1] + mplane(b, F, M_AN)[k] * xs[o + XW] +
+                             mplane(b, F, M_AS)[k] * xs[o - XW] + mplane(b, F, M_ANE)[k] * xs[o + XW + 1] +
+                             mplane(b, F, M_ANW)[k] * xs[o + XW - 1] + mplane(b, F, M_ASE)[k] * xs[o - XW + 1] +
+                             mplane(b, F, M_ASW)[k] * xs[o - XW - 1];
+            r = mplane(b, F, M_B)[k] - ax;
+        }
+        rs[e] = r;
+    }
+    __syncthreads();
+    const int li = tid % TX, lj = tid / TX;
+    const int I = t.i0 + li, J = t.j0 + lj;
     if (I < C.ilo || I > C.ihi || J > C.n1 - 2) return;
-    const int fl = F.ld;
-    const float* R = mplane(b, F, M_R);
-    const long long f = (long long)(2 * J) * fl + 2 * I;
-    const float v = 0.0625f * (R[f - fl - 1] + R[f - fl + 1] + R[f + fl - 1] + R[f + fl + 1]) +
-                    0.125f * (R[f - fl] + R[f + fl] + R[f - 1] + R[f + 1]) + 0.25f * R[f];
+    const int f = (2 * lj + 1) * RW + (2 * li + 1);  // fine (2I, 2J) in the residual region
+    const float v = 0.0625f * (rs[f - RW - 1] + rs[f - RW + 1] + rs[f + RW - 1] + rs[f + RW + 1]) +
+                    0.125f * (rs[f - RW] + rs[f + RW] + rs[f - 1] + rs[f + 1]) + 0.25f * rs[f];
     const long long kc = (long long)J * C.ld + I;
     mplane(b, C, M_B)[kc] = v;
-    store_mirrored(mplane(b, C, M_X), C.ld, I, J, C.W, c.periodic, 0.0f);
+    store_mirrored(mplane(b, C, M_X), C.ld, I, J, C.W, per, 0.0f);
 }
 
-// bilinear prolongation + correction of level l from level l+1 (tiles of level l)
-__global__ void __launch_bounds__(NT) k_mg_prolong(BatchDev b, int l) {
+// bilinear prolongation of the coarse result at fine point (i, j), i in [0, W)
+__device__ __forceinline__ float mg_prolong_at(const float* XC, int cl, int i, int j) {
+    const int I = i >> 1, J = j >> 1;
+    const long long q = (long long)J * cl + I;
+    if (!(i & 1) && !(j & 1)) return XC[q];
+    if (!(j & 1)) return 0.5f * (XC[q] + XC[q + 1]);
+    if (!(i & 1)) return 0.5f * (XC[q] + XC[q + cl]);
+    return 0.25f * (XC[q] + XC[q + 1] + XC[q + cl] + XC[q + cl + 1]);
+}
+
+// One multicolour Gauss-Seidel sweep of level l on a 32 x 16 tile (block Gauss-Seidel at
+// tile edges: the halo ring holds the neighbouring tiles' values from before the sweep,
+// plus a redundantly relaxed overlap of MGS_OV cells). The sweep reads plane `src` and
+// writes plane `dst` != src, so nothing is read that another CTA writes.
+//   mode 0: from x = 0, colours in order (first pre-sweep; src unused)
+//   mode 1: from src, colours in order (further pre-sweeps)
+//   mode 2: from src plus the prolonged result of level l + 1, colours reversed (first
+//           post-sweep)
+//   mode 3: from src, colours reversed (further post-sweeps)
+constexpr int MGS_OV = 0;                          // overlap relaxed redundantly around the tile
+constexpr int MGS_OVM = MGS_OV;
+constexpr int MGS_RW = TX + 2 * MGS_OVM, MGS_RH = TYJ + 2 * MGS_OVM;
+constexpr int MGS_XW = MGS_RW + 2, MGS_XH = MGS_RH + 2;
+constexpr size_t MGS_SMEM = (size_t)(MGS_XH * MGS_XW + 10 * MGS_RW * MGS_RH) * sizeof(float) + MGS_RW * MGS_RH;
+const size_t kMgGsSmem = MGS_SMEM;
+__global__ void __launch_bounds__(NT) k_mg_gs(BatchDev b, int l, int mode, int src, int dst) {
+    extern __shared__ __align__(16) unsigned char mgraw[];
+    float* xs = reinterpret_cast<float*>(mgraw);
+    float(*cf)[MGS_RW * MGS_RH] = reinterpret_cast<float(*)[MGS_RW * MGS_RH]>(xs + MGS_XH * MGS_XW);
+    // cf: ap, ae, aw, an, as, ane, anw, ase, asw, b of every relaxed point
+    signed char* colr = reinterpret_cast<signed char*>(xs + MGS_XH * MGS_XW + 10 * MGS_RW * MGS_RH);
     const Tile t = b.mtiles[l][blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
-    const LevelDev& F = c.lev[l];
-    const LevelDev& C = c.lev[l + 1];
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
-    if (i < F.ilo || i > F.ihi || j > F.n1 - 2) return;
-    const float* XC = mplane(b, C, M_X);
-    const int cl = C.ld;
-    const int I = i >> 1, J = j >> 1;
-    const long long q = (long long)J * cl + I;
-    float v;
-    if (!(i & 1) && !(j & 1)) v = XC[q];
-    else if (!(j & 1)) v = 0.5f * (XC[q] + XC[q + 1]);
-    else if (!(i & 1)) v = 0.5f * (XC[q] + XC[q + cl]);
-    else v = 0.25f * (XC[q] + XC[q + 1] + XC[q + cl] + XC[q + cl + 1]);
-    float* X = mplane(b, F, M_X);
-    const long long k = (long long)j * F.ld + i;
-    store_mirrored(X, F.ld, i, j, F.W, c.periodic, X[k] + v);
+    const LevelDev& L = c.lev[l];
+    const int tid = threadIdx.x;
+    const int ld = L.ld, W = L.W, per = c.periodic, n1 = L.n1;
+    const int ncol = (per && (W & 1)) ? 6 : 4;
+    const int ov = MGS_OV;
+    const int rw = TX + 2 * ov, rh = TYJ + 2 * ov, xw = rw + 2, xh = rh + 2;
+    const bool zero = mode == 0, prolong = mode == 2, reverse = mode >= 2;
+    const float* X = mplane(b, L, src);
+    const float* XC = prolong ? mplane(b, c.lev[l + 1], mg_result_plane(b, c, l + 1)) : nullptr;
+    const int cl = prolong ? c.lev[l + 1].ld : 0;
+    // stored column of global column gi (periodic wrap), or -1 outside the level
+    auto column = [&](int gi) -> int {
+        if (per) return ((gi % W) + W) % W;
+        return (gi >= 0 && gi < W) ? gi : -1;
+    };
+    for (int e = tid; e < xh * xw; e += NT) {
+        const int gj = t.j0 - ov - 1 + e / xw, col = column(t.i0 - ov - 1 + e % xw);
+        float v = 0.0f;
+        if (!zero && gj >= 0 && gj < n1 && col >= 0) {
+            v = X[(long long)gj * ld + col];
+            if (prolong && gj >= 1 && gj <= n1 - 2 && col >= L.ilo && col <= L.ihi)
+                v += mg_prolong_at(XC, cl, col, gj);
+        }
+        xs[e] = v;
+    }
+    for (int e = tid; e < rh * rw; e += NT) {
+        const int gj = t.j0 - ov + e / rw, col = column(t.i0 - ov + e % rw);
+        signed char cc = -1;
+        if (gj >= 1 && gj <= n1 - 2 && col >= L.ilo && col <= L.ihi) {
+            const long long k = (long long)gj * ld + col;
+#pragma unroll
+            for (int m = 0; m < 9; m++) cf[m][e] = mplane(b, L, M_AP + m)[k];
+            cf[9][e] = mplane(b, L, M_B)[k];
+            cc = (signed char)mg_colour(col, gj, W, per);
+        }
+        colr[e] = cc;
+    }
+    __syncthreads();
+    for (int n = 0; n < ncol; n++) {
+        const int cc = reverse ? ncol - 1 - n : n;
+        for (int e = tid; e < rh * rw; e += NT) {
+            if (colr[e] != cc) continue;
+            const int o = (e / rw + 1) * xw + (e % rw + 1);
+            const float s = cf[1][e] * xs[o + 1] + cf[2][e] * xs[o - 1] + cf[3][e] * xs[o + xw] +
+                            cf[4][e] * xs[o - xw] + cf[5][e] * xs[o + xw + 1] + cf[6][e] * xs[o + xw - 1] +
+                            cf[7][e] * xs[o - xw + 1] + cf[8][e] * xs[o - xw - 1];
+            xs[o] = (cf[9][e] - s) / cf[0][e];
+        }
+        __syncthreads();
+    }
+    float* OUT = mplane(b, L, dst);
+    for (int e = tid; e < TX * TYJ; e += NT) {
+        const int i = t.i0 + e % TX, j = t.j0 + e / TX;
+        if (i < L.ilo || i > L.ihi || j > n1 - 2) continue;
+        store_mirrored(OUT, ld, i, j, W, per, xs[(e / TX + ov + 1) * xw + (e % TX + ov + 1)]);
+    }
 }
 
-// coarsest level: `sweeps` multicolour GS sweeps by one CTA per case
-__global__ void __launch_bounds__(1024) k_mg_coarse(BatchDev b, int l, int sweeps) {
+// coarsest level: `sweeps` multicolour GS sweeps by one CTA per case, x in shared memory
+// and each thread's stencil in registers when the level fits (one unknown per thread);
+// larger levels (a case whose grid does not coarsen) sweep through global memory
+constexpr int MGC_THREADS = 1024, MGC_SMEM = 4096;
+__global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse(BatchDev b, int l, int sweeps) {
+    __shared__ float xs[MGC_SMEM];
     const int cid = b.ccases[l][blockIdx.x];
     if (b.iscal[(long long)cid * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[cid];
     const LevelDev& L = c.lev[l];
-    const int ld = L.ld;
+    const int ld = L.ld, per = c.periodic;
     const int nx = L.ihi - L.ilo + 1, ny = L.n1 - 2;
     float* X = mplane(b, L, M_X);
     const float* Bv = mplane(b, L, M_B);
-    const int ncol = (c.periodic && (L.W & 1)) ? 6 : 4;
+    const int ncol = (per && (L.W & 1)) ? 6 : 4;
+    const int sw = L.W + 2 * H;  // shared copy: all rows, columns -H .. W+H-1
+    if (nx * ny <= MGC_THREADS && L.n1 * sw <= MGC_SMEM) {
+        for (int e = threadIdx.x; e < L.n1 * sw; e += MGC_THREADS) xs[e] = 0.0f;  // x = 0 (and boundaries)
+        const int e = threadIdx.x;
+        const bool in = e < nx * ny;
+        const int i = L.ilo + (in ? e % nx : 0), j = 1 + (in ? e / nx : 0);
+        const long long k = (long long)j * ld + i;
+        float ap = 1.f, ae = 0.f, aw = 0.f, an = 0.f, as = 0.f, ane = 0.f, anw = 0.f, ase = 0.f, asw = 0.f, bv = 0.f;
+        int col = -1;
+        if (in) {
+            ap = mplane(b, L, M_AP)[k]; ae = mplane(b, L, M_AE)[k]; aw = mplane(b, L, M_AW)[k];
+            an = mplane(b, L, M_AN)[k]; as = mplane(b, L, M_AS)[k]; ane = mplane(b, L, M_ANE)[k];
+            anw = mplane(b, L, M_ANW)[k]; ase = mplane(b, L, M_ASE)[k]; asw = mplane(b, L, M_ASW)[k];
+            bv = Bv[k];
+            col = mg_colour(i, j, L.W, per);
+        }
+        const int o = j * sw + i + H;
+        const int m = mirror_col(i, L.W, per);
+        __syncthreads();
+        for (int s = 0; s < sweeps; s++) {
+            for (int cc = 0; cc < ncol; cc++) {
+                if (col == cc) {
+                    const float sm = ae * xs[o + 1] + aw * xs[o - 1] + an * xs[o + sw] + as * xs[o - sw] +
+                                     ane * xs[o + sw + 1] + anw * xs[o + sw - 1] + ase * xs[o - sw + 1] +
+                                     asw * xs[o - sw - 1];
+                    const float v = (bv - sm) / ap;
+                    xs[o] = v;
+                    if (m > -1000000) xs[j * sw + m + H] = v;
+                }
+                __syncthreads();
+            }
+        }
+        if (in) store_mirrored(X, ld, i, j, L.W, per, xs[o]);
+        return;
+    }
+    for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {  // x = 0
+        const int i = L.ilo + e % nx, j = 1 + e / nx;
+        store_mirrored(X, ld, i, j, L.W, per, 0.0f);
+    }
+    __syncthreads();
     for (int s = 0; s < sweeps; s++) {
         for (int col = 0; col < ncol; col++) {
             for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
                 const int i = L.ilo + e % nx, j = 1 + e / nx;
-                if (mg_colour(i, j, L.W, c.periodic) != col) continue;
+                if (mg_colour(i, j, L.W, per) != col) continue;
                 const long long k = (long long)j * ld + i;
                 const float sm = mplane(b, L, M_AE)[k] * X[k + 1] + mplane(b, L, M_AW)[k] * X[k - 1] +
                                  mplane(b, L, M_AN)[k] * X[k + ld] + mplane(b, L, M_AS)[k] * X[k - ld] +
                                  mplane(b, L, M_ANE)[k] * X[k + ld + 1] + mplane(b, L, M_ANW)[k] * X[k + ld - 1] +
                                  mplane(b, L, M_ASE)[k] * X[k - ld + 1] + mplane(b, L, M_ASW)[k] * X[k - ld - 1];
-                store_mirrored(X, ld, i, j, L.W, c.periodic, (Bv[k] - sm) / mplane(b, L, M_AP)[k]);
+                store_mirrored(X, ld, i, j, L.W, per, (Bv[k] - sm) / mplane(b, L, M_AP)[k]);
             }
             __syncthreads();
         }

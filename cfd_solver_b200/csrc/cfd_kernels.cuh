@@ -13,11 +13,9 @@ __global__ void k_bicg_p(BatchDev b);
 __global__ void k_spmv(BatchDev b, int mode);
 __global__ void k_bicg_s(BatchDev b);
 __global__ void k_bicg_x(BatchDev b, int maxit);
-__global__ void k_mg_smooth(BatchDev b, int l, int colour);
-__global__ void k_mg_smooth_blk(BatchDev b, int l, int reverse, int zero_init);
-__global__ void k_mg_resid(BatchDev b, int l);
-__global__ void k_mg_restrict(BatchDev b, int l);
-__global__ void k_mg_prolong(BatchDev b, int l);
+__global__ void k_mg_gs(BatchDev b, int l, int mode, int src, int dst);
+extern const size_t kMgGsSmem;  // dynamic shared memory of k_mg_gs
+__global__ void k_mg_rr(BatchDev b, int l, int src);
 __global__ void k_mg_coarse(BatchDev b, int l, int sweeps);
 __global__ void k_mg_galerkin(BatchDev b, int l, int toff);
 __global__ void k_correct(BatchDev b);

@@ -127,6 +127,16 @@ size_t cfd_case_bytes(int n0, int n1, int profile);
 /* the stats of every case (cap entries at most), one device -> host copy */
 int cfd_batch_fetch_stats(cfd_batch* b, cfd_step_stats* out, int cap);
 
+/* ---- multigrid schedule of the pressure preconditioner (no counterpart in the reference,
+ * whose SIP solver has none): pre- and post-sweeps per level (1..8) and sweeps on the
+ * coarsest level (1..256); defaults 1, 2, 12. cfd_batch_autotune() times a fixed list of
+ * candidate schedules over `steps` steps each from the batch's current state (restored
+ * before each candidate and on return, so the batch continues exactly where it was),
+ * keeps the fastest and reports it as {pre, post, coarse} with its time per step. */
+int cfd_batch_set_mg(cfd_batch* b, int nu_pre, int nu_post, int coarse_sweeps);
+int cfd_batch_get_mg(cfd_batch* b, int* nu_pre, int* nu_post, int* coarse_sweeps);
+int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule3, double* out_ms_per_step);
+
 /* ---- slots: continuous batching over a batch of fixed-geometry slots ----
  * Every case of a batch is a slot. cfd_batch_admit() writes a new case into slot `slot`
  * (same n0, n1 and profile as the slot): grid, initial state, parameters and its pressure

@@ -1,0 +1,73 @@
+"""Multigrid preconditioner: determinism, schedule independence, autotuner.
+
+Every multigrid kernel reads planes that no other CTA of the same launch writes, so
+the V-cycle is a fixed linear map and a run gives the same bits every time. At a
+tight pressure tolerance the step is a property of the discretisation, so every
+smoother schedule gives the same fields (1e-9 relative). The autotuner times
+candidate schedules from a device snapshot of the state and restores it.
+"""
+import numpy as np
+import pytest
+
+from cfd_solver_b200.grid import cavity, ogrid
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    from cfd_solver_b200.solver import case_params
+    gs = [ogrid(65, 49, skew=0.12), ogrid(129, 65, skew=0.05), cavity(65, 65, skew=0.15), cavity(97, 97, skew=0.1)]
+    ps = [case_params(gs[0], Re=300.0, Ri=1.0, dt=1e-3), case_params(gs[1], Re=120.0, Ri=0.3, dt=2e-3),
+          case_params(gs[2], Re=200.0, Ri=2.0, dt=2e-3), case_params(gs[3], Re=400.0, Ri=0.5, Pr=7.0, dt=1e-3)]
+    return gs, ps
+
+
+def _run(schedule=None, steps=6, tight=False):
+    from cfd_solver_b200.solver import Batch, case_params
+    gs, ps = _cases()
+    if tight:
+        for p in ps:
+            p.tol_p, p.atol_p, p.maxit_p = 1e-11, 1e-13, 400
+    with Batch(gs, ps) as b:
+        if schedule:
+            b.set_mg(*schedule)
+        b.step(steps)
+        return [{k: b.plane(c, k) for k in ("u", "v", "T", "p", "pcor")} for c in range(len(gs))]
+
+
+def test_runs_are_bitwise_reproducible():
+    a, b = _run(), _run()
+    for fa, fb in zip(a, b):
+        for k in fa:
+            np.testing.assert_array_equal(fa[k], fb[k], err_msg=k)
+
+
+def test_schedules_agree_at_tight_tolerance():
+    ref = _run((1, 1, 12), tight=True)
+    for sch in [(2, 2, 12), (1, 2, 24), (2, 1, 6)]:
+        got = _run(sch, tight=True)
+        for fr, fg in zip(ref, got):
+            for k in ("u", "v", "T"):
+                d = np.linalg.norm(fg[k] - fr[k]) / max(np.linalg.norm(fr[k]), 1e-300)
+                assert d < 1e-9, (sch, k, d)
+
+
+def test_autotune_keeps_state():
+    from cfd_solver_b200.solver import Batch
+    gs, ps = _cases()
+    with Batch(gs, ps) as b:
+        b.step(3)
+        (pre, post, coarse), ms = b.autotune(steps=3)
+        assert ms > 0 and b.get_mg() == (pre, post, coarse)
+        b.step(4)
+        got = [{k: b.plane(c, k) for k in ("u", "v", "T", "p")} for c in range(len(gs))]
+        nstep = b.stats(0)["steps"]
+    assert nstep == 7
+    with Batch(gs, ps) as b:
+        b.step(3)
+        b.set_mg(pre, post, coarse)
+        b.step(4)
+        ref = [{k: b.plane(c, k) for k in ("u", "v", "T", "p")} for c in range(len(gs))]
+    for fr, fg in zip(ref, got):
+        for k in fr:
+            np.testing.assert_array_equal(fg[k], fr[k], err_msg=k)
