@@ -222,6 +222,26 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ------------------------------------------------------------------ ranks
+def rank_draws(ncases: int, rank: int):
+    """Rank r runs its own seeded sweep (seed 1234 + r): whole cases per rank, no data
+    exchange between ranks (weak scaling)."""
+    from cfd_solver_b200.workloads import SWEEP_SEED, sweep_draws
+    return sweep_draws(ncases, seed=SWEEP_SEED + rank)
+
+
+def job_totals(dist, device, cells: float, ms: float, world: int):
+    """Whole-job figures: cells summed over ranks, time the max over ranks."""
+    if world == 1:
+        return float(cells), float(ms)
+    import torch
+    c = torch.tensor([float(cells)], dtype=torch.float64, device=device)
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(c.item()), float(t.item())
+
+
 # ------------------------------------------------------------------ plain single-case path
 def plain_step_ms(grid, prm, warm: int, timed: int) -> float:
     """Device time per step of one case alone on the plain FP64 path (a batch of one), after
@@ -412,7 +432,7 @@ def main():
         if world > 1:
             dist.barrier(device_ids=[local])
 
-    draws = sweep_draws(args.ncases, seed=SWEEP_SEED + rank)
+    draws = rank_draws(args.ncases, rank)
     grids, params = [], []
     for d in draws:
         g, prm = make_case(d, args.form)
@@ -455,11 +475,8 @@ def main():
     work1 = b.work()
     kt = b.kernel_times()
     b.profile(False)
-    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = cells * args.steps * world / (ms_max / 1e3)
+    job_cells, ms_max = job_totals(dist, "cuda", cells, ms, world)
+    value = job_cells * args.steps / (ms_max / 1e3)
 
     # roofline of the dominant kernel (the u/v/T sweeps): algorithmic bytes per launch from
     # the traffic counters (field-cells of all sweeps, of sweep 0, of sweep 1; cells).
@@ -517,10 +534,8 @@ def main():
         b.stats(0)
     b.sync()
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = cells * args.e2e_steps * world / float(te.item())
+    _, e2e_max = job_totals(dist, "cuda", cells, e2e_s, world)
+    e2e_value = job_cells * args.e2e_steps / e2e_max
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and args.form == "twin":
@@ -539,7 +554,7 @@ def main():
                 "dtype": "f64" if args.precision == "fp64" else "f64+f32",
                 "data": "synthetic (seeded sweep draws; grids generated in INP.DAT format)",
                 "config": workload_config(args),
-                "cells_per_step": cells * world,
+                "cells_per_step": job_cells,
                 "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "cell-updates/s",
                         "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 200},
