@@ -47,7 +47,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["step", "converged", "serve"], default="step",
+    ap.add_argument("--config", choices=["c1", "c2", "c3"], default="c3",
+                    help="single-case configuration of the precision workload")
+    ap.add_argument("--workload", choices=["step", "converged", "serve", "precision"], default="step",
                     help="step: outer-step throughput of the sweep (default); converged: every case of "
                          "the sweep to its steady tolerance or the step cap, batched vs the plain "
                          "single-case FP64 path; serve: Poisson request stream through cfd_serve")
@@ -395,6 +397,47 @@ def run_serve(args):
     print(json.dumps(line))
 
 
+def run_precision(args):
+    """One single-case configuration (cavity form) in the plain FP64 path and in the
+    precision form for the same number of steps: time per step of each and the relative
+    L2 difference of u, v, p (mean removed), T and Nu of the precision form."""
+    import numpy as np
+    import torch
+    from cfd_solver_b200.grid import cavity
+    from cfd_solver_b200.solver import Batch, case_params
+    from cfd_solver_b200.workloads import CONFIGS, cavity_dt
+    c = CONFIGS[args.config]
+    g = cavity(c["N"], c["N"], skew=c["skew"])
+    dt = cavity_dt(c["N"], c["Ri"], c["Re"], c["Pr"])
+    out = {}
+    for prec in (0, 1):
+        with Batch([g], [case_params(g, Re=c["Re"], Ri=c["Ri"], Pr=c["Pr"], dt=dt, precision=prec)]) as b:
+            b.step(args.warmup)
+            b.sync()
+            stream = torch.cuda.ExternalStream(b.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.step(args.steps)
+            e1.record(stream)
+            e1.synchronize()
+            st = b.stats(0)
+            f = {k: b.plane(0, k) for k in ("u", "v", "p", "T")}
+            f["p"] = f["p"] - f["p"][1:-1, 1:-1].mean()
+            out[prec] = (e0.elapsed_time(e1) / args.steps, f, st)
+    rel = {k: float(np.linalg.norm(out[1][1][k] - out[0][1][k]) / max(np.linalg.norm(out[0][1][k]), 1e-300))
+           for k in ("u", "v", "p", "T")}
+    nu0, nu1 = out[0][2]["nu"], out[1][2]["nu"]
+    line = {"metric": "precision form vs FP64", "config": {"workload": f"{args.config}: {c['N']}x{c['N']} cavity, "
+            f"skew {c['skew']}, Re {c['Re']}, Ri {c['Ri']}, Pr {c['Pr']}", "dt": dt,
+            "steps": args.steps + args.warmup},
+            "ms_per_step_fp64": out[0][0], "ms_per_step_mixed": out[1][0],
+            "speedup": out[0][0] / out[1][0], "rel_l2": rel, "nu_fp64": nu0, "nu_mixed": nu1,
+            "nu_rel": abs(nu1 - nu0) / max(abs(nu0), 1e-300),
+            "steady_res_rel_fp64": out[0][2]["steady_res_rel"], "steady_res_rel_mixed": out[1][2]["steady_res_rel"],
+            "status": [out[0][2]["status"], out[1][2]["status"]]}
+    print(json.dumps(line))
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     args = parse()
@@ -407,6 +450,9 @@ def main():
         if "--precision" not in sys.argv:
             args.precision = "mixed"
         run_converged(args)
+        return
+    if args.workload == "precision":
+        run_precision(args)
         return
     if args.workload == "serve":
         if "--precision" not in sys.argv:

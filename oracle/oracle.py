@@ -83,6 +83,10 @@ class OracleCase:
         self.grid = grid
         if "profile" not in params:
             params["profile"] = CAVITY if grid.kind == "cavity" else OGRID
+        if params["profile"] == CAVITY:
+            # the C++ T-solve slot bug destabilises T on skewed grids; the cavity takes the
+            # Fortran-intent coefficient by default, as the library's case_params does
+            params.setdefault("fix_T_annw", 1)
         self.params = make_params(**params)
         self._planes = np.ascontiguousarray(grid.planes())
         self._normals = np.ascontiguousarray(grid.normals())
