@@ -173,6 +173,8 @@ struct cfd_batch {
     unsigned long long* work = nullptr;  // k_jac traffic counters
     long long launches = 0;              // kernels launched since creation
     int* h_flags = nullptr;
+    double* stage = nullptr;        // state snapshot staging (allocated on first use)
+    long long* stage_off = nullptr; // per-case offsets into it (doubles)
     Tile* dtiles = nullptr;
     int* dcc = nullptr;
     char* dtmaps = nullptr;  // two CUtensorMaps per case
@@ -394,6 +396,9 @@ void case_params_to_dev(CaseDev& d, const cfd_grid& g, const cfd_params& p) {
     d.ca = cos(p.alpha_deg * d.Pi / 180.0);
     d.ar = g.ar; d.omega_p = p.omega_p; d.lid_u = p.lid_u;
     d.tol_mom = p.tol_mom; d.atol_mom = p.atol_mom; d.tol_p = p.tol_p; d.atol_p = p.atol_p;
+    d.pc1 = 1.0 / (2.0 * g.dxi0 * g.dxi0);
+    d.pc2 = 1.0 / (8.0 * g.dxi0 * g.dxi1);
+    d.pc3 = 1.0 / (2.0 * g.dxi1 * g.dxi1);
     cheb_bounds(g, p, d);
 }
 
@@ -1027,6 +1032,7 @@ int cfd_batch_destroy(cfd_batch* b) {
     for (auto& l : b->pending) { cudaEventDestroy(l.e0); cudaEventDestroy(l.e1); }
     for (auto e : b->pool) cudaEventDestroy(e);
     cudaFree(b->f64); cudaFree(b->f32); cudaFree(b->dc); cudaFree(b->scal); cudaFree(b->iscal);
+    cudaFree(b->stage); cudaFree(b->stage_off);
     cudaFree(b->partial); cudaFree(b->counter); cudaFree(b->flags); cudaFree(b->work); cudaFree(b->dtiles); cudaFree(b->dcc); cudaFree(b->dtmaps);
     if (b->h_flags) cudaFreeHost(b->h_flags);
     if (b->st) cudaStreamDestroy(b->st);
@@ -1194,10 +1200,6 @@ int cfd_batch_work(cfd_batch* b, unsigned long long* out4) {
 
 // the resident state of every case: u, v, p, T, up, vp (padded device planes, in case order)
 static const int kStatePlanes = 6;
-static int state_plane(const cfd_batch* b, int m) {
-    const int ids[kStatePlanes] = {P_U, P_V, P_P, P_T0 + b->cur, P_UP0 + b->cur, P_VP0 + b->cur};
-    return ids[m];
-}
 
 size_t cfd_batch_state_bytes(cfd_batch* b) {
     if (!b) return 0;
@@ -1206,23 +1208,32 @@ size_t cfd_batch_state_bytes(cfd_batch* b) {
     return s + 16 * sizeof(double) * b->n;
 }
 
+// The state crosses PCIe as one copy per direction: a kernel packs (or unpacks) every
+// case's state planes into a device staging buffer laid out as the host buffer.
 static int state_copy(cfd_batch* b, void* host, size_t bytes, bool to_host) {
     if (!b || !host) return fail(CFD_E_ARG, "bad arguments");
-    if (bytes < cfd_batch_state_bytes(b)) return fail(CFD_E_ARG, "state buffer too small");
-    char* h = (char*)host;
-    for (int c = 0; c < b->n; c++) {
-        const CaseDev& d = b->hc[c];
-        for (int m = 0; m < kStatePlanes; m++) {
-            double* dev = b->f64 + d.base + H - 16 + (long long)state_plane(b, m) * d.ps;
-            const size_t nb = sizeof(double) * d.ps;
-            if (to_host) CK(cudaMemcpyAsync(h, dev, nb, cudaMemcpyDeviceToHost, b->st));
-            else CK(cudaMemcpyAsync(dev, h, nb, cudaMemcpyHostToDevice, b->st));
-            h += nb;
+    const size_t need = cfd_batch_state_bytes(b);
+    if (bytes < need) return fail(CFD_E_ARG, "state buffer too small");
+    if (!b->stage) {
+        std::vector<long long> off(b->n);
+        long long o = 0;
+        for (int c = 0; c < b->n; c++) {
+            off[c] = o;
+            o += (long long)kStatePlanes * b->hc[c].ps + 16;
         }
-        // per-case scalars that carry across steps: the reference's int time
-        if (to_host) CK(cudaMemcpyAsync(h, b->iscal + (long long)c * NISCAL + I_TIME, sizeof(int), cudaMemcpyDeviceToHost, b->st));
-        else CK(cudaMemcpyAsync(b->iscal + (long long)c * NISCAL + I_TIME, h, sizeof(int), cudaMemcpyHostToDevice, b->st));
-        h += 16 * sizeof(double);
+        CK(cudaMalloc((void**)&b->stage, need));
+        CK(cudaMalloc((void**)&b->stage_off, sizeof(long long) * b->n));
+        CK(cudaMemcpy(b->stage_off, off.data(), sizeof(long long) * b->n, cudaMemcpyHostToDevice));
+    }
+    b->bd.cur = b->cur;
+    if (to_host) {
+        k_state_pack<<<b->n * 7, 256, 0, b->st>>>(b->bd, b->stage, b->stage_off, 1);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(host, b->stage, need, cudaMemcpyDeviceToHost, b->st));
+    } else {
+        CK(cudaMemcpyAsync(b->stage, host, need, cudaMemcpyHostToDevice, b->st));
+        k_state_pack<<<b->n * 7, 256, 0, b->st>>>(b->bd, b->stage, b->stage_off, 0);
+        CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(b->st));
     return CFD_OK;

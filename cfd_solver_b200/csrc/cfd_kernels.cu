@@ -41,73 +41,63 @@ __device__ __forceinline__ bool near_wall(const CaseDev& c, int i, int j) {
 }
 
 // ---------------------------------------------------------------------------
-// pressure stencil assembly (PSolver.cpp:944-1040), also the set-up of MG level 0
+// The 9-point pressure stencil at one cell (PSolver.cpp:944-1040) from the four metric
+// planes X = xi_x, Y = xi_y, E = eta_x, G = eta_y at the cell and its four neighbours,
+// in the order ap, ae, aw, an, as, ane, anw, ase, asw. c1 = 1 / (2 dxi0^2), c2 = 1 / (8 dxi0
+// dxi1), c3 = 1 / (2 dxi1^2) (the reference divides by these; multiplying by reciprocals
+// moves each coefficient by at most a unit in the last place). The stencil is stored
+// once (k_assemble_p): rebuilding it inside the SpMV was measured slower (about 100 FP64
+// operations per cell against 40 bytes saved).
+template <typename T>
+struct P9In {
+    T x, xe, xw, xn, xs, y, ye, yw, yn, ys, e, ee, ew, en, es, g, ge, gw, gn, gs;
+};
+
+template <typename T>
+__device__ __forceinline__ void p9_coefs(const P9In<T>& m, T c1, T c2, T c3, T (&a)[9]) {
+    const T X = m.x, Y = m.y, E = m.e, G = m.g;
+    a[1] = (X * c1) * (X + m.xe) + (E * c2) * (m.xn - m.xs) + (Y * c1) * (Y + m.ye) + (G * c2) * (m.yn - m.ys);
+    a[2] = (X * c1) * (X + m.xw) + (E * c2) * (m.xs - m.xn) + (Y * c1) * (Y + m.yw) + (G * c2) * (m.ys - m.yn);
+    a[3] = (X * c2) * (m.ee - m.ew) + (E * c3) * (E + m.en) + (Y * c2) * (m.ge - m.gw) + (G * c3) * (G + m.gn);
+    a[4] = (X * c2) * (m.ew - m.ee) + (E * c3) * (E + m.es) + (Y * c2) * (m.gw - m.ge) + (G * c3) * (G + m.gs);
+    a[5] = (X * c2) * (E + m.ee) + (E * c2) * (X + m.xn) + (Y * c2) * (G + m.ge) + (G * c2) * (Y + m.yn);
+    a[8] = (X * c2) * (E + m.ew) + (E * c2) * (X + m.xs) + (Y * c2) * (G + m.gw) + (G * c2) * (Y + m.ys);
+    a[6] = -((X * c2) * (E + m.ew)) - (E * c2) * (X + m.xn) - (Y * c2) * (G + m.gw) - (G * c2) * (Y + m.yn);
+    a[7] = -((X * c2) * (E + m.ee)) - (E * c2) * (X + m.xs) - (Y * c2) * (G + m.ge) - (G * c2) * (Y + m.ys);
+    a[0] = (-X * (T(2) * X + m.xw + m.xe)) * c1 + (-E * (T(2) * E + m.es + m.en)) * c3 +
+           (-Y * (T(2) * Y + m.yw + m.ye)) * c1 + (-G * (T(2) * G + m.gs + m.gn)) * c3;
+}
+
+// the metrics around flat index k of planes X, Y, E, G with row pitch ld
+template <typename T, typename S>
+__device__ __forceinline__ P9In<T> p9_load(const S* X, const S* Y, const S* E, const S* G, long long k, int ld) {
+    P9In<T> m;
+    m.x = X[k]; m.xe = X[k + 1]; m.xw = X[k - 1]; m.xn = X[k + ld]; m.xs = X[k - ld];
+    m.y = Y[k]; m.ye = Y[k + 1]; m.yw = Y[k - 1]; m.yn = Y[k + ld]; m.ys = Y[k - ld];
+    m.e = E[k]; m.ee = E[k + 1]; m.ew = E[k - 1]; m.en = E[k + ld]; m.es = E[k - ld];
+    m.g = G[k]; m.ge = G[k + 1]; m.gw = G[k - 1]; m.gn = G[k + ld]; m.gs = G[k - ld];
+    return m;
+}
+
+// pressure stencil assembly, also the set-up of multigrid level 0 (stencil and the FP32
+// metric copies its matrix-free sweeps read)
 __global__ void __launch_bounds__(NT) k_assemble_p(BatchDev b, int toff) {
     const Tile t = b.ftiles[toff + blockIdx.x];
     const CaseDev& c = b.cases[t.c];
     const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
     if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
     const int ld = c.ld, W = c.W, per = c.periodic;
-    const double d0 = c.d0, d1 = c.d1;
-    const double* X = plane(b, c, P_XIX);
-    const double* Y = plane(b, c, P_XIY);
-    const double* E = plane(b, c, P_ETX);
-    const double* G = plane(b, c, P_ETY);
-    const long long k = (long long)j * ld + i, kE = k + 1, kW = k - 1, kN = k + ld, kS = k - ld;
-    double aae = (X[k] / (2.0 * d0 * d0)) * (X[k] + X[kE]);
-    double bbe = (E[k] / (8.0 * d0 * d1)) * (X[kN] - X[kS]);
-    double cce = (Y[k] / (2.0 * d0 * d0)) * (Y[k] + Y[kE]);
-    double dde = (G[k] / (8.0 * d0 * d1)) * (Y[kN] - Y[kS]);
-    const double ae = aae + bbe + cce + dde;
-    double aaw = (X[k] / (2.0 * d0 * d0)) * (X[k] + X[kW]);
-    double bbw = (E[k] / (8.0 * d0 * d1)) * (X[kS] - X[kN]);
-    double ccw = (Y[k] / (2.0 * d0 * d0)) * (Y[k] + Y[kW]);
-    double ddw = (G[k] / (8.0 * d0 * d1)) * (Y[kS] - Y[kN]);
-    const double aw = aaw + bbw + ccw + ddw;
-    double aan = (X[k] / (8.0 * d0 * d1)) * (E[kE] - E[kW]);
-    double bbn = (E[k] / (2.0 * d1 * d1)) * (E[k] + E[kN]);
-    double ccn = (Y[k] / (8.0 * d0 * d1)) * (G[kE] - G[kW]);
-    double ddn = (G[k] / (2.0 * d1 * d1)) * (G[k] + G[kN]);
-    const double an = aan + bbn + ccn + ddn;
-    double aas = (X[k] / (8.0 * d0 * d1)) * (E[kW] - E[kE]);
-    double bbs = (E[k] / (2.0 * d1 * d1)) * (E[k] + E[kS]);
-    double ccs = (Y[k] / (8.0 * d0 * d1)) * (G[kW] - G[kE]);
-    double dds = (G[k] / (2.0 * d1 * d1)) * (G[k] + G[kS]);
-    const double as = aas + bbs + ccs + dds;
-    double aane = (X[k] / (8.0 * d0 * d1)) * (E[k] + E[kE]);
-    double bbne = (E[k] / (8.0 * d0 * d1)) * (X[k] + X[kN]);
-    double ccne = (Y[k] / (8.0 * d0 * d1)) * (G[k] + G[kE]);
-    double ddne = (G[k] / (8.0 * d0 * d1)) * (Y[k] + Y[kN]);
-    const double ane = aane + bbne + ccne + ddne;
-    double aasw = (X[k] / (8.0 * d0 * d1)) * (E[k] + E[kW]);
-    double bbsw = (E[k] / (8.0 * d0 * d1)) * (X[k] + X[kS]);
-    double ccsw = (Y[k] / (8.0 * d0 * d1)) * (G[k] + G[kW]);
-    double ddsw = (G[k] / (8.0 * d0 * d1)) * (Y[k] + Y[kS]);
-    const double asw = aasw + bbsw + ccsw + ddsw;
-    double aanw = -(X[k] / (8.0 * d0 * d1)) * (E[k] + E[kW]);
-    double bbnw = -(E[k] / (8.0 * d0 * d1)) * (X[k] + X[kN]);
-    double ccnw = -(Y[k] / (8.0 * d0 * d1)) * (G[k] + G[kW]);
-    double ddnw = -(G[k] / (8.0 * d0 * d1)) * (Y[k] + Y[kN]);
-    const double anw = aanw + bbnw + ccnw + ddnw;
-    double aase = -(X[k] / (8.0 * d0 * d1)) * (E[k] + E[kE]);
-    double bbse = -(E[k] / (8.0 * d0 * d1)) * (X[k] + X[kS]);
-    double ccse = -(Y[k] / (8.0 * d0 * d1)) * (G[k] + G[kE]);
-    double ddse = -(G[k] / (8.0 * d0 * d1)) * (Y[k] + Y[kS]);
-    const double ase = aase + bbse + ccse + ddse;
-    const double pxi = 1.0 / (2. * d0 * d0);
-    const double pet = 1.0 / (2. * d1 * d1);
-    double aap = -X[k] * (2. * X[k] + X[kW] + X[kE]);
-    double bbp = -E[k] * (2. * E[k] + E[kS] + E[kN]);
-    double ccp = -Y[k] * (2. * Y[k] + Y[kW] + Y[kE]);
-    double ddp = -G[k] * (2. * G[k] + G[kS] + G[kN]);
-    const double ap = aap * pxi + bbp * pet + ccp * pxi + ddp * pet;
-    const double vals[9] = {ap, ae, aw, an, as, ane, anw, ase, asw};
+    const long long k = (long long)j * ld + i;
+    const P9In<double> m = p9_load<double>(plane(b, c, P_XIX), plane(b, c, P_XIY), plane(b, c, P_ETX),
+                                           plane(b, c, P_ETY), k, ld);
+    double vals[9];
+    p9_coefs<double>(m, c.pc1, c.pc2, c.pc3, vals);
     const LevelDev& L0 = c.lev[0];
     const int ld0 = L0.ld;
 #pragma unroll
-    for (int m = 0; m < 9; m++) {
-        store_mirrored(plane(b, c, P_AP + m), ld, i, j, W, per, vals[m]);
-        store_mirrored(mplane(b, L0, M_AP + m), ld0, i, j, W, per, (float)vals[m]);
+    for (int q = 0; q < 9; q++) {
+        store_mirrored(plane(b, c, P_AP + q), ld, i, j, W, per, vals[q]);
+        store_mirrored(mplane(b, L0, M_AP + q), ld0, i, j, W, per, (float)vals[q]);
     }
 }
 
@@ -1364,4 +1354,29 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, const int* flag, int* 
 }
 
 #undef AT
+// ---------------------------------------------------------------------------
+// Resident state <-> one contiguous staging buffer (so a state snapshot crosses PCIe as one
+// copy per direction). Per case: the six state planes u, v, p, T, up, vp (whole padded
+// planes, ps doubles each, in that order), then 16 doubles whose first 4 bytes hold the
+// reference's int time. blockIdx.x = case * 7 + m (m = 6: the scalar slot).
+__global__ void __launch_bounds__(256) k_state_pack(BatchDev b, double* stage, const long long* off, int to_stage) {
+    const int c = blockIdx.x / 7, m = blockIdx.x % 7;
+    const CaseDev& d = b.cases[c];
+    double* dst = stage + off[c] + (long long)m * d.ps;
+    if (m == 6) {
+        int* it = b.iscal + (long long)c * NISCAL + I_TIME;
+        if (threadIdx.x == 0) {
+            if (to_stage) *reinterpret_cast<int*>(dst) = *it;
+            else *it = *reinterpret_cast<const int*>(dst);
+        }
+        return;
+    }
+    const int ids[6] = {P_U, P_V, P_P, P_T0 + b.cur, P_UP0 + b.cur, P_VP0 + b.cur};
+    double* src = b.f64 + d.base + H - 16 + (long long)ids[m] * d.ps;  // 128-byte aligned plane start
+    const long long n2 = d.ps / 2;                                       // ps is a multiple of 16
+    double2* a = reinterpret_cast<double2*>(to_stage ? dst : src);
+    const double2* s2 = reinterpret_cast<const double2*>(to_stage ? src : dst);
+    for (long long e = threadIdx.x; e < n2; e += blockDim.x) a[e] = s2[e];
+}
+
 }  // namespace cfd

@@ -22,5 +22,6 @@ __global__ void k_correct(BatchDev b);
 __global__ void k_bc(BatchDev b);
 __global__ void k_diag(BatchDev b);
 __global__ void k_si(BatchDev b);
+__global__ void k_state_pack(BatchDev b, double* stage, const long long* off, int to_stage);
 __global__ void k_loop_cond(cudaGraphConditionalHandle h, const int* flag, int* counter, int maxc, int* total);
 }  // namespace cfd
