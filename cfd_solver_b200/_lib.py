@@ -147,9 +147,9 @@ def lib():
     L.cfd_batch_fetch_stats.argtypes = [vp, ctypes.POINTER(CfdStepStats), ctypes.c_int]
     L.cfd_batch_admit.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CfdGrid), ctypes.POINTER(CfdParams)]
     L.cfd_batch_set_active.argtypes = [vp, ctypes.c_int, ctypes.c_int]
-    L.cfd_batch_set_mg.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.cfd_batch_set_mg.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     ip = ctypes.POINTER(ctypes.c_int)
-    L.cfd_batch_get_mg.argtypes = [vp, ip, ip, ip]
+    L.cfd_batch_get_mg.argtypes = [vp, ip, ip, ip, ip]
     L.cfd_batch_autotune.argtypes = [vp, ctypes.c_int, ip, ctypes.POINTER(ctypes.c_double)]
     L.cfd_serve.argtypes = [ctypes.POINTER(CfdServeConfig), ctypes.POINTER(CfdRequest), ctypes.c_int,
                             ctypes.POINTER(CfdResult), ctypes.POINTER(CfdServeStats)]

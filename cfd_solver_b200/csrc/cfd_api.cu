@@ -187,6 +187,7 @@ struct cfd_batch {
     size_t sw_smem = 0;
     int coarse_sweeps = 12;
     int mg_pre = 1, mg_post = 2;  // multigrid sweeps before / after the coarse correction
+    int mg_fused = 1;             // 1: a smoothing phase's sweeps in one launch
     int max_W = 0;
     int cur = 0;
     long long steps_done = 0;
@@ -412,25 +413,33 @@ void make_tiles(int ilo, int ihi, int n1, int cid, std::vector<Tile>& out, int t
 // one time step of every case in the batch
 // planes of the pre-smoothed x and of the V-cycle result of a non-coarsest level: sweeps
 // alternate between x and r, starting in x
-int mg_pre_plane(int nu_pre) { return (nu_pre & 1) ? M_X : M_R; }
-int mg_res_plane(int nu_pre, int nu_post) {
-    const int p = mg_pre_plane(nu_pre);
-    return (nu_post & 1) ? (p == M_X ? M_R : M_X) : p;
+int mg_pre_plane(int nu_pre, int fused) { return (fused || (nu_pre & 1)) ? M_X : M_R; }
+int mg_res_plane(int nu_pre, int nu_post, int fused) {
+    const int p = mg_pre_plane(nu_pre, fused);
+    const int q = p == M_X ? M_R : M_X;
+    return (fused || (nu_post & 1)) ? q : p;
 }
 
+// One V-cycle. Smoothing phases of several sweeps run either as one launch per sweep
+// (each sweep sees the neighbouring tiles' latest values) or, `mg_fused`, as one launch
+// doing all of the phase's sweeps in shared memory.
 int run_vcycle(cfd_batch* b) {
     BatchDev& bd = b->bd;
-    const int pre = mg_pre_plane(b->mg_pre);
+    const int fused = b->mg_fused;
+    const int pre = mg_pre_plane(b->mg_pre, fused);
+    const int npre = fused ? 1 : b->mg_pre, inpre = fused ? b->mg_pre : 1;
+    const int npost = fused ? 1 : b->mg_post, inpost = fused ? b->mg_post : 1;
     for (int l = 0; l < b->nlev_max; l++) {
         if (bd.nccases[l] > 0) {
             Prof pr(b, K_MG_COARSE);
             k_mg_coarse<<<bd.nccases[l], 1024, 0, b->st>>>(bd, l, b->coarse_sweeps);
         }
         if (bd.nmtiles[l] > 0) {
-            for (int s = 0; s < b->mg_pre; s++) {  // pre-smoothing from zero
+            for (int s = 0; s < npre; s++) {  // pre-smoothing from zero
                 Prof pr(b, K_MG_SMOOTH);
                 const int dst = (s & 1) ? M_R : M_X;
-                k_mg_gs<<<bd.nmtiles[l], NT, kMgGsSmem, b->st>>>(bd, l, s == 0 ? 0 : 1, dst == M_X ? M_R : M_X, dst);
+                k_mg_gs<<<bd.nmtiles[l], NT, kMgGsSmem, b->st>>>(bd, l, s == 0 ? 0 : 1, dst == M_X ? M_R : M_X, dst,
+                                                                  inpre);
             }
             Prof pr(b, K_MG_RR);
             k_mg_rr<<<bd.natiles[l + 1], NT, 0, b->st>>>(bd, l, pre);
@@ -439,10 +448,10 @@ int run_vcycle(cfd_batch* b) {
     for (int l = b->nlev_max - 2; l >= 0; l--) {
         if (bd.nmtiles[l] == 0) continue;
         int src = pre;
-        for (int s = 0; s < b->mg_post; s++) {
+        for (int s = 0; s < npost; s++) {
             Prof pr(b, K_MG_POST);
             const int dst = src == M_X ? M_R : M_X;
-            k_mg_gs<<<bd.nmtiles[l], NT, kMgGsSmem, b->st>>>(bd, l, s == 0 ? 2 : 3, src, dst);
+            k_mg_gs<<<bd.nmtiles[l], NT, kMgGsSmem, b->st>>>(bd, l, s == 0 ? 2 : 3, src, dst, inpost);
             src = dst;
         }
     }
@@ -957,7 +966,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
     bd.jtiles = b->dtiles + pos_jt; bd.njtiles = (int)jtiles.size();
     bd.error = b->flags + 4;
-    bd.mg_res = mg_res_plane(b->mg_pre, b->mg_post);
+    bd.mg_res = mg_res_plane(b->mg_pre, b->mg_post, b->mg_fused);
     bd.sweep_no = b->flags + 7;
     for (int l = 0; l < MAXLEV; l++) {
         bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
@@ -1040,24 +1049,27 @@ int cfd_batch_destroy(cfd_batch* b) {
     return CFD_OK;
 }
 
-int cfd_batch_set_mg(cfd_batch* b, int nu_pre, int nu_post, int coarse_sweeps) {
+int cfd_batch_set_mg(cfd_batch* b, int nu_pre, int nu_post, int coarse_sweeps, int fused) {
     if (!b) return fail(CFD_E_ARG, "null batch");
-    if (nu_pre < 1 || nu_pre > 8 || nu_post < 1 || nu_post > 8 || coarse_sweeps < 1 || coarse_sweeps > 256)
-        return fail(CFD_E_ARG, "multigrid schedule out of range (sweeps 1..8, coarse sweeps 1..256)");
+    if (nu_pre < 1 || nu_pre > 8 || nu_post < 1 || nu_post > 8 || coarse_sweeps < 1 || coarse_sweeps > 256 ||
+        (fused != 0 && fused != 1))
+        return fail(CFD_E_ARG, "multigrid schedule out of range (sweeps 1..8, coarse sweeps 1..256, fused 0/1)");
     CK(cudaStreamSynchronize(b->st));
     b->mg_pre = nu_pre;
     b->mg_post = nu_post;
     b->coarse_sweeps = coarse_sweeps;
-    b->bd.mg_res = mg_res_plane(nu_pre, nu_post);
+    b->mg_fused = fused;
+    b->bd.mg_res = mg_res_plane(nu_pre, nu_post, fused);
     drop_graphs(b);  // the step graphs hold the old schedule
     return CFD_OK;
 }
 
-int cfd_batch_get_mg(cfd_batch* b, int* nu_pre, int* nu_post, int* coarse_sweeps) {
+int cfd_batch_get_mg(cfd_batch* b, int* nu_pre, int* nu_post, int* coarse_sweeps, int* fused) {
     if (!b) return fail(CFD_E_ARG, "null batch");
     if (nu_pre) *nu_pre = b->mg_pre;
     if (nu_post) *nu_post = b->mg_post;
     if (coarse_sweeps) *coarse_sweeps = b->coarse_sweeps;
+    if (fused) *fused = b->mg_fused;
     return CFD_OK;
 }
 
@@ -1066,7 +1078,8 @@ int cfd_batch_get_mg(cfd_batch* b, int* nu_pre, int* nu_post, int* coarse_sweeps
 // fastest and reports its time per step. The batch's state is unchanged on return.
 int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule, double* out_ms_per_step) {
     if (!b || steps < 1) return fail(CFD_E_ARG, "bad arguments");
-    static const int cand[][3] = {{1, 1, 12}, {1, 2, 12}, {2, 1, 12}, {2, 2, 12}, {1, 1, 24}, {1, 1, 6}, {2, 2, 24}};
+    static const int cand[][4] = {{1, 1, 12, 0}, {1, 2, 12, 0}, {2, 1, 12, 0}, {2, 2, 12, 0}, {1, 1, 24, 0},
+                                  {1, 2, 24, 0}, {1, 2, 12, 1}, {1, 3, 12, 1}, {2, 2, 12, 1}, {2, 3, 12, 1}};
     const int ncand = (int)(sizeof(cand) / sizeof(cand[0]));
     const size_t n64 = (size_t)b->n64 * sizeof(double), nsc = sizeof(double) * NSCAL * b->n,
                  nis = sizeof(int) * NISCAL * b->n;
@@ -1091,14 +1104,14 @@ int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule, double* out_m
         b->steps_done = steps0;
         return CFD_OK;
     };
-    const int mp = b->mg_pre, mq = b->mg_post, mc = b->coarse_sweeps;
+    const int mp = b->mg_pre, mq = b->mg_post, mc = b->coarse_sweeps, mf = b->mg_fused;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int rc = copy(true), best = -1;
     float best_ms = 0.f;
     for (int k = 0; k < ncand && !rc; k++) {
-        rc = cfd_batch_set_mg(b, cand[k][0], cand[k][1], cand[k][2]);
+        rc = cfd_batch_set_mg(b, cand[k][0], cand[k][1], cand[k][2], cand[k][3]);
         if (!rc) rc = copy(false);
         if (!rc) rc = cfd_batch_step(b, 1);  // builds the step graphs of this schedule
         if (!rc) rc = copy(false);
@@ -1117,7 +1130,8 @@ int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule, double* out_m
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    int rc2 = rc ? cfd_batch_set_mg(b, mp, mq, mc) : cfd_batch_set_mg(b, cand[best][0], cand[best][1], cand[best][2]);
+    int rc2 = rc ? cfd_batch_set_mg(b, mp, mq, mc, mf)
+                 : cfd_batch_set_mg(b, cand[best][0], cand[best][1], cand[best][2], cand[best][3]);
     int rc3 = copy(false);
     if (!rc3) rc3 = cudaStreamSynchronize(b->st) == cudaSuccess ? CFD_OK : fail(CFD_E_CUDA, "autotune sync");
     cudaFree(snap);
@@ -1125,11 +1139,8 @@ int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule, double* out_m
     if (rc) return rc;
     if (rc2) return rc2;
     if (rc3) return rc3;
-    if (out_schedule) {
-        out_schedule[0] = cand[best][0];
-        out_schedule[1] = cand[best][1];
-        out_schedule[2] = cand[best][2];
-    }
+    if (out_schedule)
+        for (int q = 0; q < 4; q++) out_schedule[q] = cand[best][q];
     if (out_ms_per_step) *out_ms_per_step = best_ms / steps;
     return CFD_OK;
 }

@@ -731,13 +731,16 @@ __device__ __forceinline__ float mg_prolong_at(const float* XC, int cl, int i, i
 //   mode 2: from src plus the prolonged result of level l + 1, colours reversed (first
 //           post-sweep)
 //   mode 3: from src, colours reversed (further post-sweeps)
+// `inner` sweeps run back to back in shared memory, the halo kept from before the first
+// (one launch and one read of the stencil for several sweeps, at the price of weaker
+// coupling between tiles).
 constexpr int MGS_OV = 0;                          // overlap relaxed redundantly around the tile
 constexpr int MGS_OVM = MGS_OV;
 constexpr int MGS_RW = TX + 2 * MGS_OVM, MGS_RH = TYJ + 2 * MGS_OVM;
 constexpr int MGS_XW = MGS_RW + 2, MGS_XH = MGS_RH + 2;
 constexpr size_t MGS_SMEM = (size_t)(MGS_XH * MGS_XW + 10 * MGS_RW * MGS_RH) * sizeof(float) + MGS_RW * MGS_RH;
 const size_t kMgGsSmem = MGS_SMEM;
-__global__ void __launch_bounds__(NT) k_mg_gs(BatchDev b, int l, int mode, int src, int dst) {
+__global__ void __launch_bounds__(NT) k_mg_gs(BatchDev b, int l, int mode, int src, int dst, int inner) {
     extern __shared__ __align__(16) unsigned char mgraw[];
     float* xs = reinterpret_cast<float*>(mgraw);
     float(*cf)[MGS_RW * MGS_RH] = reinterpret_cast<float(*)[MGS_RW * MGS_RH]>(xs + MGS_XH * MGS_XW);
@@ -784,8 +787,9 @@ __global__ void __launch_bounds__(NT) k_mg_gs(BatchDev b, int l, int mode, int s
         colr[e] = cc;
     }
     __syncthreads();
-    for (int n = 0; n < ncol; n++) {
-        const int cc = reverse ? ncol - 1 - n : n;
+    for (int n = 0; n < ncol * inner; n++) {
+        const int cn = n % ncol;
+        const int cc = reverse ? ncol - 1 - cn : cn;
         for (int e = tid; e < rh * rw; e += NT) {
             if (colr[e] != cc) continue;
             const int o = (e / rw + 1) * xw + (e % rw + 1);

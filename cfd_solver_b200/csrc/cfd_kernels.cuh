@@ -13,7 +13,7 @@ __global__ void k_bicg_p(BatchDev b);
 __global__ void k_spmv(BatchDev b, int mode);
 __global__ void k_bicg_s(BatchDev b);
 __global__ void k_bicg_x(BatchDev b, int maxit);
-__global__ void k_mg_gs(BatchDev b, int l, int mode, int src, int dst);
+__global__ void k_mg_gs(BatchDev b, int l, int mode, int src, int dst, int inner);
 extern const size_t kMgGsSmem;  // dynamic shared memory of k_mg_gs
 __global__ void k_mg_rr(BatchDev b, int l, int src);
 __global__ void k_mg_coarse(BatchDev b, int l, int sweeps);

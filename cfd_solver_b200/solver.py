@@ -85,18 +85,18 @@ class Batch:
     def set_active(self, slot: int, active: bool):
         _lib.check(_lib.lib().cfd_batch_set_active(self.h, slot, int(active)), "cfd_batch_set_active")
 
-    def set_mg(self, nu_pre: int, nu_post: int, coarse_sweeps: int):
-        _lib.check(_lib.lib().cfd_batch_set_mg(self.h, nu_pre, nu_post, coarse_sweeps), "cfd_batch_set_mg")
+    def set_mg(self, nu_pre: int, nu_post: int, coarse_sweeps: int, fused: int = 0):
+        _lib.check(_lib.lib().cfd_batch_set_mg(self.h, nu_pre, nu_post, coarse_sweeps, fused), "cfd_batch_set_mg")
 
     def get_mg(self) -> tuple:
-        v = [ctypes.c_int() for _ in range(3)]
+        v = [ctypes.c_int() for _ in range(4)]
         _lib.check(_lib.lib().cfd_batch_get_mg(self.h, *[ctypes.byref(x) for x in v]), "cfd_batch_get_mg")
         return tuple(x.value for x in v)
 
     def autotune(self, steps: int = 5) -> tuple:
         """Pick the fastest multigrid schedule by timing candidates from the current state
-        (which is restored). Returns ((pre, post, coarse), ms per step)."""
-        out = (ctypes.c_int * 3)()
+        (which is restored). Returns ((pre, post, coarse, fused), ms per step)."""
+        out = (ctypes.c_int * 4)()
         ms = ctypes.c_double()
         _lib.check(_lib.lib().cfd_batch_autotune(self.h, steps, out, ctypes.byref(ms)), "cfd_batch_autotune")
         return tuple(out), ms.value

@@ -128,14 +128,16 @@ size_t cfd_case_bytes(int n0, int n1, int profile);
 int cfd_batch_fetch_stats(cfd_batch* b, cfd_step_stats* out, int cap);
 
 /* ---- multigrid schedule of the pressure preconditioner (no counterpart in the reference,
- * whose SIP solver has none): pre- and post-sweeps per level (1..8) and sweeps on the
- * coarsest level (1..256); defaults 1, 2, 12. cfd_batch_autotune() times a fixed list of
- * candidate schedules over `steps` steps each from the batch's current state (restored
- * before each candidate and on return, so the batch continues exactly where it was),
- * keeps the fastest and reports it as {pre, post, coarse} with its time per step. */
-int cfd_batch_set_mg(cfd_batch* b, int nu_pre, int nu_post, int coarse_sweeps);
-int cfd_batch_get_mg(cfd_batch* b, int* nu_pre, int* nu_post, int* coarse_sweeps);
-int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule3, double* out_ms_per_step);
+ * whose SIP solver has none): pre- and post-sweeps per level (1..8), sweeps on the
+ * coarsest level (1..256) and `fused` (1: a smoothing phase's sweeps run in one launch,
+ * tile halos held; 0: one launch per sweep); defaults 1, 2, 12, 1. cfd_batch_autotune()
+ * times a fixed list of candidate schedules over `steps` steps each from the batch's
+ * current state (restored before each candidate and on return, so the batch continues
+ * exactly where it was), keeps the fastest and reports it as {pre, post, coarse, fused}
+ * with its time per step. */
+int cfd_batch_set_mg(cfd_batch* b, int nu_pre, int nu_post, int coarse_sweeps, int fused);
+int cfd_batch_get_mg(cfd_batch* b, int* nu_pre, int* nu_post, int* coarse_sweeps, int* fused);
+int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule4, double* out_ms_per_step);
 
 /* ---- slots: continuous batching over a batch of fixed-geometry slots ----
  * Every case of a batch is a slot. cfd_batch_admit() writes a new case into slot `slot`

@@ -44,7 +44,7 @@ def test_runs_are_bitwise_reproducible():
 
 def test_schedules_agree_at_tight_tolerance():
     ref = _run((1, 1, 12), tight=True)
-    for sch in [(2, 2, 12), (1, 2, 24), (2, 1, 6)]:
+    for sch in [(2, 2, 12), (1, 2, 24), (2, 1, 6), (1, 2, 12, 1), (2, 3, 12, 1)]:
         got = _run(sch, tight=True)
         for fr, fg in zip(ref, got):
             for k in ("u", "v", "T"):
@@ -57,15 +57,15 @@ def test_autotune_keeps_state():
     gs, ps = _cases()
     with Batch(gs, ps) as b:
         b.step(3)
-        (pre, post, coarse), ms = b.autotune(steps=3)
-        assert ms > 0 and b.get_mg() == (pre, post, coarse)
+        (pre, post, coarse, fused), ms = b.autotune(steps=3)
+        assert ms > 0 and b.get_mg() == (pre, post, coarse, fused)
         b.step(4)
         got = [{k: b.plane(c, k) for k in ("u", "v", "T", "p")} for c in range(len(gs))]
         nstep = b.stats(0)["steps"]
     assert nstep == 7
     with Batch(gs, ps) as b:
         b.step(3)
-        b.set_mg(pre, post, coarse)
+        b.set_mg(pre, post, coarse, fused)
         b.step(4)
         ref = [{k: b.plane(c, k) for k in ("u", "v", "T", "p")} for c in range(len(gs))]
     for fr, fg in zip(ref, got):
