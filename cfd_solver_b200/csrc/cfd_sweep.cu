@@ -83,9 +83,11 @@ constexpr int SW_CELLS = TX * TYJ;
 constexpr int align128(int x) { return (x + 127) / 128 * 128; }
 
 // shared-memory layout: two field buffers, then alpha/beta/gamma (FP64, 3 planes) which
-// every thread overwrites with its cells' operator (5 planes of ST: E, G, B, 1/ap_u,
-// 1/ap_T) -- in place for FP64, behind them for FP32 (4-byte slots would overlap other
-// threads' unread 8-byte inputs)
+// every thread overwrites with its cells' operator (3 planes of ST: E, G, B -- in place for
+// FP64, behind them for FP32, whose 4-byte slots would overlap other threads' unread 8-byte
+// inputs), then the two inverse diagonals 1/ap_u, 1/ap_T in FP32. The diagonal only scales
+// each Jacobi correction (the residual is exact in ST), so its precision moves no fixed
+// point; holding it in FP32 lets five CTAs share an SM.
 template <int MODE>
 struct SwLayout {
     using C = SwCfg<MODE>;
@@ -99,7 +101,8 @@ struct SwLayout {
     static constexpr int BUF = PREV + (C::PREV ? align128(PBYTES) : 0);
     static constexpr int MET = 2 * BUF;
     static constexpr int OPS = sizeof(typename C::ST) == 8 ? MET : MET + (int)MBYTES;
-    static constexpr int TOTAL = OPS + 5 * SW_CELLS * (int)sizeof(typename C::ST);
+    static constexpr int RAP = OPS + 3 * SW_CELLS * (int)sizeof(typename C::ST);  // 1/ap_u, 1/ap_T (FP32)
+    static constexpr int TOTAL = RAP + 2 * SW_CELLS * (int)sizeof(float);
 };
 
 // FP64 plane of field f's iterate for state parity nxt (u*, v*, T, up, vp)
@@ -217,6 +220,7 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
     __syncthreads();
 
     ST* OPS = reinterpret_cast<ST*>(sm + L::OPS);
+    float* RAP = reinterpret_cast<float*>(sm + L::RAP);
     bool any_nearw = false;
 #pragma unroll
     for (int q = 0; q < SW_ROWS; q++) any_nearw |= nearw[q];
@@ -244,8 +248,8 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
                 OPS[o] = (ST)E;
                 OPS[SW_CELLS + o] = (ST)G;
                 OPS[2 * SW_CELLS + o] = (ST)B;
-                OPS[3 * SW_CELLS + o] = (ST)(1.0 / (1.0 + D));
-                OPS[4 * SW_CELLS + o] = (ST)(1.0 / (1.0 + D * rPr64));
+                RAP[o] = (float)(1.0 / (1.0 + D));
+                RAP[SW_CELLS + o] = (float)(1.0 / (1.0 + D * rPr64));
             }
         }
         const bool isT = f == F_T;
@@ -292,7 +296,7 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
         // the reference's T solve passes atnw in the annw slot (PSolver.cpp:1290): the
         // (i-1, j+2) coefficient of the 25-point T rows becomes anw = -8/9 B instead of B/9
         const bool tbug = isT && !c.fix_T_annw;
-        const int rapoff = (isT ? 4 : 3) * SW_CELLS;
+        const int rapoff = isT ? SW_CELLS : 0;
         double* dst64 = nullptr;
         float* dst32 = nullptr;
         float* res32 = nullptr;
@@ -317,7 +321,7 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
             sm_ *= scale;
             const ST D = (nearw[q] ? ST(2) : ST(2.5)) * (E + G);
             const ST ap = ST(1) + D * scale;
-            const ST rap = OPS[rapoff + o];
+            const ST rap = (ST)RAP[rapoff + o];
             const ST xk = w[q + 2][2];
             const ST res = rhs[q] - ap * xk - sm_;
             racc += inq[q] ? fabs((double)res) : 0.0;
