@@ -489,7 +489,7 @@ void enq_mid(cfd_batch* b, BatchDev& bd) {
     k_face_q<<<bd.njtiles, NT, kFaceQSmem, b->st>>>(bd);
 }
 void enq_p_iter(cfd_batch* b, BatchDev& bd) {
-    const int nf = bd.nftiles;
+    const int nf = bd.njtiles;  // the BiCGStab kernels run on the 32 x 16 tiles
     { Prof pr(b, K_BICG_P); k_bicg_p<<<nf, NT, 0, b->st>>>(bd); }
     run_vcycle(b);
     { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 0); }
@@ -1248,6 +1248,72 @@ static int state_copy(cfd_batch* b, void* host, size_t bytes, bool to_host) {
     }
     CK(cudaStreamSynchronize(b->st));
     return CFD_OK;
+}
+
+// Checkpoint file (replaces the reference's spa100.dat restart writer, PSolver.cpp:2006-2016):
+//   "CFDB200C" | u32 version 1 | u32 cases | per case i32 n0, n1, profile, precision |
+//   the state image of cfd_batch_get_state | u64 FNV-1a hash of all preceding bytes
+namespace {
+const char kCkptMagic[8] = {'C', 'F', 'D', 'B', '2', '0', '0', 'C'};
+uint64_t fnv1a(const unsigned char* p, size_t n, uint64_t h = 1469598103934665603ull) {
+    for (size_t k = 0; k < n; k++) {
+        h ^= p[k];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+}  // namespace
+
+int cfd_batch_save(cfd_batch* b, const char* path) {
+    if (!b || !path) return fail(CFD_E_ARG, "bad arguments");
+    const size_t sb = cfd_batch_state_bytes(b);
+    std::vector<unsigned char> buf(8 + 8 + (size_t)16 * b->n + sb + 8);
+    unsigned char* p = buf.data();
+    memcpy(p, kCkptMagic, 8);
+    const uint32_t hdr[2] = {1u, (uint32_t)b->n};
+    memcpy(p + 8, hdr, 8);
+    for (int c = 0; c < b->n; c++) {
+        const int32_t g[4] = {b->hc[c].n0, b->hc[c].n1, b->hc[c].profile, b->prm[c].precision};
+        memcpy(p + 16 + 16 * (size_t)c, g, 16);
+    }
+    unsigned char* st = p + 16 + 16 * (size_t)b->n;
+    if (int rc = cfd_batch_get_state(b, st, sb)) return rc;
+    const uint64_t h = fnv1a(p, buf.size() - 8);
+    memcpy(p + buf.size() - 8, &h, 8);
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(CFD_E_ARG, std::string("cannot write ") + path);
+    const bool ok = fwrite(p, 1, buf.size(), f) == buf.size();
+    if (fclose(f) != 0 || !ok) return fail(CFD_E_ARG, std::string("write failed: ") + path);
+    return CFD_OK;
+}
+
+int cfd_batch_load(cfd_batch* b, const char* path) {
+    if (!b || !path) return fail(CFD_E_ARG, "bad arguments");
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(CFD_E_ARG, std::string("cannot open ") + path);
+    std::vector<unsigned char> buf;
+    unsigned char tmp[1 << 16];
+    size_t n;
+    while ((n = fread(tmp, 1, sizeof(tmp), f)) > 0) buf.insert(buf.end(), tmp, tmp + n);
+    fclose(f);
+    const size_t sb = cfd_batch_state_bytes(b);
+    const size_t need = 8 + 8 + (size_t)16 * b->n + sb + 8;
+    if (buf.size() < 16 || memcmp(buf.data(), kCkptMagic, 8) != 0) return fail(CFD_E_ARG, "not a checkpoint file");
+    uint32_t hdr[2];
+    memcpy(hdr, buf.data() + 8, 8);
+    if (hdr[0] != 1u) return fail(CFD_E_ARG, "unsupported checkpoint version");
+    if ((int)hdr[1] != b->n || buf.size() != need)
+        return fail(CFD_E_ARG, "checkpoint does not match the batch (number of cases or sizes)");
+    uint64_t h;
+    memcpy(&h, buf.data() + need - 8, 8);
+    if (h != fnv1a(buf.data(), need - 8)) return fail(CFD_E_ARG, "checkpoint is corrupt (hash mismatch)");
+    for (int c = 0; c < b->n; c++) {
+        int32_t g[4];
+        memcpy(g, buf.data() + 16 + 16 * (size_t)c, 16);
+        if (g[0] != b->hc[c].n0 || g[1] != b->hc[c].n1 || g[2] != b->hc[c].profile || g[3] != b->prm[c].precision)
+            return fail(CFD_E_ARG, "checkpoint case " + std::to_string(c) + " has another geometry or precision");
+    }
+    return cfd_batch_set_state(b, buf.data() + 16 + 16 * (size_t)b->n, sb);
 }
 
 int cfd_batch_get_state(cfd_batch* b, void* host, size_t bytes) { return state_copy(b, host, bytes, true); }

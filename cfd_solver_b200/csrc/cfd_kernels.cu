@@ -493,58 +493,89 @@ __global__ void __launch_bounds__(NT, 3) k_face_q(BatchDev b) {
 
 // ---------------------------------------------------------------------------
 // BiCGStab, right-preconditioned, FP64 vectors; per-case scalars live on the device
-__global__ void __launch_bounds__(NT) k_bicg_p(BatchDev b) {
-    const Tile t = b.ftiles[blockIdx.x];
+// The BiCGStab kernels run on the 32 x 16 tiles, two cells per thread (rows lj and
+// lj + 8), every load of both cells issued before the arithmetic.
+__global__ void __launch_bounds__(NT, 3) k_bicg_p(BatchDev b) {
+    const Tile t = b.jtiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const bool first = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
     const CaseDev& c = b.cases[t.c];
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
-    if (i < c.ilo || i > c.ihi || j > c.n1 - 2) return;
+    const int i = t.i0 + (int)(threadIdx.x % TX), j0 = t.j0 + (int)(threadIdx.x / TX);
     const double* sc = b.scal + (long long)t.c * NSCAL;
     const double beta = sc[S_BETA], omega = sc[S_OMEGA];
-    const long long k = (long long)j * c.ld + i;
     double* Pv = plane(b, c, P_KP);
-    const double r = plane(b, c, P_KR)[k];
-    const double p = first ? r : r + beta * (Pv[k] - omega * plane(b, c, P_KV)[k]);
-    Pv[k] = p;
+    const double* R = plane(b, c, P_KR);
+    const double* Vv = plane(b, c, P_KV);
     const LevelDev& L = c.lev[0];
-    const long long k0 = (long long)j * L.ld + i;
-    mplane(b, L, M_B)[k0] = (float)p;
-    store_mirrored(mplane(b, L, M_X), L.ld, i, j, L.W, c.periodic, 0.0f);
+    bool in[2];
+    long long k[2];
+    double r[2], po[2], v[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int j = j0 + h * TY;
+        in[h] = i >= c.ilo && i <= c.ihi && j <= c.n1 - 2;
+        k[h] = in[h] ? (long long)j * c.ld + i : (long long)c.ld + c.ilo;
+        r[h] = R[k[h]];
+        po[h] = first ? 0.0 : Pv[k[h]];
+        v[h] = first ? 0.0 : Vv[k[h]];
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        if (!in[h]) continue;
+        const int j = j0 + h * TY;
+        const double p = first ? r[h] : r[h] + beta * (po[h] - omega * v[h]);
+        Pv[k[h]] = p;
+        mplane(b, L, M_B)[(long long)j * L.ld + i] = (float)p;
+        store_mirrored(mplane(b, L, M_X), L.ld, i, j, L.W, c.periodic, 0.0f);
+    }
 }
 
-// y = A * x with x = (double) MG level-0 iterate; mode 0: p_hat, v, (r_hat, v) -> alpha
-//                                                 mode 1: s_hat, t, (t, s), (t, t) -> omega
-__global__ void __launch_bounds__(NT) k_spmv(BatchDev b, int mode) {
-    const Tile t = b.ftiles[blockIdx.x];
+// y = A * x with x = (double) MG level-0 result; mode 0: p_hat, v, (r_hat, v) -> alpha
+//                                               mode 1: s_hat, t, (t, s), (t, t) -> omega
+__global__ void __launch_bounds__(NT, 3) k_spmv(BatchDev b, int mode) {
+    const Tile t = b.jtiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    const int i = t.i0 + (int)(threadIdx.x % TX), j0 = t.j0 + (int)(threadIdx.x / TX);
+    const int ld = c.ld;
+    const LevelDev& L = c.lev[0];
+    const int l0 = L.ld;
+    const float* X = mplane(b, L, mg_result_plane(b, c, 0));
+    const double* DOT = plane(b, c, mode == 0 ? P_Q : P_KS);
+    bool in[2];
+    long long k[2];
+    double y[2], xc[2], dv[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int j = j0 + h * TY;
+        in[h] = i >= c.ilo && i <= c.ihi && j <= c.n1 - 2;
+        const int jj = in[h] ? j : 1, ii = in[h] ? i : c.ilo;
+        const long long kk = (long long)jj * ld + ii, q = (long long)jj * l0 + ii;
+        k[h] = kk;
+        xc[h] = (double)X[q];
+        y[h] = plane(b, c, P_AP)[kk] * xc[h] + plane(b, c, P_AE)[kk] * (double)X[q + 1] +
+               plane(b, c, P_AW)[kk] * (double)X[q - 1] + plane(b, c, P_AN)[kk] * (double)X[q + l0] +
+               plane(b, c, P_AS)[kk] * (double)X[q - l0] + plane(b, c, P_ANE)[kk] * (double)X[q + l0 + 1] +
+               plane(b, c, P_ANW)[kk] * (double)X[q + l0 - 1] + plane(b, c, P_ASE)[kk] * (double)X[q - l0 + 1] +
+               plane(b, c, P_ASW)[kk] * (double)X[q - l0 - 1];
+        dv[h] = DOT[kk];
+    }
     double red[2] = {0.0, 0.0};
-    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
-        const int ld = c.ld;
-        const LevelDev& L = c.lev[0];
-        const int l0 = L.ld;
-        const float* X = mplane(b, L, mg_result_plane(b, c, 0));
-        const long long k = (long long)j * ld + i, q = (long long)j * l0 + i;
-        const double xc = (double)X[q];
-        const double y = plane(b, c, P_AP)[k] * xc + plane(b, c, P_AE)[k] * (double)X[q + 1] +
-                         plane(b, c, P_AW)[k] * (double)X[q - 1] + plane(b, c, P_AN)[k] * (double)X[q + l0] +
-                         plane(b, c, P_AS)[k] * (double)X[q - l0] + plane(b, c, P_ANE)[k] * (double)X[q + l0 + 1] +
-                         plane(b, c, P_ANW)[k] * (double)X[q + l0 - 1] + plane(b, c, P_ASE)[k] * (double)X[q - l0 + 1] +
-                         plane(b, c, P_ASW)[k] * (double)X[q - l0 - 1];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        if (!in[h]) continue;
         if (mode == 0) {
-            plane(b, c, P_KPH)[k] = xc;
-            plane(b, c, P_KV)[k] = y;
-            red[0] = plane(b, c, P_Q)[k] * y;
+            plane(b, c, P_KPH)[k[h]] = xc[h];
+            plane(b, c, P_KV)[k[h]] = y[h];
+            red[0] += dv[h] * y[h];
         } else {
-            plane(b, c, P_KSH)[k] = xc;
-            plane(b, c, P_KT)[k] = y;
-            red[0] = y * plane(b, c, P_KS)[k];
-            red[1] = y * y;
+            plane(b, c, P_KSH)[k[h]] = xc[h];
+            plane(b, c, P_KT)[k[h]] = y[h];
+            red[0] += y[h] * dv[h];
+            red[1] += y[h] * y[h];
         }
     }
-    if (case_reduce<2, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0) {
+    if (case_reduce<2, 0u>(b, t.c, blockIdx.x, c.jt_begin, c.jt_count, red) && threadIdx.x == 0) {
         double* sc = b.scal + (long long)t.c * NSCAL;
         int* is = b.iscal + (long long)t.c * NISCAL;
         if (mode == 0) {
@@ -564,28 +595,43 @@ __global__ void __launch_bounds__(NT) k_spmv(BatchDev b, int mode) {
 // s = r - alpha v, and the half step x += alpha p_hat; when |s| already meets the stop rule
 // the solve ends here (the standard early exit: x + alpha p_hat is the iterate whose
 // residual is s) and the second preconditioner application of the iteration is skipped
-__global__ void __launch_bounds__(NT) k_bicg_s(BatchDev b) {
-    const Tile t = b.ftiles[blockIdx.x];
+__global__ void __launch_bounds__(NT, 3) k_bicg_s(BatchDev b) {
+    const Tile t = b.jtiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const bool first = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
     const CaseDev& c = b.cases[t.c];
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    const int i = t.i0 + (int)(threadIdx.x % TX), j0 = t.j0 + (int)(threadIdx.x / TX);
     const double alpha = b.scal[(long long)t.c * NSCAL + S_ALPHA];
+    double* X = plane(b, c, P_PCOR);
+    const double *R = plane(b, c, P_KR), *Vv = plane(b, c, P_KV), *PH = plane(b, c, P_KPH);
+    const LevelDev& L = c.lev[0];
+    bool in[2];
+    long long k[2];
+    double x0[2], r[2], v[2], ph[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int j = j0 + h * TY;
+        in[h] = i >= c.ilo && i <= c.ihi && j <= c.n1 - 2;
+        k[h] = in[h] ? (long long)j * c.ld + i : (long long)c.ld + c.ilo;
+        x0[h] = first ? 0.0 : X[k[h]];
+        r[h] = R[k[h]];
+        v[h] = Vv[k[h]];
+        ph[h] = PH[k[h]];
+    }
     double red[1] = {0.0};
-    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
-        const long long k = (long long)j * c.ld + i;
-        double* X = plane(b, c, P_PCOR);
-        const double x0 = first ? 0.0 : X[k];
-        const double s = plane(b, c, P_KR)[k] - alpha * plane(b, c, P_KV)[k];
-        const double x = x0 + alpha * plane(b, c, P_KPH)[k];
-        plane(b, c, P_KS)[k] = s;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        if (!in[h]) continue;
+        const int j = j0 + h * TY;
+        const double s = r[h] - alpha * v[h];
+        const double x = x0[h] + alpha * ph[h];
+        plane(b, c, P_KS)[k[h]] = s;
         store_mirrored(X, c.ld, i, j, c.W, c.periodic, x);
-        const LevelDev& L = c.lev[0];
         mplane(b, L, M_B)[(long long)j * L.ld + i] = (float)s;
         store_mirrored(mplane(b, L, M_X), L.ld, i, j, L.W, c.periodic, 0.0f);
-        red[0] = fabs(s);
+        red[0] += fabs(s);
     }
-    if (case_reduce<1, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0) {
+    if (case_reduce<1, 0u>(b, t.c, blockIdx.x, c.jt_begin, c.jt_count, red) && threadIdx.x == 0) {
         double* sc = b.scal + (long long)t.c * NSCAL;
         int* is = b.iscal + (long long)t.c * NISCAL;
         const bool conv = red[0] <= c.tol_p * sc[S_NB1] || red[0] <= c.atol_p;
@@ -599,27 +645,43 @@ __global__ void __launch_bounds__(NT) k_bicg_s(BatchDev b) {
     }
 }
 
-__global__ void __launch_bounds__(NT) k_bicg_x(BatchDev b, int maxit) {
-    const Tile t = b.ftiles[blockIdx.x];
+__global__ void __launch_bounds__(NT, 3) k_bicg_x(BatchDev b, int maxit) {
+    const Tile t = b.jtiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
-    const int i = t.i0 + (int)(threadIdx.x % TX), j = t.j0 + (int)(threadIdx.x / TX);
+    const int i = t.i0 + (int)(threadIdx.x % TX), j0 = t.j0 + (int)(threadIdx.x / TX);
     const double* sc0 = b.scal + (long long)t.c * NSCAL;
     const double alpha = sc0[S_ALPHA], omega = sc0[S_OMEGA];
-    double red[2] = {0.0, 0.0};
-    if (i >= c.ilo && i <= c.ihi && j <= c.n1 - 2) {
-        const int ld = c.ld;
-        const long long k = (long long)j * ld + i;
-        double* X = plane(b, c, P_PCOR);
-        // x already carries the half step alpha p_hat (k_bicg_s)
-        const double x = X[k] + omega * plane(b, c, P_KSH)[k];
-        store_mirrored(X, ld, i, j, c.W, c.periodic, x);
-        const double r = plane(b, c, P_KS)[k] - omega * plane(b, c, P_KT)[k];
-        plane(b, c, P_KR)[k] = r;
-        red[0] = plane(b, c, P_Q)[k] * r;
-        red[1] = fabs(r);
+    const int ld = c.ld;
+    double* X = plane(b, c, P_PCOR);
+    const double *SH = plane(b, c, P_KSH), *S = plane(b, c, P_KS), *T = plane(b, c, P_KT), *Q = plane(b, c, P_Q);
+    bool in[2];
+    long long k[2];
+    double x0[2], sh[2], s[2], tt[2], q[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int j = j0 + h * TY;
+        in[h] = i >= c.ilo && i <= c.ihi && j <= c.n1 - 2;
+        k[h] = in[h] ? (long long)j * ld + i : (long long)ld + c.ilo;
+        x0[h] = X[k[h]];
+        sh[h] = SH[k[h]];
+        s[h] = S[k[h]];
+        tt[h] = T[k[h]];
+        q[h] = Q[k[h]];
     }
-    if (case_reduce<2, 0u>(b, t.c, blockIdx.x, c.tile_begin, c.tile_count, red) && threadIdx.x == 0) {
+    double red[2] = {0.0, 0.0};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        if (!in[h]) continue;
+        const int j = j0 + h * TY;
+        // x already carries the half step alpha p_hat (k_bicg_s)
+        store_mirrored(X, ld, i, j, c.W, c.periodic, x0[h] + omega * sh[h]);
+        const double r = s[h] - omega * tt[h];
+        plane(b, c, P_KR)[k[h]] = r;
+        red[0] += q[h] * r;
+        red[1] += fabs(r);
+    }
+    if (case_reduce<2, 0u>(b, t.c, blockIdx.x, c.jt_begin, c.jt_count, red) && threadIdx.x == 0) {
         double* sc = b.scal + (long long)t.c * NSCAL;
         int* is = b.iscal + (long long)t.c * NISCAL;
         const int it = ++is[I_PIT];
@@ -1361,17 +1423,31 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, const int* flag, int* 
 // ---------------------------------------------------------------------------
 // Resident state <-> one contiguous staging buffer (so a state snapshot crosses PCIe as one
 // copy per direction). Per case: the six state planes u, v, p, T, up, vp (whole padded
-// planes, ps doubles each, in that order), then 16 doubles whose first 4 bytes hold the
-// reference's int time. blockIdx.x = case * 7 + m (m = 6: the scalar slot).
+// planes, ps doubles each, in that order), then 16 doubles: int time and int steps taken,
+// then the first-step steady residual and continuity norm (the references of the relative
+// residuals). blockIdx.x = case * 7 + m (m = 6: the counter slot).
 __global__ void __launch_bounds__(256) k_state_pack(BatchDev b, double* stage, const long long* off, int to_stage) {
     const int c = blockIdx.x / 7, m = blockIdx.x % 7;
     const CaseDev& d = b.cases[c];
     double* dst = stage + off[c] + (long long)m * d.ps;
     if (m == 6) {
-        int* it = b.iscal + (long long)c * NISCAL + I_TIME;
+        // the case's counters: the reference's int time, the steps taken, and the
+        // first-step references of the relative residuals
+        int* is = b.iscal + (long long)c * NISCAL;
+        double* sc = b.scal + (long long)c * NSCAL;
+        int* di = reinterpret_cast<int*>(dst);
         if (threadIdx.x == 0) {
-            if (to_stage) *reinterpret_cast<int*>(dst) = *it;
-            else *it = *reinterpret_cast<const int*>(dst);
+            if (to_stage) {
+                di[0] = is[I_TIME];
+                di[1] = is[I_NSTEP];
+                dst[1] = sc[S_SR0];
+                dst[2] = sc[S_QL2_0];
+            } else {
+                is[I_TIME] = di[0];
+                is[I_NSTEP] = di[1];
+                sc[S_SR0] = dst[1];
+                sc[S_QL2_0] = dst[2];
+            }
         }
         return;
     }

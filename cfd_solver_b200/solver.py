@@ -130,6 +130,14 @@ class Batch:
         _lib.check(_lib.lib().cfd_batch_set_state(self.h, ctypes.c_void_p(_addr(buf)), self.state_bytes()),
                    "cfd_batch_set_state")
 
+    def save(self, path):
+        """Write a checkpoint file of every case's state (cfd_batch_save)."""
+        _lib.check(_lib.lib().cfd_batch_save(self.h, str(path).encode()), "cfd_batch_save")
+
+    def load(self, path):
+        """Restore a checkpoint written by save() for the same cases (cfd_batch_load)."""
+        _lib.check(_lib.lib().cfd_batch_load(self.h, str(path).encode()), "cfd_batch_load")
+
     def close(self):
         if self.h:
             _lib.lib().cfd_batch_destroy(self.h)

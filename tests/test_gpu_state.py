@@ -51,3 +51,38 @@ def test_snapshot_round_trip_is_exact():
         for k in FIELDS:
             np.testing.assert_array_equal(x[k], r[k], err_msg=k)
             np.testing.assert_array_equal(y[k], r[k], err_msg=k)
+
+
+def test_checkpoint_file_restart_is_exact(tmp_path):
+    from cfd_solver_b200 import _lib
+    from cfd_solver_b200.solver import Batch
+    gs, ps = _cases()
+    ck = tmp_path / "state.ckpt"
+    with Batch(gs, ps) as a:
+        a.step(5)
+        a.save(ck)
+        a.step(4)
+        ref = _fields(a, len(gs))
+        ref_st = [a.stats(c) for c in range(len(gs))]
+    with Batch(gs, ps) as fresh:
+        fresh.load(ck)
+        fresh.step(4)
+        got = _fields(fresh, len(gs))
+        got_st = [fresh.stats(c) for c in range(len(gs))]
+    for r, x, sr, sx in zip(ref, got, ref_st, got_st):
+        for k in FIELDS:
+            np.testing.assert_array_equal(x[k], r[k], err_msg=k)
+        # counters and relative residuals continue where they were
+        assert sx["steps"] == sr["steps"] == 9
+        assert sx["steady_res_rel"] == sr["steady_res_rel"]
+    # a corrupt file or another batch is rejected and leaves the batch untouched
+    raw = bytearray(ck.read_bytes())
+    raw[100] ^= 0xFF
+    bad = tmp_path / "bad.ckpt"
+    bad.write_bytes(bytes(raw))
+    with Batch(gs, ps) as other:
+        with pytest.raises(_lib.CfdError, match="corrupt"):
+            other.load(bad)
+    with Batch(gs[:2], ps[:2]) as other:
+        with pytest.raises(_lib.CfdError, match="does not match"):
+            other.load(ck)
