@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=512, help="requests of the serve workload")
     ap.add_argument("--rate", type=float, default=4.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--max-steps", type=int, default=1000, help="step cap per request (serve)")
+    ap.add_argument("--mg", default=None,
+                    help="multigrid schedule pre,post,coarse,fused (default: the library's)")
     return ap.parse_args()
 
 
@@ -158,6 +160,7 @@ def workload_config(args):
             "dt": "1e-4 (reference)" if args.form == "twin" else "CFL 0.4 / max(1, sqrt(Ri))",
             "inner_tolerances": "reference: relative L1 0.75e-2 (momentum and pressure)",
             "precision": args.precision,
+            "mg_schedule": args.mg or "library default (1,3,12,2)",
             "l2_flush": "inputs larger than L2 (>= 2.4 GB resident per step)",
             "parallelism": f"case-sharded, dp{args.gpus}"}
 
@@ -487,6 +490,9 @@ def main():
         params.append(case_params(g, precision=1 if args.precision == "mixed" else 0, **prm))
     cells = sum(g.n0 * g.n1 for g in grids)
     b = Batch(grids, params)
+    mg = tuple(int(x) for x in args.mg.split(",")) if args.mg else None
+    if mg:
+        b.set_mg(*mg)
     stream = torch.cuda.ExternalStream(b.stream())
 
     clocks = ClockSampler(local)
@@ -578,6 +584,8 @@ def main():
     subs = [Batch([grids[i] for i in p], [params[i] for i in p]) for p in parts]
     hosts = []
     for sb in subs:
+        if mg:
+            sb.set_mg(*mg)
         sb.step(1)  # builds the step graphs
         h = torch.empty(sb.state_bytes(), dtype=torch.uint8, pin_memory=True)
         sb.get_state(h)

@@ -52,12 +52,12 @@ long long rup(long long x, long long a) { return (x + a - 1) / a * a; }
 enum KernelId {
     K_ASSEMBLE_P, K_RHS, K_SWEEP, K_UPBC, K_FACE_Q, K_BICG_P, K_SPMV, K_BICG_S, K_BICG_X,
     K_MG_SMOOTH, K_MG_RR, K_MG_POST, K_MG_COARSE, K_MG_GALERKIN,
-    K_CORRECT, K_BC, K_DIAG, K_SI, K_MOM_UPDATE, K_SWEEP_FIN, NKERNEL
+    K_CORRECT, K_BC, K_DIAG, K_SI, K_MOM_UPDATE, K_SWEEP_FIN, K_MG_PRR, NKERNEL
 };
 const char* kKernelNames[NKERNEL] = {
     "k_assemble_p", "k_rhs", "k_sweep", "k_upbc", "k_face_q", "k_bicg_p", "k_spmv", "k_bicg_s",
     "k_bicg_x", "k_mg_presmooth", "k_mg_rr", "k_mg_postsmooth", "k_mg_coarse",
-    "k_mg_galerkin", "k_correct", "k_bc", "k_diag", "k_si", "k_mom_update", "k_sweep_fin"};
+    "k_mg_galerkin", "k_correct", "k_bc", "k_diag", "k_si", "k_mom_update", "k_sweep_fin", "k_mg_prr"};
 
 struct LevelGeom {
     int W, n1, ld, ilo, ihi;
@@ -183,11 +183,12 @@ struct cfd_batch {
     int ncol[MAXLEV] = {};
     int maxit_mom = 100, maxit_p = 200;
     int precision = CFD_PRECISION_FP64;
-    int sw_grid = 0;      // CTAs of the persistent sweep kernel
+    int sw_grid = 0;      // CTAs of the sweep kernel (one per 32 x 16 tile)
     size_t sw_smem = 0;
     int coarse_sweeps = 12;
-    int mg_pre = 1, mg_post = 2;  // multigrid sweeps before / after the coarse correction
-    int mg_fused = 1;             // 1: a smoothing phase's sweeps in one launch
+    int mg_pre = 1, mg_post = 3;  // multigrid sweeps before / after the coarse correction
+    int mg_fused = 2;             // 1: a smoothing phase's sweeps in one launch; 2: and the
+                                  // pre-smoothing inside the residual + restriction launch
     int max_W = 0;
     int cur = 0;
     long long steps_done = 0;
@@ -422,7 +423,8 @@ int mg_res_plane(int nu_pre, int nu_post, int fused) {
 
 // One V-cycle. Smoothing phases of several sweeps run either as one launch per sweep
 // (each sweep sees the neighbouring tiles' latest values) or, `mg_fused`, as one launch
-// doing all of the phase's sweeps in shared memory.
+// doing all of the phase's sweeps in shared memory; `mg_fused` = 2 also folds each level's
+// pre-smoothing into its residual + restriction launch (k_mg_prr).
 int run_vcycle(cfd_batch* b) {
     BatchDev& bd = b->bd;
     const int fused = b->mg_fused;
@@ -434,7 +436,10 @@ int run_vcycle(cfd_batch* b) {
             Prof pr(b, K_MG_COARSE);
             k_mg_coarse<<<bd.nccases[l], 1024, 0, b->st>>>(bd, l, b->coarse_sweeps);
         }
-        if (bd.nmtiles[l] > 0) {
+        if (bd.nmtiles[l] > 0 && fused == 2) {
+            Prof pr(b, K_MG_PRR);
+            k_mg_prr<<<bd.natiles[l + 1], NT, kMgPrrSmem, b->st>>>(bd, l, pre, b->mg_pre);
+        } else if (bd.nmtiles[l] > 0) {
             for (int s = 0; s < npre; s++) {  // pre-smoothing from zero
                 Prof pr(b, K_MG_SMOOTH);
                 const int dst = (s & 1) ? M_R : M_X;
@@ -900,6 +905,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         CK(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem));
         CK(cudaFuncSetAttribute(k_face_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFaceQSmem));
         CK(cudaFuncSetAttribute(k_mg_gs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgGsSmem));
+        CK(cudaFuncSetAttribute(k_mg_prr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgPrrSmem));
     }
 
     // ---- tile tables
@@ -1052,8 +1058,8 @@ int cfd_batch_destroy(cfd_batch* b) {
 int cfd_batch_set_mg(cfd_batch* b, int nu_pre, int nu_post, int coarse_sweeps, int fused) {
     if (!b) return fail(CFD_E_ARG, "null batch");
     if (nu_pre < 1 || nu_pre > 8 || nu_post < 1 || nu_post > 8 || coarse_sweeps < 1 || coarse_sweeps > 256 ||
-        (fused != 0 && fused != 1))
-        return fail(CFD_E_ARG, "multigrid schedule out of range (sweeps 1..8, coarse sweeps 1..256, fused 0/1)");
+        fused < 0 || fused > 2)
+        return fail(CFD_E_ARG, "multigrid schedule out of range (sweeps 1..8, coarse sweeps 1..256, fused 0..2)");
     CK(cudaStreamSynchronize(b->st));
     b->mg_pre = nu_pre;
     b->mg_post = nu_post;
@@ -1078,8 +1084,10 @@ int cfd_batch_get_mg(cfd_batch* b, int* nu_pre, int* nu_post, int* coarse_sweeps
 // fastest and reports its time per step. The batch's state is unchanged on return.
 int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule, double* out_ms_per_step) {
     if (!b || steps < 1) return fail(CFD_E_ARG, "bad arguments");
-    static const int cand[][4] = {{1, 1, 12, 0}, {1, 2, 12, 0}, {2, 1, 12, 0}, {2, 2, 12, 0}, {1, 1, 24, 0},
-                                  {1, 2, 24, 0}, {1, 2, 12, 1}, {1, 3, 12, 1}, {2, 2, 12, 1}, {2, 3, 12, 1}};
+    static const int cand[][4] = {{1, 1, 12, 0}, {1, 2, 12, 0}, {2, 1, 12, 0}, {2, 2, 12, 0},
+                                  {1, 2, 12, 1}, {1, 3, 12, 1}, {2, 2, 12, 1}, {2, 3, 12, 1},
+                                  {1, 2, 12, 2}, {1, 3, 12, 2}, {1, 4, 12, 2}, {1, 3, 8, 2},
+                                  {2, 2, 12, 2}, {2, 3, 12, 2}};
     const int ncand = (int)(sizeof(cand) / sizeof(cand[0]));
     const size_t n64 = (size_t)b->n64 * sizeof(double), nsc = sizeof(double) * NSCAL * b->n,
                  nis = sizeof(int) * NISCAL * b->n;

@@ -426,7 +426,10 @@ __global__ void __launch_bounds__(NT, 3) k_face_q(BatchDev b) {
     const double *P = sm, *U = sm + JTW * JTH, *V = sm + 2 * JTW * JTH, *X = sm + 3 * JTW * JTH,
                  *Y = sm + 4 * JTW * JTH, *E = sm + 5 * JTW * JTH, *G = sm + 6 * JTW * JTH;
     const int ld = c.ld;
-    const double d0 = c.d0, d1 = c.d1, dt = c.dt;
+    // reciprocals once per thread: the per-cell quotients become products (each within an
+    // ulp of the quotient; 1 / (4 d) is 0.25 / d exactly)
+    const double dt = c.dt, rd0 = 1.0 / c.d0, rd1 = 1.0 / c.d1, q0 = 0.25 * rd0, q1 = 0.25 * rd1;
+    const double hdt = 0.5 * dt, rdt = 1.0 / dt;
     const int li = tid % TX, lj = tid / TX;
     const int i = t.i0 + li;
     double red[3] = {0.0, 0.0, 0.0};
@@ -435,28 +438,28 @@ __global__ void __launch_bounds__(NT, 3) k_face_q(BatchDev b) {
         if (!ok || i < c.ilo || i > c.ihi || j > c.n1 - 2) continue;
         const int k = (lj + h * TY + 2) * JTW + (li + 2);
         const int kE = k + 1, kW = k - 1, kN = k + JTW, kS = k - JTW;
-        double dpdxi_ip = (P[kE] - P[k]) / d0;
-        double dpde_ip = (P[kN + 1] + P[kN] - P[kS] - P[kS + 1]) / (4.0 * d1);
-        double dpdxi_in = (P[k] - P[kW]) / d0;
-        double dpde_in = (P[kN] + P[kN - 1] - P[kS] - P[kS - 1]) / (4.0 * d1);
-        double dpdxi_jp = (P[kN + 1] - P[kN - 1] + P[kE] - P[kW]) / (4.0 * d0);
-        double dpde_jp = (P[kN] - P[k]) / d1;
-        double dpdxi_jn = (P[kE] - P[kW] + P[kS + 1] - P[kS - 1]) / (4.0 * d0);
-        double dpde_jn = (P[k] - P[kS]) / d1;
-        double us_ip = 0.5 * (U[k] + U[kE]) - 0.5 * dt * ((X[k] + X[kE]) * dpdxi_ip + (E[k] + E[kE]) * dpde_ip);
-        double us_in = 0.5 * (U[k] + U[kW]) - 0.5 * dt * ((X[k] + X[kW]) * dpdxi_in + (E[k] + E[kW]) * dpde_in);
-        double us_jp = 0.5 * (U[k] + U[kN]) - 0.5 * dt * ((X[k] + X[kN]) * dpdxi_jp + (E[k] + E[kN]) * dpde_jp);
-        double us_jn = 0.5 * (U[k] + U[kS]) - 0.5 * dt * ((X[k] + X[kS]) * dpdxi_jn + (E[k] + E[kS]) * dpde_jn);
-        double vs_ip = 0.5 * (V[k] + V[kE]) - 0.5 * dt * ((Y[k] + Y[kE]) * dpdxi_ip + (G[k] + G[kE]) * dpde_ip);
-        double vs_in = 0.5 * (V[k] + V[kW]) - 0.5 * dt * ((Y[k] + Y[kW]) * dpdxi_in + (G[k] + G[kW]) * dpde_in);
-        double vs_jp = 0.5 * (V[k] + V[kN]) - 0.5 * dt * ((Y[k] + Y[kN]) * dpdxi_jp + (G[k] + G[kN]) * dpde_jp);
-        double vs_jn = 0.5 * (V[k] + V[kS]) - 0.5 * dt * ((Y[k] + Y[kS]) * dpdxi_jn + (G[k] + G[kS]) * dpde_jn);
-        double dusdxi = (us_ip - us_in) / d0;
-        double dusde = (us_jp - us_jn) / d1;
-        double dvsdxi = (vs_ip - vs_in) / d0;
-        double dvsde = (vs_jp - vs_jn) / d1;
+        double dpdxi_ip = (P[kE] - P[k]) * rd0;
+        double dpde_ip = (P[kN + 1] + P[kN] - P[kS] - P[kS + 1]) * q1;
+        double dpdxi_in = (P[k] - P[kW]) * rd0;
+        double dpde_in = (P[kN] + P[kN - 1] - P[kS] - P[kS - 1]) * q1;
+        double dpdxi_jp = (P[kN + 1] - P[kN - 1] + P[kE] - P[kW]) * q0;
+        double dpde_jp = (P[kN] - P[k]) * rd1;
+        double dpdxi_jn = (P[kE] - P[kW] + P[kS + 1] - P[kS - 1]) * q0;
+        double dpde_jn = (P[k] - P[kS]) * rd1;
+        double us_ip = 0.5 * (U[k] + U[kE]) - hdt * ((X[k] + X[kE]) * dpdxi_ip + (E[k] + E[kE]) * dpde_ip);
+        double us_in = 0.5 * (U[k] + U[kW]) - hdt * ((X[k] + X[kW]) * dpdxi_in + (E[k] + E[kW]) * dpde_in);
+        double us_jp = 0.5 * (U[k] + U[kN]) - hdt * ((X[k] + X[kN]) * dpdxi_jp + (E[k] + E[kN]) * dpde_jp);
+        double us_jn = 0.5 * (U[k] + U[kS]) - hdt * ((X[k] + X[kS]) * dpdxi_jn + (E[k] + E[kS]) * dpde_jn);
+        double vs_ip = 0.5 * (V[k] + V[kE]) - hdt * ((Y[k] + Y[kE]) * dpdxi_ip + (G[k] + G[kE]) * dpde_ip);
+        double vs_in = 0.5 * (V[k] + V[kW]) - hdt * ((Y[k] + Y[kW]) * dpdxi_in + (G[k] + G[kW]) * dpde_in);
+        double vs_jp = 0.5 * (V[k] + V[kN]) - hdt * ((Y[k] + Y[kN]) * dpdxi_jp + (G[k] + G[kN]) * dpde_jp);
+        double vs_jn = 0.5 * (V[k] + V[kS]) - hdt * ((Y[k] + Y[kS]) * dpdxi_jn + (G[k] + G[kS]) * dpde_jn);
+        double dusdxi = (us_ip - us_in) * rd0;
+        double dusde = (us_jp - us_jn) * rd1;
+        double dvsdxi = (vs_ip - vs_in) * rd0;
+        double dvsde = (vs_jp - vs_jn) * rd1;
         double qq = (X[k] * dusdxi) + (E[k] * dusde) + (Y[k] * dvsdxi) + (G[k] * dvsde);
-        const double q = qq / dt;
+        const double q = qq * rdt;
         // q doubles as BiCGStab's shadow residual r_hat; p, v and the iterate pcor are
         // initialised by the first iteration's kernels (beta = 0, x = 0)
         const long long kg = (long long)j * ld + i;
@@ -774,6 +777,122 @@ __global__ void __launch_bounds__(NT) k_mg_rr(BatchDev b, int l, int src) {
     store_mirrored(mplane(b, C, M_X), C.ld, I, J, C.W, per, 0.0f);
 }
 
+// Pre-smoothing folded into the residual + restriction pass (schedule form `fused` = 2).
+// One CTA per 32 x 8 tile of level l + 1. Its fine region E (the 65 x 17 fine points the
+// restriction reads plus a one-cell ring: 67 x 19) is smoothed from zero in shared memory,
+// zero outside E, by `inner` multicolour Gauss-Seidel sweeps; the residual is formed from
+// that x and restricted into b_{l+1}; x is stored for the fine points the tile owns
+// (columns 2 i0 .. 2 i0 + 63, rows 2 j0 - 1 .. 2 j0 + 14, and in the last tile row also the
+// rows up to n1 - 2), where the post-smoother starts. Neighbouring regions overlap by up to
+// three cells, and on a region's ring the residual uses the region's own smoothed x, not
+// the owner's stored one. The V-cycle stays a fixed linear map (each CTA reads only level
+// planes no CTA of the launch writes); it is a different map from form 1's, with the
+// level's pre-smoothing pass and its read of the stencil saved.
+constexpr int MPR_EW = 2 * TX + 3, MPR_EH = 2 * TY + 3;  // smoothed region E
+constexpr int MPR_XW = MPR_EW + 2, MPR_XH = MPR_EH + 2;  // E plus a zero ring
+constexpr int MPR_RW = 2 * TX + 1, MPR_RH = 2 * TY + 1;  // fine residual region
+constexpr int MPR_NE = MPR_EW * MPR_EH;
+constexpr size_t MPR_SMEM = (size_t)(10 * MPR_NE + MPR_XW * MPR_XH + MPR_RW * MPR_RH) * sizeof(float) + MPR_NE;
+const size_t kMgPrrSmem = MPR_SMEM;
+
+__global__ void __launch_bounds__(NT) k_mg_prr(BatchDev b, int l, int dst, int inner) {
+    extern __shared__ __align__(16) unsigned char mpraw[];
+    // cf: ap, ae, aw, an, as, ane, anw, ase, asw, b of every point of E
+    float(*cf)[MPR_NE] = reinterpret_cast<float(*)[MPR_NE]>(mpraw);
+    float* xs = reinterpret_cast<float*>(mpraw) + 10 * MPR_NE;
+    float* rs = xs + MPR_XW * MPR_XH;
+    signed char* unk = reinterpret_cast<signed char*>(rs + MPR_RW * MPR_RH);  // 1: an unknown
+    const Tile t = b.atiles[l + 1][blockIdx.x];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const LevelDev& F = c.lev[l];
+    const LevelDev& C = c.lev[l + 1];
+    const int tid = threadIdx.x;
+    const int fl = F.ld, W = F.W, per = c.periodic, n1 = F.n1;
+    // a level with a coarser one has an even width when periodic, so its colours are the
+    // four parity classes, and E (whose origin is even in both directions) holds colour
+    // (x & 1) | ((y & 1) << 1) at its point (x, y)
+    if (per && (W & 1)) {
+        if (tid == 0) atomicExch(b.error, 1);
+        return;
+    }
+    const int ei0 = 2 * t.i0 - 2, ej0 = 2 * t.j0 - 2;  // level-l (column, row) of E's first point
+    for (int e = tid; e < MPR_XW * MPR_XH; e += NT) xs[e] = 0.0f;
+    // every load of the stencil of E issued before the first shared-memory store
+    constexpr int NLD = (MPR_NE + NT - 1) / NT;
+    float v[NLD][10];
+    bool ok[NLD];
+#pragma unroll
+    for (int m = 0; m < NLD; m++) {
+        const int e = tid + m * NT;
+        const int gj = ej0 + e / MPR_EW, gi = ei0 + e % MPR_EW;
+        const int col = per ? ((gi % W) + W) % W : gi;
+        ok[m] = e < MPR_NE && gj >= 1 && gj <= n1 - 2 && col >= F.ilo && col <= F.ihi;
+        const long long k = ok[m] ? (long long)gj * fl + col : (long long)fl + F.ilo;
+#pragma unroll
+        for (int q = 0; q < 9; q++) v[m][q] = mplane(b, F, M_AP + q)[k];
+        v[m][9] = mplane(b, F, M_B)[k];
+    }
+#pragma unroll
+    for (int m = 0; m < NLD; m++) {
+        const int e = tid + m * NT;
+        if (e >= MPR_NE) continue;
+#pragma unroll
+        for (int q = 0; q < 10; q++) cf[q][e] = ok[m] ? v[m][q] : 0.0f;
+        unk[e] = ok[m] ? 1 : 0;
+    }
+    __syncthreads();
+    // multicolour Gauss-Seidel, each colour's points enumerated directly
+    for (int n = 0; n < 4 * inner; n++) {
+        const int cc = n & 3, px = cc & 1, py = cc >> 1;
+        const int nx = (MPR_EW - px + 1) >> 1, ny = (MPR_EH - py + 1) >> 1;
+        for (int s2 = tid; s2 < nx * ny; s2 += NT) {
+            const int x = px + 2 * (s2 % nx), y = py + 2 * (s2 / nx);
+            const int e = y * MPR_EW + x;
+            if (!unk[e]) continue;
+            const int o = (y + 1) * MPR_XW + (x + 1);
+            const float sm = cf[1][e] * xs[o + 1] + cf[2][e] * xs[o - 1] + cf[3][e] * xs[o + MPR_XW] +
+                             cf[4][e] * xs[o - MPR_XW] + cf[5][e] * xs[o + MPR_XW + 1] +
+                             cf[6][e] * xs[o + MPR_XW - 1] + cf[7][e] * xs[o - MPR_XW + 1] +
+                             cf[8][e] * xs[o - MPR_XW - 1];
+            xs[o] = (cf[9][e] - sm) / cf[0][e];
+        }
+        __syncthreads();
+    }
+    // residual on the restriction's fine points (E without its ring)
+    for (int e = tid; e < MPR_RW * MPR_RH; e += NT) {
+        const int rj = e / MPR_RW, ri = e % MPR_RW;
+        const int q = (rj + 1) * MPR_EW + (ri + 1);
+        float r = 0.0f;
+        if (unk[q]) {
+            const int o = (rj + 2) * MPR_XW + (ri + 2);
+            const float ax = cf[0][q] * xs[o] + cf[1][q] * xs[o + 1] + cf[2][q] * xs[o - 1] +
+                             cf[3][q] * xs[o + MPR_XW] + cf[4][q] * xs[o - MPR_XW] + cf[5][q] * xs[o + MPR_XW + 1] +
+                             cf[6][q] * xs[o + MPR_XW - 1] + cf[7][q] * xs[o - MPR_XW + 1] +
+                             cf[8][q] * xs[o - MPR_XW - 1];
+            r = cf[9][q] - ax;
+        }
+        rs[e] = r;
+    }
+    // smoothed x of the owned fine points
+    float* OUT = mplane(b, F, dst);
+    const int jhi = (t.j0 + TY > C.n1 - 2) ? n1 - 2 : min(2 * t.j0 + 14, n1 - 2);
+    for (int e = tid; e < 2 * TX * (2 * TY + 1); e += NT) {
+        const int gi = 2 * t.i0 + e % (2 * TX), gj = 2 * t.j0 - 1 + e / (2 * TX);
+        if (gi < F.ilo || gi > F.ihi || gj > jhi) continue;
+        store_mirrored(OUT, fl, gi, gj, W, per, xs[(gj - ej0 + 1) * MPR_XW + (gi - ei0 + 1)]);
+    }
+    __syncthreads();
+    const int li = tid % TX, lj = tid / TX;
+    const int I = t.i0 + li, J = t.j0 + lj;
+    if (I < C.ilo || I > C.ihi || J > C.n1 - 2) return;
+    const int f = (2 * lj + 1) * MPR_RW + (2 * li + 1);  // fine (2I, 2J) in the residual region
+    const float r4 = 0.0625f * (rs[f - MPR_RW - 1] + rs[f - MPR_RW + 1] + rs[f + MPR_RW - 1] + rs[f + MPR_RW + 1]) +
+                     0.125f * (rs[f - MPR_RW] + rs[f + MPR_RW] + rs[f - 1] + rs[f + 1]) + 0.25f * rs[f];
+    mplane(b, C, M_B)[(long long)J * C.ld + I] = r4;
+    store_mirrored(mplane(b, C, M_X), C.ld, I, J, C.W, per, 0.0f);
+}
+
 // bilinear prolongation of the coarse result at fine point (i, j), i in [0, W)
 __device__ __forceinline__ float mg_prolong_at(const float* XC, int cl, int i, int j) {
     const int I = i >> 1, J = j >> 1;
@@ -807,16 +926,22 @@ __global__ void __launch_bounds__(NT) k_mg_gs(BatchDev b, int l, int mode, int s
     float* xs = reinterpret_cast<float*>(mgraw);
     float(*cf)[MGS_RW * MGS_RH] = reinterpret_cast<float(*)[MGS_RW * MGS_RH]>(xs + MGS_XH * MGS_XW);
     // cf: ap, ae, aw, an, as, ane, anw, ase, asw, b of every relaxed point
-    signed char* colr = reinterpret_cast<signed char*>(xs + MGS_XH * MGS_XW + 10 * MGS_RW * MGS_RH);
+    signed char* unk = reinterpret_cast<signed char*>(xs + MGS_XH * MGS_XW + 10 * MGS_RW * MGS_RH);
     const Tile t = b.mtiles[l][blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
     const LevelDev& L = c.lev[l];
     const int tid = threadIdx.x;
     const int ld = L.ld, W = L.W, per = c.periodic, n1 = L.n1;
-    const int ncol = (per && (W & 1)) ? 6 : 4;
-    const int ov = MGS_OV;
-    const int rw = TX + 2 * ov, rh = TYJ + 2 * ov, xw = rw + 2, xh = rh + 2;
+    // a level with a coarser one has an even width when periodic: the colours are the four
+    // parity classes, and with the tile origin (even column, odd row) the point (x, y) of
+    // the tile has colour (x & 1) | ((~y & 1) << 1)
+    if (per && (W & 1)) {
+        if (tid == 0) atomicExch(b.error, 1);
+        return;
+    }
+    constexpr int ov = MGS_OV, rw = MGS_RW, rh = MGS_RH, xw = MGS_XW, xh = MGS_XH;
+    static_assert(MGS_OV == 0, "the colour lattice below assumes no overlap");
     const bool zero = mode == 0, prolong = mode == 2, reverse = mode >= 2;
     const float* X = mplane(b, L, src);
     const float* XC = prolong ? mplane(b, c.lev[l + 1], mg_result_plane(b, c, l + 1)) : nullptr;
@@ -826,39 +951,58 @@ __global__ void __launch_bounds__(NT) k_mg_gs(BatchDev b, int l, int mode, int s
         if (per) return ((gi % W) + W) % W;
         return (gi >= 0 && gi < W) ? gi : -1;
     };
-    for (int e = tid; e < xh * xw; e += NT) {
+    // every global load issued before the first shared-memory store
+    constexpr int NXL = (xh * xw + NT - 1) / NT, NPL = (rw * rh + NT - 1) / NT;
+    float xv[NXL];
+#pragma unroll
+    for (int m = 0; m < NXL; m++) {
+        const int e = tid + m * NT;
         const int gj = t.j0 - ov - 1 + e / xw, col = column(t.i0 - ov - 1 + e % xw);
         float v = 0.0f;
-        if (!zero && gj >= 0 && gj < n1 && col >= 0) {
+        if (!zero && e < xh * xw && gj >= 0 && gj < n1 && col >= 0) {
             v = X[(long long)gj * ld + col];
             if (prolong && gj >= 1 && gj <= n1 - 2 && col >= L.ilo && col <= L.ihi)
                 v += mg_prolong_at(XC, cl, col, gj);
         }
-        xs[e] = v;
+        xv[m] = v;
     }
-    for (int e = tid; e < rh * rw; e += NT) {
-        const int gj = t.j0 - ov + e / rw, col = column(t.i0 - ov + e % rw);
-        signed char cc = -1;
-        if (gj >= 1 && gj <= n1 - 2 && col >= L.ilo && col <= L.ihi) {
-            const long long k = (long long)gj * ld + col;
+    float cv[NPL][10];
+    bool ok[NPL];
 #pragma unroll
-            for (int m = 0; m < 9; m++) cf[m][e] = mplane(b, L, M_AP + m)[k];
-            cf[9][e] = mplane(b, L, M_B)[k];
-            cc = (signed char)mg_colour(col, gj, W, per);
-        }
-        colr[e] = cc;
+    for (int m = 0; m < NPL; m++) {
+        const int e = tid + m * NT;
+        const int gj = t.j0 - ov + e / rw, col = column(t.i0 - ov + e % rw);
+        ok[m] = e < rw * rh && gj >= 1 && gj <= n1 - 2 && col >= L.ilo && col <= L.ihi;
+        const long long k = ok[m] ? (long long)gj * ld + col : (long long)ld + L.ilo;
+#pragma unroll
+        for (int q = 0; q < 9; q++) cv[m][q] = mplane(b, L, M_AP + q)[k];
+        cv[m][9] = mplane(b, L, M_B)[k];
+    }
+#pragma unroll
+    for (int m = 0; m < NXL; m++)
+        if (tid + m * NT < xh * xw) xs[tid + m * NT] = xv[m];
+#pragma unroll
+    for (int m = 0; m < NPL; m++) {
+        const int e = tid + m * NT;
+        if (e >= rw * rh) continue;
+#pragma unroll
+        for (int q = 0; q < 10; q++) cf[q][e] = ok[m] ? cv[m][q] : 0.0f;
+        unk[e] = ok[m] ? 1 : 0;
     }
     __syncthreads();
-    for (int n = 0; n < ncol * inner; n++) {
-        const int cn = n % ncol;
-        const int cc = reverse ? ncol - 1 - cn : cn;
-        for (int e = tid; e < rh * rw; e += NT) {
-            if (colr[e] != cc) continue;
-            const int o = (e / rw + 1) * xw + (e % rw + 1);
-            const float s = cf[1][e] * xs[o + 1] + cf[2][e] * xs[o - 1] + cf[3][e] * xs[o + xw] +
-                            cf[4][e] * xs[o - xw] + cf[5][e] * xs[o + xw + 1] + cf[6][e] * xs[o + xw - 1] +
-                            cf[7][e] * xs[o - xw + 1] + cf[8][e] * xs[o - xw - 1];
-            xs[o] = (cf[9][e] - s) / cf[0][e];
+    for (int n = 0; n < 4 * inner; n++) {
+        const int cc = reverse ? 3 - (n & 3) : (n & 3);
+        const int px = cc & 1, py = ((cc >> 1) & 1) ^ 1;  // row parity of the colour within the tile
+        const int nx = (rw - px + 1) >> 1, ny = (rh - py + 1) >> 1;
+        for (int s2 = tid; s2 < nx * ny; s2 += NT) {
+            const int x = px + 2 * (s2 % nx), y = py + 2 * (s2 / nx);
+            const int e = y * rw + x;
+            if (!unk[e]) continue;
+            const int o = (y + 1) * xw + (x + 1);
+            const float sm = cf[1][e] * xs[o + 1] + cf[2][e] * xs[o - 1] + cf[3][e] * xs[o + xw] +
+                             cf[4][e] * xs[o - xw] + cf[5][e] * xs[o + xw + 1] + cf[6][e] * xs[o + xw - 1] +
+                             cf[7][e] * xs[o - xw + 1] + cf[8][e] * xs[o - xw - 1];
+            xs[o] = (cf[9][e] - sm) / cf[0][e];
         }
         __syncthreads();
     }
@@ -1045,7 +1189,7 @@ __global__ void __launch_bounds__(NT, 3) k_correct(BatchDev b) {
         u0[h] = U[k]; v0[h] = V[k]; p0[h] = P[k];
     }
     const double vnn = c.uinf * VEC[2LL * ld + i] + c.vinf * VEC[3LL * ld + i];
-    const double d0 = c.d0, d1 = c.d1, dt = c.dt;
+    const double h0 = 0.5 / c.d0, h1 = 0.5 / c.d1, dt = c.dt;  // the gradients' quotients as products
     double red[1] = {0.0};
 #pragma unroll
     for (int h = 0; h < 2; h++) {
@@ -1059,8 +1203,8 @@ __global__ void __launch_bounds__(NT, 3) k_correct(BatchDev b) {
         const double pS = none ? 0.0 : (j == 1) ? pc : ps0[h];
         const double pE = none ? 0.0 : (cav && i == n0 - 2) ? pc : pe0[h];
         const double pW = none ? 0.0 : (cav && i == 1) ? pc : pw0[h];
-        const double dpcor_dxi = 0.5 * (pE - pW) / d0;
-        const double dpcor_de = 0.5 * (pN - pS) / d1;
+        const double dpcor_dxi = (pE - pW) * h0;
+        const double dpcor_de = (pN - pS) * h1;
         const double un = us[h] - dt * (xix[h] * dpcor_dxi + etx[h] * dpcor_de);
         const double vn = vs[h] - dt * (xiy[h] * dpcor_dxi + ety[h] * dpcor_de);
         red[0] += fabs(un - u0[h]) + fabs(vn - v0[h]);
@@ -1350,18 +1494,19 @@ __global__ void __launch_bounds__(NT, 3) k_diag(BatchDev b) {
         xix[h] = XIX[k]; xiy[h] = XIY[k]; etx[h] = ETX[k]; ety[h] = ETY[k];
         tn[h] = TN[k]; to[h] = TO[k];
     }
-    const double d0 = c.d0, d1 = c.d1;
+    // 0.5 / d is 1 / (2 d) exactly: the dilatation's quotients become products
+    const double h0 = 0.5 / c.d0, h1 = 0.5 / c.d1;
     double red[3] = {-1.0e300, 0.0, 0.0};
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         if (!in[h]) continue;
         const int j = t.j0 + (int)(threadIdx.x / TX) + h * TY;
-        const double dil = xix[h] * (ue[h] - uw[h]) / (2 * d0) + etx[h] * (un[h] - us[h]) / (2 * d1) +
-                           ety[h] * (vn[h] - vs[h]) / (2 * d1) + xiy[h] * (ve[h] - vw[h]) / (2 * d0);
-        const double dv_dxi = 0.5 / d0 * (ve[h] - vw[h]);
-        const double dv_det = 0.5 / d1 * (vn[h] - vs[h]);
-        const double du_dxi = 0.5 / d0 * (ue[h] - uw[h]);
-        const double du_det = 0.5 / d1 * (un[h] - us[h]);
+        const double dil = xix[h] * (ue[h] - uw[h]) * h0 + etx[h] * (un[h] - us[h]) * h1 +
+                           ety[h] * (vn[h] - vs[h]) * h1 + xiy[h] * (ve[h] - vw[h]) * h0;
+        const double dv_dxi = h0 * (ve[h] - vw[h]);
+        const double dv_det = h1 * (vn[h] - vs[h]);
+        const double du_dxi = h0 * (ue[h] - uw[h]);
+        const double du_det = h1 * (un[h] - us[h]);
         const double vort = (xix[h] * dv_dxi + etx[h] * dv_det) - (xiy[h] * du_dxi + ety[h] * du_det);
         store_mirrored(plane(b, c, P_VORT), ld, i, j, W, per, vort);
         store_mirrored(plane(b, c, P_DIL), ld, i, j, W, per, dil);

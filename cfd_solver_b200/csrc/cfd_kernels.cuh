@@ -16,6 +16,8 @@ __global__ void k_bicg_x(BatchDev b, int maxit);
 __global__ void k_mg_gs(BatchDev b, int l, int mode, int src, int dst, int inner);
 extern const size_t kMgGsSmem;  // dynamic shared memory of k_mg_gs
 __global__ void k_mg_rr(BatchDev b, int l, int src);
+__global__ void k_mg_prr(BatchDev b, int l, int dst, int inner);
+extern const size_t kMgPrrSmem;  // dynamic shared memory of k_mg_prr
 __global__ void k_mg_coarse(BatchDev b, int l, int sweeps);
 __global__ void k_mg_galerkin(BatchDev b, int l, int toff);
 __global__ void k_correct(BatchDev b);

@@ -130,8 +130,9 @@ int cfd_batch_fetch_stats(cfd_batch* b, cfd_step_stats* out, int cap);
 /* ---- multigrid schedule of the pressure preconditioner (no counterpart in the reference,
  * whose SIP solver has none): pre- and post-sweeps per level (1..8), sweeps on the
  * coarsest level (1..256) and `fused` (1: a smoothing phase's sweeps run in one launch,
- * tile halos held; 0: one launch per sweep); defaults 1, 2, 12, 1. cfd_batch_autotune()
- * times a fixed list of candidate schedules over `steps` steps each from the batch's
+ * tile halos held; 0: one launch per sweep; 2: as 1, with each level's pre-smoothing done
+ * inside its residual + restriction launch on overlapping regions); defaults 1, 3, 12, 2.
+ * cfd_batch_autotune() times a fixed list of candidate schedules over `steps` steps each from the batch's
  * current state (restored before each candidate and on return, so the batch continues
  * exactly where it was), keeps the fastest and reports it as {pre, post, coarse, fused}
  * with its time per step. */
