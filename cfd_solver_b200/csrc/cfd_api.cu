@@ -49,6 +49,8 @@ namespace {
 
 long long rup(long long x, long long a) { return (x + a - 1) / a * a; }
 
+constexpr int NFLAGS = 10;  // device flag words of a batch
+
 enum KernelId {
     K_ASSEMBLE_P, K_RHS, K_SWEEP, K_UPBC, K_FACE_Q, K_BICG_P, K_SPMV, K_BICG_S, K_BICG_X,
     K_MG_SMOOTH, K_MG_RR, K_MG_POST, K_MG_COARSE, K_MG_GALERKIN,
@@ -164,12 +166,13 @@ struct cfd_batch {
     // device flags: [0] cases still in the pressure solve, [1] (case, field) pairs still in
     // the momentum solves, [2] / [3] this step's momentum-pair / pressure-iteration counts,
     // [4] kernel wait timeout, [5] / [6] cumulative pair / iteration counts (graph steps),
-    // [7] this step's momentum sweep launches
+    // [7] this step's momentum sweep launches, [8] cumulative count of pressure iterations
+    // whose second half ran (graph steps)
     int* flags = nullptr;
     bool use_graph = true;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-    int launches_per_pair = 2, launches_per_iter = 0, launches_fixed = 0;
-    int flags_total0[2] = {0, 0};
+    int launches_per_pair = 2, launches_per_iter = 0, launches_per_half = 0, launches_fixed = 0;
+    int flags_total0[3] = {0, 0, 0};
     unsigned long long* work = nullptr;  // k_jac traffic counters
     long long launches = 0;              // kernels launched since creation
     int* h_flags = nullptr;
@@ -255,7 +258,7 @@ int flush_profile(cfd_batch* b) {
 
 // reads the device flags (one copy); fails if a kernel's bounded wait gave up
 int read_flag(cfd_batch* b, int idx, int* out) {
-    CK(cudaMemcpyAsync(b->h_flags, b->flags, 8 * sizeof(int), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(b->h_flags, b->flags, NFLAGS * sizeof(int), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
     *out = b->h_flags[idx];
     if (b->h_flags[4]) return fail(CFD_E_CUDA, "a bounded wait inside a kernel timed out");
@@ -438,12 +441,12 @@ int run_vcycle(cfd_batch* b) {
         }
         if (bd.nmtiles[l] > 0 && fused == 2) {
             Prof pr(b, K_MG_PRR);
-            k_mg_prr<<<bd.natiles[l + 1], NT, kMgPrrSmem, b->st>>>(bd, l, pre, b->mg_pre);
+            k_mg_prr<<<bd.natiles[l + 1], MG_PRR_THREADS, 0, b->st>>>(bd, l, pre, b->mg_pre);
         } else if (bd.nmtiles[l] > 0) {
             for (int s = 0; s < npre; s++) {  // pre-smoothing from zero
                 Prof pr(b, K_MG_SMOOTH);
                 const int dst = (s & 1) ? M_R : M_X;
-                k_mg_gs<<<bd.nmtiles[l], NT, kMgGsSmem, b->st>>>(bd, l, s == 0 ? 0 : 1, dst == M_X ? M_R : M_X, dst,
+                k_mg_gs<<<bd.nmtiles[l], MG_GS_THREADS, 0, b->st>>>(bd, l, s == 0 ? 0 : 1, dst == M_X ? M_R : M_X, dst,
                                                                   inpre);
             }
             Prof pr(b, K_MG_RR);
@@ -456,7 +459,7 @@ int run_vcycle(cfd_batch* b) {
         for (int s = 0; s < npost; s++) {
             Prof pr(b, K_MG_POST);
             const int dst = src == M_X ? M_R : M_X;
-            k_mg_gs<<<bd.nmtiles[l], NT, kMgGsSmem, b->st>>>(bd, l, s == 0 ? 2 : 3, src, dst, inpost);
+            k_mg_gs<<<bd.nmtiles[l], MG_GS_THREADS, 0, b->st>>>(bd, l, s == 0 ? 2 : 3, src, dst, inpost);
             src = dst;
         }
     }
@@ -493,15 +496,24 @@ void enq_mid(cfd_batch* b, BatchDev& bd) {
     Prof pr(b, K_FACE_Q);
     k_face_q<<<bd.njtiles, NT, kFaceQSmem, b->st>>>(bd);
 }
-void enq_p_iter(cfd_batch* b, BatchDev& bd) {
+// one BiCGStab iteration in two halves: up to the half-step exit (k_bicg_s), and the rest,
+// which the step graph skips when every case stopped at the half step
+void enq_p_first(cfd_batch* b, BatchDev& bd) {
     const int nf = bd.njtiles;  // the BiCGStab kernels run on the 32 x 16 tiles
     { Prof pr(b, K_BICG_P); k_bicg_p<<<nf, NT, 0, b->st>>>(bd); }
     run_vcycle(b);
     { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 0); }
     { Prof pr(b, K_BICG_S); k_bicg_s<<<nf, NT, 0, b->st>>>(bd); }
+}
+void enq_p_second(cfd_batch* b, BatchDev& bd) {
+    const int nf = bd.njtiles;
     run_vcycle(b);
     { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 1); }
     { Prof pr(b, K_BICG_X); k_bicg_x<<<nf, NT, 0, b->st>>>(bd, b->maxit_p); }
+}
+void enq_p_iter(cfd_batch* b, BatchDev& bd) {
+    enq_p_first(b, bd);
+    enq_p_second(b, bd);
 }
 void enq_end(cfd_batch* b, BatchDev& bd) {
     { Prof pr(b, K_CORRECT); k_correct<<<bd.njtiles, NT, 0, b->st>>>(bd); }
@@ -584,6 +596,52 @@ int build_step_graph(cfd_batch* b, int cur) {
         prev = n;
         return CFD_OK;
     };
+    // the pressure loop: the iteration's first half, a condition kernel, an if-node holding
+    // the second half (run while some case is still iterating), the loop condition
+    long long lh0 = 0, lh1 = 0, lh2 = 0;
+    auto p_loop = [&]() -> int {
+        cudaGraphConditionalHandle h;
+        CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t n = nullptr;
+        CK(cudaGraphAddNode(&n, g, prev ? &prev : nullptr, prev ? 1 : 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        cudaGraphConditionalHandle hif;
+        CK(cudaGraphConditionalHandleCreate(&hif, body, 0, cudaGraphCondAssignDefault));
+        CK(cudaStreamBeginCaptureToGraph(b->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        lh0 = b->launches;
+        enq_p_first(b, bd);
+        lh1 = b->launches;
+        k_if_cond<<<1, 32, 0, b->st>>>(hif, b->flags + 0, b->flags + 8);
+        cudaStreamCaptureStatus cst;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        CK(cudaStreamGetCaptureInfo(b->st, &cst, nullptr, nullptr, &deps, &ndeps));
+        std::vector<cudaGraphNode_t> tail(deps, deps + ndeps);
+        cudaGraph_t out = nullptr;
+        CK(cudaStreamEndCapture(b->st, &out));
+        cudaGraphNodeParams ip = {};
+        ip.type = cudaGraphNodeTypeConditional;
+        ip.conditional.handle = hif;
+        ip.conditional.type = cudaGraphCondTypeIf;
+        ip.conditional.size = 1;
+        cudaGraphNode_t ifn = nullptr;
+        CK(cudaGraphAddNode(&ifn, body, tail.data(), tail.size(), &ip));
+        CK(cudaStreamBeginCaptureToGraph(b->st, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal));
+        enq_p_second(b, bd);
+        lh2 = b->launches;
+        CK(cudaStreamEndCapture(b->st, &out));
+        CK(cudaStreamBeginCaptureToGraph(b->st, body, &ifn, nullptr, 1, cudaStreamCaptureModeThreadLocal));
+        k_loop_cond<<<1, 32, 0, b->st>>>(h, b->flags + 0, b->flags + 3, b->maxit_p, b->flags + 6);
+        CK(cudaStreamEndCapture(b->st, &out));
+        prev = n;
+        return CFD_OK;
+    };
     int rc = child([&] { enq_begin(b, bd); });
     const long long la = b->launches;
     if (!rc) rc = loop([&] { enq_mom_pair(b, bd); }, b->flags + 1, b->flags + 2,
@@ -591,13 +649,15 @@ int build_step_graph(cfd_batch* b, int cur) {
     const long long lm = b->launches;
     if (!rc) rc = child([&] { enq_mid(b, bd); });
     const long long lp0 = b->launches;
-    if (!rc) rc = loop([&] { enq_p_iter(b, bd); }, b->flags + 0, b->flags + 3, b->maxit_p, b->flags + 6);
+    if (!rc) rc = p_loop();
     const long long lp1 = b->launches;
     if (!rc) rc = child([&] { enq_end(b, bd); });
     if (!rc) {
-        // kernels per straight segment, per loop iteration (+1: the condition kernel)
+        // kernels per straight segment, per loop iteration (+2: the two condition kernels),
+        // per executed second half
         b->launches_per_pair = (int)(lm - la) + 1;
-        b->launches_per_iter = (int)(lp1 - lp0) + 1;
+        b->launches_per_iter = (int)(lh1 - lh0) + 2;
+        b->launches_per_half = (int)(lh2 - lh1);
         b->launches_fixed = (int)((la - l0) + (lp0 - lm) + (b->launches - lp1));
         if (cudaGraphInstantiate(&b->gexec[cur], g, 0) != cudaSuccess) rc = fail(CFD_E_CUDA, "graph instantiation failed");
     }
@@ -640,11 +700,13 @@ int account_graph_launches(cfd_batch* b) {
     int dummy = 0;
     int rc = read_flag(b, 0, &dummy);
     if (rc) return rc;
-    const int tp = b->h_flags[5], ti = b->h_flags[6];
+    const int tp = b->h_flags[5], ti = b->h_flags[6], th = b->h_flags[8];
     b->launches += (long long)(tp - b->flags_total0[0]) * b->launches_per_pair +
-                   (long long)(ti - b->flags_total0[1]) * b->launches_per_iter;
+                   (long long)(ti - b->flags_total0[1]) * b->launches_per_iter +
+                   (long long)(th - b->flags_total0[2]) * b->launches_per_half;
     b->flags_total0[0] = tp;
     b->flags_total0[1] = ti;
+    b->flags_total0[2] = th;
     return CFD_OK;
 }
 
@@ -877,13 +939,13 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     ALLOC(b->partial, sizeof(double) * PSTRIDE *
                           std::max<size_t>(std::max(ftiles.size(), jtiles.size() * SW_WARPS), 1));
     ALLOC(b->counter, sizeof(unsigned) * ncases);
-    ALLOC(b->flags, sizeof(int) * 8);
+    ALLOC(b->flags, sizeof(int) * NFLAGS);
     ALLOC(b->work, sizeof(unsigned long long) * 4);
     ALLOC(b->dtmaps, (size_t)TMAP_STRIDE * ncases);
     ALLOC(b->dtiles, sizeof(Tile) * std::max<size_t>(ntl, 1));
     ALLOC(b->dcc, sizeof(int) * std::max<size_t>(ncc, 1));
 #undef ALLOC
-    if (cudaHostAlloc((void**)&b->h_flags, sizeof(int) * 8, cudaHostAllocDefault) != cudaSuccess)
+    if (cudaHostAlloc((void**)&b->h_flags, sizeof(int) * NFLAGS, cudaHostAllocDefault) != cudaSuccess)
         return cleanup(fail(CFD_E_CUDA, "pinned allocation failed"));
     cudaMemsetAsync(b->f64, 0, (size_t)b->n64 * sizeof(double), b->st);
     cudaMemsetAsync(b->f32, 0, (size_t)b->n32 * sizeof(float), b->st);
@@ -891,7 +953,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     cudaMemsetAsync(b->iscal, 0, sizeof(int) * NISCAL * ncases, b->st);
     cudaMemsetAsync(b->counter, 0, sizeof(unsigned) * ncases, b->st);
     cudaMemsetAsync(b->work, 0, sizeof(unsigned long long) * 4, b->st);
-    cudaMemsetAsync(b->flags, 0, sizeof(int) * 8, b->st);
+    cudaMemsetAsync(b->flags, 0, sizeof(int) * NFLAGS, b->st);
     CK(cudaStreamSynchronize(b->st));
     {
         const size_t smem = 2 * (size_t)(b->max_W + 1) * sizeof(double);
@@ -904,8 +966,6 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         b->sw_grid = (int)jtiles.size();  // one CTA per 32 x 16 tile
         CK(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem));
         CK(cudaFuncSetAttribute(k_face_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFaceQSmem));
-        CK(cudaFuncSetAttribute(k_mg_gs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgGsSmem));
-        CK(cudaFuncSetAttribute(k_mg_prr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMgPrrSmem));
     }
 
     // ---- tile tables

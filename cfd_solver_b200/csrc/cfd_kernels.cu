@@ -17,6 +17,8 @@
 //                    boundary pressure, wall integrals   PSolver.cpp:1901-1983
 //   k_diag           dilatation, vorticity, dmax         PSolver.cpp:1807-1853
 //   k_si             stream function (output only)       PSolver.cpp:1789-1801
+#include <type_traits>
+
 #include "cfd_common.cuh"
 #include "cfd_reduce.cuh"
 #include "cfd_kernels.cuh"
@@ -716,6 +718,14 @@ __global__ void __launch_bounds__(NT, 3) k_bicg_x(BatchDev b, int maxit) {
 // plane that another CTA of the same launch writes, so the V-cycle is a fixed linear map
 // (the same bits whatever the CTA schedule), as the Krylov method needs. The level's
 // final result lives in r (x for a case whose coarsest level it is).
+// stored column of level column gi, gi in [-W, inf): the periodic wrap without a division
+// in the common case (gi within one width of the level)
+__device__ __forceinline__ int mg_wrap(int gi, int W) {
+    int col = gi < 0 ? gi + W : gi;
+    if (col >= W) col = col >= 2 * W ? col % W : col - W;
+    return col;
+}
+
 __device__ __forceinline__ int mg_colour(int i, int j, int W, int periodic) {
     // 4 colours by parity; an odd periodic width gets 2 extra colours for its last column
     if (periodic && (W & 1) && i == W - 1) return 4 + (j & 1);
@@ -789,19 +799,26 @@ __global__ void __launch_bounds__(NT) k_mg_rr(BatchDev b, int l, int src) {
 // planes no CTA of the launch writes); it is a different map from form 1's, with the
 // level's pre-smoothing pass and its read of the stencil saved.
 constexpr int MPR_EW = 2 * TX + 3, MPR_EH = 2 * TY + 3;  // smoothed region E
-constexpr int MPR_XW = MPR_EW + 2, MPR_XH = MPR_EH + 2;  // E plus a zero ring
 constexpr int MPR_RW = 2 * TX + 1, MPR_RH = 2 * TY + 1;  // fine residual region
-constexpr int MPR_NE = MPR_EW * MPR_EH;
-constexpr size_t MPR_SMEM = (size_t)(10 * MPR_NE + MPR_XW * MPR_XH + MPR_RW * MPR_RH) * sizeof(float) + MPR_NE;
-const size_t kMgPrrSmem = MPR_SMEM;
+constexpr int MPR_BX = (MPR_EW + 1) / 2, MPR_BY = (MPR_EH + 1) / 2;  // 2 x 2 blocks of E: 34 x 10
+// x of E with a zero ring (69 x 21 points), split by column parity; a parity half has rows
+// of 40 words, and the second half starts 16 banks after the first
+constexpr int MPR_XW = MPR_EW + 2, MPR_XH = MPR_EH + 2;
+constexpr int MPR_XS = 40, MPR_XP = MPR_XH * MPR_XS + 8;
+static_assert(MPR_XS >= (MPR_XW + 1) / 2 && MPR_XP % 32 == 16, "split layout of the region's x");
+static_assert(MG_PRR_THREADS >= MPR_BX * MPR_BY && MG_PRR_THREADS >= TX * TY && MG_PRR_THREADS % 32 == 0,
+              "one thread per 2 x 2 block of E, one per coarse point");
 
-__global__ void __launch_bounds__(NT) k_mg_prr(BatchDev b, int l, int dst, int inner) {
-    extern __shared__ __align__(16) unsigned char mpraw[];
-    // cf: ap, ae, aw, an, as, ane, anw, ase, asw, b of every point of E
-    float(*cf)[MPR_NE] = reinterpret_cast<float(*)[MPR_NE]>(mpraw);
-    float* xs = reinterpret_cast<float*>(mpraw) + 10 * MPR_NE;
-    float* rs = xs + MPR_XW * MPR_XH;
-    signed char* unk = reinterpret_cast<signed char*>(rs + MPR_RW * MPR_RH);  // 1: an unknown
+__device__ __forceinline__ int mpr_at(int xx, int ry) {  // point (xx, ry) of the ringed region
+    return (xx & 1) * MPR_XP + ry * MPR_XS + (xx >> 1);
+}
+
+// Each thread owns one 2 x 2 block of E, which holds one point of each colour (E starts at
+// an even column and row, and a level with a coarser one has an even width when periodic,
+// so the colours are the four parity classes); its four stencils stay in registers.
+__global__ void __launch_bounds__(MG_PRR_THREADS) k_mg_prr(BatchDev b, int l, int dst, int inner) {
+    __shared__ float xs[2 * MPR_XP];
+    __shared__ float rs[MPR_RW * MPR_RH];
     const Tile t = b.atiles[l + 1][blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
@@ -809,80 +826,94 @@ __global__ void __launch_bounds__(NT) k_mg_prr(BatchDev b, int l, int dst, int i
     const LevelDev& C = c.lev[l + 1];
     const int tid = threadIdx.x;
     const int fl = F.ld, W = F.W, per = c.periodic, n1 = F.n1;
-    // a level with a coarser one has an even width when periodic, so its colours are the
-    // four parity classes, and E (whose origin is even in both directions) holds colour
-    // (x & 1) | ((y & 1) << 1) at its point (x, y)
     if (per && (W & 1)) {
         if (tid == 0) atomicExch(b.error, 1);
         return;
     }
     const int ei0 = 2 * t.i0 - 2, ej0 = 2 * t.j0 - 2;  // level-l (column, row) of E's first point
-    for (int e = tid; e < MPR_XW * MPR_XH; e += NT) xs[e] = 0.0f;
-    // every load of the stencil of E issued before the first shared-memory store
-    constexpr int NLD = (MPR_NE + NT - 1) / NT;
-    float v[NLD][10];
-    bool ok[NLD];
-#pragma unroll
-    for (int m = 0; m < NLD; m++) {
-        const int e = tid + m * NT;
-        const int gj = ej0 + e / MPR_EW, gi = ei0 + e % MPR_EW;
-        const int col = per ? ((gi % W) + W) % W : gi;
-        ok[m] = e < MPR_NE && gj >= 1 && gj <= n1 - 2 && col >= F.ilo && col <= F.ihi;
-        const long long k = ok[m] ? (long long)gj * fl + col : (long long)fl + F.ilo;
-#pragma unroll
-        for (int q = 0; q < 9; q++) v[m][q] = mplane(b, F, M_AP + q)[k];
-        v[m][9] = mplane(b, F, M_B)[k];
+    const bool own = tid < MPR_BX * MPR_BY;
+    const int bx = own ? tid % MPR_BX : 0, by = own ? tid / MPR_BX : 0;
+    const int gi0 = ei0 + 2 * bx;
+    int c0, c1;  // stored columns of the block's two columns (c1 = c0 + 1 when both exist)
+    if (per) {
+        c0 = mg_wrap(gi0, W);
+        c1 = c0 + 1;
+    } else {
+        c0 = (gi0 >= 0 && gi0 < W) ? gi0 : -1;
+        c1 = (gi0 + 1 >= 0 && gi0 + 1 < W) ? gi0 + 1 : -1;
     }
+    float a[2][2][10];  // [dy][dx][ap, ae, aw, an, as, ane, anw, ase, asw, b]
+    bool ok[2][2];
 #pragma unroll
-    for (int m = 0; m < NLD; m++) {
-        const int e = tid + m * NT;
-        if (e >= MPR_NE) continue;
+    for (int dy = 0; dy < 2; dy++) {
+        const int gj = ej0 + 2 * by + dy;
+        const bool rowok = own && gj >= 1 && gj <= n1 - 2 && 2 * by + dy < MPR_EH;
+        ok[dy][0] = rowok && c0 >= F.ilo && c0 <= F.ihi;
+        ok[dy][1] = rowok && c1 >= F.ilo && c1 <= F.ihi && 2 * bx + 1 < MPR_EW;
+        // the even column and its right neighbour, 8-byte aligned (safe row / column outside)
+        const long long k = (long long)((gj >= 0 && gj < n1) ? gj : 1) * fl + (c0 >= 0 ? c0 : 0);
 #pragma unroll
-        for (int q = 0; q < 10; q++) cf[q][e] = ok[m] ? v[m][q] : 0.0f;
-        unk[e] = ok[m] ? 1 : 0;
+        for (int q = 0; q < 10; q++) {
+            const float2 v = *reinterpret_cast<const float2*>(mplane(b, F, q < 9 ? M_AP + q : M_B) + k);
+            a[dy][0][q] = v.x;
+            a[dy][1][q] = v.y;
+        }
     }
+    for (int e = tid; e < 2 * MPR_XP; e += MG_PRR_THREADS) xs[e] = 0.0f;
     __syncthreads();
-    // multicolour Gauss-Seidel, each colour's points enumerated directly
-    for (int n = 0; n < 4 * inner; n++) {
-        const int cc = n & 3, px = cc & 1, py = cc >> 1;
-        const int nx = (MPR_EW - px + 1) >> 1, ny = (MPR_EH - py + 1) >> 1;
-        for (int s2 = tid; s2 < nx * ny; s2 += NT) {
-            const int x = px + 2 * (s2 % nx), y = py + 2 * (s2 / nx);
-            const int e = y * MPR_EW + x;
-            if (!unk[e]) continue;
-            const int o = (y + 1) * MPR_XW + (x + 1);
-            const float sm = cf[1][e] * xs[o + 1] + cf[2][e] * xs[o - 1] + cf[3][e] * xs[o + MPR_XW] +
-                             cf[4][e] * xs[o - MPR_XW] + cf[5][e] * xs[o + MPR_XW + 1] +
-                             cf[6][e] * xs[o + MPR_XW - 1] + cf[7][e] * xs[o - MPR_XW + 1] +
-                             cf[8][e] * xs[o - MPR_XW - 1];
-            xs[o] = (cf[9][e] - sm) / cf[0][e];
+    // point of colour cc in the block: (dx, dy) = (cc & 1, cc >> 1); its ringed position is
+    // (2 bx + dx + 1, 2 by + dy + 1)
+    float xr[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
+    auto relax = [&](auto cc_) {
+        constexpr int cc = decltype(cc_)::value;
+        constexpr int dx = cc & 1, dy = cc >> 1;
+        if (ok[dy][dx]) {
+            const float(&f)[10] = a[dy][dx];
+            const int xx = 2 * bx + dx + 1, ry = 2 * by + dy + 1;
+            const float sm = f[1] * xs[mpr_at(xx + 1, ry)] + f[2] * xs[mpr_at(xx - 1, ry)] +
+                             f[3] * xs[mpr_at(xx, ry + 1)] + f[4] * xs[mpr_at(xx, ry - 1)] +
+                             f[5] * xs[mpr_at(xx + 1, ry + 1)] + f[6] * xs[mpr_at(xx - 1, ry + 1)] +
+                             f[7] * xs[mpr_at(xx + 1, ry - 1)] + f[8] * xs[mpr_at(xx - 1, ry - 1)];
+            const float v = (f[9] - sm) / f[0];
+            xs[mpr_at(xx, ry)] = v;
+            xr[dy][dx] = v;
         }
         __syncthreads();
+    };
+    using C0 = std::integral_constant<int, 0>;
+    using C1 = std::integral_constant<int, 1>;
+    using C2 = std::integral_constant<int, 2>;
+    using C3 = std::integral_constant<int, 3>;
+    for (int n = 0; n < inner; n++) {
+        relax(C0{}); relax(C1{}); relax(C2{}); relax(C3{});
     }
-    // residual on the restriction's fine points (E without its ring)
-    for (int e = tid; e < MPR_RW * MPR_RH; e += NT) {
-        const int rj = e / MPR_RW, ri = e % MPR_RW;
-        const int q = (rj + 1) * MPR_EW + (ri + 1);
-        float r = 0.0f;
-        if (unk[q]) {
-            const int o = (rj + 2) * MPR_XW + (ri + 2);
-            const float ax = cf[0][q] * xs[o] + cf[1][q] * xs[o + 1] + cf[2][q] * xs[o - 1] +
-                             cf[3][q] * xs[o + MPR_XW] + cf[4][q] * xs[o - MPR_XW] + cf[5][q] * xs[o + MPR_XW + 1] +
-                             cf[6][q] * xs[o + MPR_XW - 1] + cf[7][q] * xs[o - MPR_XW + 1] +
-                             cf[8][q] * xs[o - MPR_XW - 1];
-            r = cf[9][q] - ax;
-        }
-        rs[e] = r;
-    }
-    // smoothed x of the owned fine points
+    // residual on the restriction's fine points (E without its ring), x of the owned points
     float* OUT = mplane(b, F, dst);
     const int jhi = (t.j0 + TY > C.n1 - 2) ? n1 - 2 : min(2 * t.j0 + 14, n1 - 2);
-    for (int e = tid; e < 2 * TX * (2 * TY + 1); e += NT) {
-        const int gi = 2 * t.i0 + e % (2 * TX), gj = 2 * t.j0 - 1 + e / (2 * TX);
-        if (gi < F.ilo || gi > F.ihi || gj > jhi) continue;
-        store_mirrored(OUT, fl, gi, gj, W, per, xs[(gj - ej0 + 1) * MPR_XW + (gi - ei0 + 1)]);
-    }
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+        for (int dx = 0; dx < 2; dx++) {
+            const int x = 2 * bx + dx, y = 2 * by + dy;
+            if (!own || x < 1 || x > MPR_RW || y < 1 || y > MPR_RH) continue;
+            float r = 0.0f;
+            if (ok[dy][dx]) {
+                const float(&f)[10] = a[dy][dx];
+                const int xx = x + 1, ry = y + 1;
+                const float ax = f[0] * xr[dy][dx] + f[1] * xs[mpr_at(xx + 1, ry)] + f[2] * xs[mpr_at(xx - 1, ry)] +
+                                 f[3] * xs[mpr_at(xx, ry + 1)] + f[4] * xs[mpr_at(xx, ry - 1)] +
+                                 f[5] * xs[mpr_at(xx + 1, ry + 1)] + f[6] * xs[mpr_at(xx - 1, ry + 1)] +
+                                 f[7] * xs[mpr_at(xx + 1, ry - 1)] + f[8] * xs[mpr_at(xx - 1, ry - 1)];
+                r = f[9] - ax;
+            }
+            rs[(y - 1) * MPR_RW + (x - 1)] = r;
+            // owned: columns 2 i0 .. 2 i0 + 63 (E columns 2 .. 65), rows 2 j0 - 1 .. jhi
+            const int gi = ei0 + x, gj = ej0 + y;
+            if (x >= 2 && gi >= F.ilo && gi <= F.ihi && gj <= jhi)
+                store_mirrored(OUT, fl, gi, gj, W, per, ok[dy][dx] ? xr[dy][dx] : 0.0f);
+        }
     __syncthreads();
+    if (tid >= TX * TY) return;
     const int li = tid % TX, lj = tid / TX;
     const int I = t.i0 + li, J = t.j0 + lj;
     if (I < C.ilo || I > C.ihi || J > C.n1 - 2) return;
@@ -903,115 +934,135 @@ __device__ __forceinline__ float mg_prolong_at(const float* XC, int cl, int i, i
     return 0.25f * (XC[q] + XC[q + 1] + XC[q + cl] + XC[q + cl + 1]);
 }
 
-// One multicolour Gauss-Seidel sweep of level l on a 32 x 16 tile (block Gauss-Seidel at
-// tile edges: the halo ring holds the neighbouring tiles' values from before the sweep,
-// plus a redundantly relaxed overlap of MGS_OV cells). The sweep reads plane `src` and
-// writes plane `dst` != src, so nothing is read that another CTA writes.
+// Multicolour Gauss-Seidel sweeps of level l on a 32 x 16 tile (block Gauss-Seidel at tile
+// edges: the halo ring holds the neighbouring tiles' values from before the first sweep).
+// The sweeps read plane `src` and write plane `dst` != src, so nothing is read that another
+// CTA writes.
 //   mode 0: from x = 0, colours in order (first pre-sweep; src unused)
 //   mode 1: from src, colours in order (further pre-sweeps)
 //   mode 2: from src plus the prolonged result of level l + 1, colours reversed (first
 //           post-sweep)
 //   mode 3: from src, colours reversed (further post-sweeps)
-// `inner` sweeps run back to back in shared memory, the halo kept from before the first
-// (one launch and one read of the stencil for several sweeps, at the price of weaker
-// coupling between tiles).
-constexpr int MGS_OV = 0;                          // overlap relaxed redundantly around the tile
-constexpr int MGS_OVM = MGS_OV;
-constexpr int MGS_RW = TX + 2 * MGS_OVM, MGS_RH = TYJ + 2 * MGS_OVM;
-constexpr int MGS_XW = MGS_RW + 2, MGS_XH = MGS_RH + 2;
-constexpr size_t MGS_SMEM = (size_t)(MGS_XH * MGS_XW + 10 * MGS_RW * MGS_RH) * sizeof(float) + MGS_RW * MGS_RH;
-const size_t kMgGsSmem = MGS_SMEM;
-__global__ void __launch_bounds__(NT) k_mg_gs(BatchDev b, int l, int mode, int src, int dst, int inner) {
-    extern __shared__ __align__(16) unsigned char mgraw[];
-    float* xs = reinterpret_cast<float*>(mgraw);
-    float(*cf)[MGS_RW * MGS_RH] = reinterpret_cast<float(*)[MGS_RW * MGS_RH]>(xs + MGS_XH * MGS_XW);
-    // cf: ap, ae, aw, an, as, ane, anw, ase, asw, b of every relaxed point
-    signed char* unk = reinterpret_cast<signed char*>(xs + MGS_XH * MGS_XW + 10 * MGS_RW * MGS_RH);
+// `inner` sweeps run back to back in shared memory (one launch and one read of the stencil
+// for several sweeps, at the price of weaker coupling between tiles).
+//
+// A level with a coarser one has an even width when periodic, so its colours are the four
+// parity classes. Tiles start at an even column and an odd row, so every 2 x 2 block of the
+// tile holds one point of each colour: a thread owns one block (16 x 8 blocks, 128
+// threads), keeps its four stencils in registers (loaded as column pairs) and relaxes one
+// point per colour. x with its halo is held in shared memory split by column parity, rows
+// padded so that a warp's two block rows fall in different banks: every read of a
+// colour pass is free of bank conflicts.
+constexpr int MG_GS_XW = TX + 2, MG_GS_XH = TYJ + 2;  // x halo region
+constexpr int MG_GS_XS = 24;                           // row stride of a parity half
+constexpr int MG_GS_XP = MG_GS_XH * MG_GS_XS;          // 432 = 16 mod 32 words
+static_assert(MG_GS_XS >= (MG_GS_XW + 1) / 2 && (2 * MG_GS_XS) % 32 == 16 && MG_GS_XP % 32 == 16,
+              "parity halves must keep a colour pass free of bank conflicts");
+static_assert(MG_GS_THREADS == (TX / 2) * (TYJ / 2), "one thread per 2 x 2 block");
+
+__device__ __forceinline__ int mg_gs_at(int xx, int ry) {  // halo point (xx, ry) in the split layout
+    return (xx & 1) * MG_GS_XP + ry * MG_GS_XS + (xx >> 1);
+}
+
+__global__ void __launch_bounds__(MG_GS_THREADS) k_mg_gs(BatchDev b, int l, int mode, int src, int dst, int inner) {
+    __shared__ float xs[2 * MG_GS_XP];
     const Tile t = b.mtiles[l][blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
     const LevelDev& L = c.lev[l];
     const int tid = threadIdx.x;
     const int ld = L.ld, W = L.W, per = c.periodic, n1 = L.n1;
-    // a level with a coarser one has an even width when periodic: the colours are the four
-    // parity classes, and with the tile origin (even column, odd row) the point (x, y) of
-    // the tile has colour (x & 1) | ((~y & 1) << 1)
     if (per && (W & 1)) {
         if (tid == 0) atomicExch(b.error, 1);
         return;
     }
-    constexpr int ov = MGS_OV, rw = MGS_RW, rh = MGS_RH, xw = MGS_XW, xh = MGS_XH;
-    static_assert(MGS_OV == 0, "the colour lattice below assumes no overlap");
     const bool zero = mode == 0, prolong = mode == 2, reverse = mode >= 2;
     const float* X = mplane(b, L, src);
     const float* XC = prolong ? mplane(b, c.lev[l + 1], mg_result_plane(b, c, l + 1)) : nullptr;
     const int cl = prolong ? c.lev[l + 1].ld : 0;
-    // stored column of global column gi (periodic wrap), or -1 outside the level
+    // stored column of level column gi (periodic wrap), or -1 outside the level
     auto column = [&](int gi) -> int {
-        if (per) return ((gi % W) + W) % W;
+        if (per) return mg_wrap(gi, W);
         return (gi >= 0 && gi < W) ? gi : -1;
     };
-    // every global load issued before the first shared-memory store
-    constexpr int NXL = (xh * xw + NT - 1) / NT, NPL = (rw * rh + NT - 1) / NT;
+    // this thread's 2 x 2 block: tile columns 2 bx, 2 bx + 1, rows 2 by, 2 by + 1
+    const int bx = tid % (TX / 2), by = tid / (TX / 2);
+    const int gi0 = t.i0 + 2 * bx;
+    const int c0 = column(gi0), c1 = column(gi0 + 1);  // c1 = c0 + 1 whenever both are in the level
+    float a[2][2][10];  // [dy][dx][ap^-1, ae, aw, an, as, ane, anw, ase, asw, b]
+    bool ok[2][2];
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++) {
+        const int gj = t.j0 + 2 * by + dy;
+        ok[dy][0] = gj >= 1 && gj <= n1 - 2 && c0 >= L.ilo && c0 <= L.ihi;
+        ok[dy][1] = gj >= 1 && gj <= n1 - 2 && c1 >= L.ilo && c1 <= L.ihi;
+        // an even column and its right neighbour, 8-byte aligned (safe row / column when outside)
+        const long long k = (long long)((gj >= 0 && gj < n1) ? gj : 1) * ld + (c0 >= 0 ? c0 : 0);
+#pragma unroll
+        for (int q = 0; q < 10; q++) {
+            const float2 v = *reinterpret_cast<const float2*>(mplane(b, L, q < 9 ? M_AP + q : M_B) + k);
+            a[dy][0][q] = v.x;
+            a[dy][1][q] = v.y;
+        }
+    }
+    // x and its halo (with the prolonged coarse correction in mode 2)
+    constexpr int NXL = (MG_GS_XW * MG_GS_XH + MG_GS_THREADS - 1) / MG_GS_THREADS;
     float xv[NXL];
 #pragma unroll
     for (int m = 0; m < NXL; m++) {
-        const int e = tid + m * NT;
-        const int gj = t.j0 - ov - 1 + e / xw, col = column(t.i0 - ov - 1 + e % xw);
+        const int e = tid + m * MG_GS_THREADS;
+        const int gj = t.j0 - 1 + e / MG_GS_XW, col = column(t.i0 - 1 + e % MG_GS_XW);
         float v = 0.0f;
-        if (!zero && e < xh * xw && gj >= 0 && gj < n1 && col >= 0) {
+        if (!zero && e < MG_GS_XW * MG_GS_XH && gj >= 0 && gj < n1 && col >= 0) {
             v = X[(long long)gj * ld + col];
             if (prolong && gj >= 1 && gj <= n1 - 2 && col >= L.ilo && col <= L.ihi)
                 v += mg_prolong_at(XC, cl, col, gj);
         }
         xv[m] = v;
     }
-    float cv[NPL][10];
-    bool ok[NPL];
 #pragma unroll
-    for (int m = 0; m < NPL; m++) {
-        const int e = tid + m * NT;
-        const int gj = t.j0 - ov + e / rw, col = column(t.i0 - ov + e % rw);
-        ok[m] = e < rw * rh && gj >= 1 && gj <= n1 - 2 && col >= L.ilo && col <= L.ihi;
-        const long long k = ok[m] ? (long long)gj * ld + col : (long long)ld + L.ilo;
-#pragma unroll
-        for (int q = 0; q < 9; q++) cv[m][q] = mplane(b, L, M_AP + q)[k];
-        cv[m][9] = mplane(b, L, M_B)[k];
+    for (int m = 0; m < NXL; m++) {
+        const int e = tid + m * MG_GS_THREADS;
+        if (e < MG_GS_XW * MG_GS_XH) xs[mg_gs_at(e % MG_GS_XW, e / MG_GS_XW)] = xv[m];
     }
 #pragma unroll
-    for (int m = 0; m < NXL; m++)
-        if (tid + m * NT < xh * xw) xs[tid + m * NT] = xv[m];
+    for (int dy = 0; dy < 2; dy++)
 #pragma unroll
-    for (int m = 0; m < NPL; m++) {
-        const int e = tid + m * NT;
-        if (e >= rw * rh) continue;
-#pragma unroll
-        for (int q = 0; q < 10; q++) cf[q][e] = ok[m] ? cv[m][q] : 0.0f;
-        unk[e] = ok[m] ? 1 : 0;
-    }
+        for (int dx = 0; dx < 2; dx++) a[dy][dx][0] = ok[dy][dx] ? 1.0f / a[dy][dx][0] : 0.0f;
     __syncthreads();
-    for (int n = 0; n < 4 * inner; n++) {
-        const int cc = reverse ? 3 - (n & 3) : (n & 3);
-        const int px = cc & 1, py = ((cc >> 1) & 1) ^ 1;  // row parity of the colour within the tile
-        const int nx = (rw - px + 1) >> 1, ny = (rh - py + 1) >> 1;
-        for (int s2 = tid; s2 < nx * ny; s2 += NT) {
-            const int x = px + 2 * (s2 % nx), y = py + 2 * (s2 / nx);
-            const int e = y * rw + x;
-            if (!unk[e]) continue;
-            const int o = (y + 1) * xw + (x + 1);
-            const float sm = cf[1][e] * xs[o + 1] + cf[2][e] * xs[o - 1] + cf[3][e] * xs[o + xw] +
-                             cf[4][e] * xs[o - xw] + cf[5][e] * xs[o + xw + 1] + cf[6][e] * xs[o + xw - 1] +
-                             cf[7][e] * xs[o - xw + 1] + cf[8][e] * xs[o - xw - 1];
-            xs[o] = (cf[9][e] - sm) / cf[0][e];
+    // point of colour cc in this thread's block: (dx, dy) = (cc & 1, 1 - (cc >> 1)) (the tile's
+    // first row is odd); its halo position is (2 bx + dx + 1, 2 by + dy + 1)
+    auto relax = [&](auto cc_) {
+        constexpr int cc = decltype(cc_)::value;
+        constexpr int dx = cc & 1, dy = 1 - (cc >> 1);
+        if (ok[dy][dx]) {
+            const float(&f)[10] = a[dy][dx];
+            const int xx = 2 * bx + dx + 1, ry = 2 * by + dy + 1;
+            const float sm = f[1] * xs[mg_gs_at(xx + 1, ry)] + f[2] * xs[mg_gs_at(xx - 1, ry)] +
+                             f[3] * xs[mg_gs_at(xx, ry + 1)] + f[4] * xs[mg_gs_at(xx, ry - 1)] +
+                             f[5] * xs[mg_gs_at(xx + 1, ry + 1)] + f[6] * xs[mg_gs_at(xx - 1, ry + 1)] +
+                             f[7] * xs[mg_gs_at(xx + 1, ry - 1)] + f[8] * xs[mg_gs_at(xx - 1, ry - 1)];
+            xs[mg_gs_at(xx, ry)] = (f[9] - sm) * f[0];
         }
         __syncthreads();
+    };
+    using C0 = std::integral_constant<int, 0>;
+    using C1 = std::integral_constant<int, 1>;
+    using C2 = std::integral_constant<int, 2>;
+    using C3 = std::integral_constant<int, 3>;
+    for (int n = 0; n < inner; n++) {
+        if (reverse) { relax(C3{}); relax(C2{}); relax(C1{}); relax(C0{}); }
+        else { relax(C0{}); relax(C1{}); relax(C2{}); relax(C3{}); }
     }
     float* OUT = mplane(b, L, dst);
-    for (int e = tid; e < TX * TYJ; e += NT) {
-        const int i = t.i0 + e % TX, j = t.j0 + e / TX;
-        if (i < L.ilo || i > L.ihi || j > n1 - 2) continue;
-        store_mirrored(OUT, ld, i, j, W, per, xs[(e / TX + ov + 1) * xw + (e % TX + ov + 1)]);
-    }
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+        for (int dx = 0; dx < 2; dx++) {
+            const int i = gi0 + dx, j = t.j0 + 2 * by + dy;
+            if (i < L.ilo || i > L.ihi || j > n1 - 2) continue;
+            store_mirrored(OUT, ld, i, j, W, per, xs[mg_gs_at(2 * bx + dx + 1, 2 * by + dy + 1)]);
+        }
 }
 
 // coarsest level: `sweeps` multicolour GS sweeps by one CTA per case, x in shared memory
@@ -1561,6 +1612,15 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, const int* flag, int* 
         const int n = ++(*counter);
         atomicAdd(total, 1);
         cudaGraphSetConditional(h, (*flag > 0 && n < maxc) ? 1u : 0u);
+    }
+}
+
+// condition of a graph if-node: run the body when `*flag > 0`; `total` counts the runs
+__global__ void k_if_cond(cudaGraphConditionalHandle h, const int* flag, int* total) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const bool go = *flag > 0;
+        if (go) atomicAdd(total, 1);
+        cudaGraphSetConditional(h, go ? 1u : 0u);
     }
 }
 

@@ -14,10 +14,10 @@ __global__ void k_spmv(BatchDev b, int mode);
 __global__ void k_bicg_s(BatchDev b);
 __global__ void k_bicg_x(BatchDev b, int maxit);
 __global__ void k_mg_gs(BatchDev b, int l, int mode, int src, int dst, int inner);
-extern const size_t kMgGsSmem;  // dynamic shared memory of k_mg_gs
+constexpr int MG_GS_THREADS = 128;  // k_mg_gs: one thread per 2 x 2 block of a 32 x 16 tile
 __global__ void k_mg_rr(BatchDev b, int l, int src);
 __global__ void k_mg_prr(BatchDev b, int l, int dst, int inner);
-extern const size_t kMgPrrSmem;  // dynamic shared memory of k_mg_prr
+constexpr int MG_PRR_THREADS = 352;  // k_mg_prr: one thread per 2 x 2 block of its 67 x 19 region
 __global__ void k_mg_coarse(BatchDev b, int l, int sweeps);
 __global__ void k_mg_galerkin(BatchDev b, int l, int toff);
 __global__ void k_correct(BatchDev b);
@@ -26,4 +26,5 @@ __global__ void k_diag(BatchDev b);
 __global__ void k_si(BatchDev b);
 __global__ void k_state_pack(BatchDev b, double* stage, const long long* off, int to_stage);
 __global__ void k_loop_cond(cudaGraphConditionalHandle h, const int* flag, int* counter, int maxc, int* total);
+__global__ void k_if_cond(cudaGraphConditionalHandle h, const int* flag, int* total);
 }  // namespace cfd
