@@ -405,7 +405,7 @@ constexpr int FQ_HALO = 7;
 constexpr size_t FQ_SMEM = (size_t)FQ_HALO * JTW * JTH * sizeof(double) + 128;
 const size_t kFaceQSmem = FQ_SMEM;
 
-__global__ void __launch_bounds__(NT, 3) k_face_q(BatchDev b) {
+__global__ void __launch_bounds__(NT, 4) k_face_q(BatchDev b) {
     extern __shared__ __align__(128) unsigned char fraw[];
     __shared__ __align__(8) uint64_t bar;
     double* sm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(fraw) + 127) & ~uintptr_t(127));
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(NT, 3) k_bicg_p(BatchDev b) {
 
 // y = A * x with x = (double) MG level-0 result; mode 0: p_hat, v, (r_hat, v) -> alpha
 //                                               mode 1: s_hat, t, (t, s), (t, t) -> omega
-__global__ void __launch_bounds__(NT, 3) k_spmv(BatchDev b, int mode) {
+__global__ void __launch_bounds__(NT, 5) k_spmv(BatchDev b, int mode) {
     const Tile t = b.jtiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(NT, 3) k_spmv(BatchDev b, int mode) {
 // s = r - alpha v, and the half step x += alpha p_hat; when |s| already meets the stop rule
 // the solve ends here (the standard early exit: x + alpha p_hat is the iterate whose
 // residual is s) and the second preconditioner application of the iteration is skipped
-__global__ void __launch_bounds__(NT, 3) k_bicg_s(BatchDev b) {
+__global__ void __launch_bounds__(NT, 5) k_bicg_s(BatchDev b) {
     const Tile t = b.jtiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const bool first = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
@@ -650,7 +650,7 @@ __global__ void __launch_bounds__(NT, 3) k_bicg_s(BatchDev b) {
     }
 }
 
-__global__ void __launch_bounds__(NT, 3) k_bicg_x(BatchDev b, int maxit) {
+__global__ void __launch_bounds__(NT, 5) k_bicg_x(BatchDev b, int maxit) {
     const Tile t = b.jtiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
@@ -1201,7 +1201,7 @@ __global__ void __launch_bounds__(NT) k_mg_galerkin(BatchDev b, int l, int toff)
 // ---------------------------------------------------------------------------
 // pcor boundary conditions + velocity / pressure correction (PSolver.cpp:1471-1542);
 // also the momentum part of the steady residual, sum |u^{n+1} - u^n| + |v^{n+1} - v^n|
-__global__ void __launch_bounds__(NT, 3) k_correct(BatchDev b) {
+__global__ void __launch_bounds__(NT, 4) k_correct(BatchDev b) {
     // a 32 x 16 tile, two cells per thread (rows lj and lj + 8): every load of both cells
     // is issued before any arithmetic
     const Tile t = b.jtiles[blockIdx.x];
