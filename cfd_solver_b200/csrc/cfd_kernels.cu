@@ -816,7 +816,7 @@ __device__ __forceinline__ int mpr_at(int xx, int ry) {  // point (xx, ry) of th
 // Each thread owns one 2 x 2 block of E, which holds one point of each colour (E starts at
 // an even column and row, and a level with a coarser one has an even width when periodic,
 // so the colours are the four parity classes); its four stencils stay in registers.
-__global__ void __launch_bounds__(MG_PRR_THREADS) k_mg_prr(BatchDev b, int l, int dst, int inner) {
+__global__ void __launch_bounds__(MG_PRR_THREADS, 3) k_mg_prr(BatchDev b, int l, int dst, int inner) {
     __shared__ float xs[2 * MPR_XP];
     __shared__ float rs[MPR_RW * MPR_RH];
     const Tile t = b.atiles[l + 1][blockIdx.x];
@@ -964,7 +964,7 @@ __device__ __forceinline__ int mg_gs_at(int xx, int ry) {  // halo point (xx, ry
     return (xx & 1) * MG_GS_XP + ry * MG_GS_XS + (xx >> 1);
 }
 
-__global__ void __launch_bounds__(MG_GS_THREADS) k_mg_gs(BatchDev b, int l, int mode, int src, int dst, int inner) {
+__global__ void __launch_bounds__(MG_GS_THREADS, 8) k_mg_gs(BatchDev b, int l, int mode, int src, int dst, int inner) {
     __shared__ float xs[2 * MG_GS_XP];
     const Tile t = b.mtiles[l][blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
