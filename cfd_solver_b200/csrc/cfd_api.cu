@@ -434,11 +434,10 @@ int run_vcycle(cfd_batch* b) {
     const int pre = mg_pre_plane(b->mg_pre, fused);
     const int npre = fused ? 1 : b->mg_pre, inpre = fused ? b->mg_pre : 1;
     const int npost = fused ? 1 : b->mg_post, inpost = fused ? b->mg_post : 1;
+    // down: pre-smoothing, residual and restriction level by level; then one launch solves
+    // every case on its own coarsest level (a case's coarse solve needs only its own
+    // restriction, done by then, and is read first by the post-smoothing of the level above)
     for (int l = 0; l < b->nlev_max; l++) {
-        if (bd.nccases[l] > 0) {
-            Prof pr(b, K_MG_COARSE);
-            k_mg_coarse<<<bd.nccases[l], 1024, 0, b->st>>>(bd, l, b->coarse_sweeps);
-        }
         if (bd.nmtiles[l] > 0 && fused == 2) {
             Prof pr(b, K_MG_PRR);
             k_mg_prr<<<bd.natiles[l + 1], MG_PRR_THREADS, 0, b->st>>>(bd, l, pre, b->mg_pre);
@@ -452,6 +451,10 @@ int run_vcycle(cfd_batch* b) {
             Prof pr(b, K_MG_RR);
             k_mg_rr<<<bd.natiles[l + 1], NT, 0, b->st>>>(bd, l, pre);
         }
+    }
+    {
+        Prof pr(b, K_MG_COARSE);
+        k_mg_coarse<<<b->n, 1024, 0, b->st>>>(bd, -1, b->coarse_sweeps);
     }
     for (int l = b->nlev_max - 2; l >= 0; l--) {
         if (bd.nmtiles[l] == 0) continue;

@@ -1071,10 +1071,12 @@ __global__ void __launch_bounds__(MG_GS_THREADS, 8) k_mg_gs(BatchDev b, int l, i
 constexpr int MGC_THREADS = 1024, MGC_SMEM = 4096;
 __global__ void __launch_bounds__(MGC_THREADS) k_mg_coarse(BatchDev b, int l, int sweeps) {
     __shared__ float xs[MGC_SMEM];
-    const int cid = b.ccases[l][blockIdx.x];
+    // l < 0: one launch for every case, each on its own coarsest level (the case lists of
+    // all levels are stored back to back from ccases[0])
+    const int cid = l >= 0 ? b.ccases[l][blockIdx.x] : b.ccases[0][blockIdx.x];
     if (b.iscal[(long long)cid * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[cid];
-    const LevelDev& L = c.lev[l];
+    const LevelDev& L = c.lev[l >= 0 ? l : c.nlev - 1];
     const int ld = L.ld, per = c.periodic;
     const int nx = L.ihi - L.ilo + 1, ny = L.n1 - 2;
     float* X = mplane(b, L, M_X);
