@@ -54,12 +54,12 @@ constexpr int NFLAGS = 10;  // device flag words of a batch
 enum KernelId {
     K_ASSEMBLE_P, K_RHS, K_SWEEP, K_UPBC, K_FACE_Q, K_BICG_P, K_SPMV, K_BICG_S, K_BICG_X,
     K_MG_SMOOTH, K_MG_RR, K_MG_POST, K_MG_COARSE, K_MG_GALERKIN,
-    K_CORRECT, K_BC, K_DIAG, K_SI, K_MOM_UPDATE, K_SWEEP_FIN, K_MG_PRR, NKERNEL
+    K_CORRECT, K_BC, K_DIAG, K_SI, K_MOM_UPDATE, K_SWEEP_FIN, K_MG_PRR, K_MOM_FIX, NKERNEL
 };
 const char* kKernelNames[NKERNEL] = {
     "k_assemble_p", "k_rhs", "k_sweep", "k_upbc", "k_face_q", "k_bicg_p", "k_spmv", "k_bicg_s",
     "k_bicg_x", "k_mg_presmooth", "k_mg_rr", "k_mg_postsmooth", "k_mg_coarse",
-    "k_mg_galerkin", "k_correct", "k_bc", "k_diag", "k_si", "k_mom_update", "k_sweep_fin", "k_mg_prr"};
+    "k_mg_galerkin", "k_correct", "k_bc", "k_diag", "k_si", "k_mom_update", "k_sweep_fin", "k_mg_prr", "k_mom_fix"};
 
 struct LevelGeom {
     int W, n1, ld, ilo, ihi;
@@ -491,6 +491,9 @@ void enq_mid(cfd_batch* b, BatchDev& bd) {
     if (b->precision == CFD_PRECISION_MIXED) {
         Prof pr(b, K_MOM_UPDATE);
         k_mom_update<<<bd.nftiles, NT, 0, b->st>>>(bd);
+    } else {
+        Prof pr(b, K_MOM_FIX);
+        k_mom_fix<<<bd.njtiles, NT, 0, b->st>>>(bd);
     }
     {
         Prof pr(b, K_UPBC);
@@ -1037,6 +1040,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     bd.error = b->flags + 4;
     bd.mg_res = mg_res_plane(b->mg_pre, b->mg_post, b->mg_fused);
     bd.sweep_no = b->flags + 7;
+    bd.mixed = b->precision == CFD_PRECISION_MIXED;
     for (int l = 0; l < MAXLEV; l++) {
         bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
         bd.mtiles[l] = b->dtiles + pos_mt[l]; bd.nmtiles[l] = (int)mt[l].size();

@@ -79,7 +79,12 @@ enum IScalar {
     I_PDONE, I_PIT, I_PSTATUS, I_TIME,
     I_MDONE0,                 // 5 momentum done flags
     I_MIT0 = I_MDONE0 + NFIELD,  // 5 momentum sweep counts
-    I_STATUS = I_MIT0 + NFIELD,
+    I_MODD0 = I_MIT0 + NFIELD,   // 5 flags: the solve's result is in the scratch plane
+    I_MFLIP0 = I_MODD0 + NFIELD,  // 5 flags: this step's first iterate is in the scratch plane
+    I_MNEXT0 = I_MFLIP0 + NFIELD, // 5 flags: the same, predicted for the next step
+    I_MWORD = I_MNEXT0 + NFIELD,  // the sweep kernel's one read: bits 0-4 fields still iterating,
+                                  // 5-9 I_MFLIP0 bits, 10+ sweeps done (same for every active field)
+    I_STATUS,
     I_ACTIVE,                 // 0: an empty slot, skipped by every kernel
     I_NSTEP,                  // steps taken since the case was admitted
     NISCAL
@@ -131,6 +136,7 @@ struct BatchDev {
     int* mactive;          // global count of (case, field) pairs still iterating (momentum)
     int* error;            // set when a bounded wait in a kernel gives up
     int* sweep_no;         // momentum sweep launches of the current step (k_sweep_fin counts)
+    int mixed;             // 1: the precision form (momentum iterates are FP32 corrections)
     const Tile* ftiles;    // fine-grid tiles of every case (FP64 kernels, multigrid level 0)
     int nftiles;
     const Tile* jtiles;    // 32 x 16 tiles of every case (u/v/T sweeps)

@@ -231,7 +231,15 @@ __global__ void __launch_bounds__(NT, 2) k_rhs(BatchDev b) {
     const bool active = b.iscal[(long long)t.c * NISCAL + I_ACTIVE] != 0;
     if (tid == 0 && t.k == 0) {
         int* is = b.iscal + (long long)t.c * NISCAL;
-        for (int f = 0; f < NFIELD; f++) { is[I_MDONE0 + f] = active ? 0 : 1; is[I_MIT0 + f] = 0; }
+        int word = active ? (1 << NFIELD) - 1 : 0;
+        for (int f = 0; f < NFIELD; f++) {
+            is[I_MDONE0 + f] = active ? 0 : 1;
+            is[I_MIT0 + f] = 0;
+            is[I_MODD0 + f] = 0;
+            is[I_MFLIP0 + f] = b.mixed ? 0 : is[I_MNEXT0 + f];
+            word |= (is[I_MFLIP0 + f] != 0) << (NFIELD + f);
+        }
+        is[I_MWORD] = word;
         if (active) atomicAdd(b.mactive, NFIELD);
         else is[I_PDONE] = 1;  // an empty slot takes no part in the step
     }
@@ -267,6 +275,9 @@ __global__ void __launch_bounds__(NT, 2) k_rhs(BatchDev b) {
     auto Ap = [&](int f) { return plane(b, c, f < 2 ? P_US + f : P_T0 + 2 * (f - 2) + nxt); };
     auto Bp = [&](int f) { return plane(b, c, P_BU + f); };
     const bool warm = c.warm_up != 0;
+    int nextm = 0;  // fields whose first iterate goes into the scratch plane (FP64 form)
+    if (!b.mixed)
+        for (int f = 0; f < NFIELD; f++) nextm |= (b.iscal[(long long)t.c * NISCAL + I_MNEXT0 + f] != 0) << f;
     const int li = tid % TX, lj = tid / TX;
     const int i = t.i0 + li;
 #pragma unroll 1
@@ -335,12 +346,15 @@ __global__ void __launch_bounds__(NT, 2) k_rhs(BatchDev b) {
         plane(b, c, P_RUP)[k] = qup;
         plane(b, c, P_RVP)[k] = qvp;
         // seed the iterates (PSolver.cpp:1241-1337): u*, v*, T from the current fields;
-        // up/vp from the previous solution (warm start) or zero
-        store_mirrored(Ap(F_U), ld, i, j, W, per, uc);
-        store_mirrored(Ap(F_V), ld, i, j, W, per, vc);
-        store_mirrored(Ap(F_T), ld, i, j, W, per, tc);
-        store_mirrored(Ap(F_UP), ld, i, j, W, per, warm ? UPs[o] : 0.0);
-        store_mirrored(Ap(F_VP), ld, i, j, W, per, warm ? VPs[o] : 0.0);
+        // up/vp from the previous solution (warm start) or zero. A solve predicted to stop
+        // after an odd number of sweeps starts in the scratch plane, so that its result
+        // ends in the iterate plane (the prediction is the previous step's parity; FP64 form)
+        auto X0 = [&](int f) { return ((nextm >> f) & 1) ? Bp(f) : Ap(f); };
+        store_mirrored(X0(F_U), ld, i, j, W, per, uc);
+        store_mirrored(X0(F_V), ld, i, j, W, per, vc);
+        store_mirrored(X0(F_T), ld, i, j, W, per, tc);
+        store_mirrored(X0(F_UP), ld, i, j, W, per, warm ? UPs[o] : 0.0);
+        store_mirrored(X0(F_VP), ld, i, j, W, per, warm ? VPs[o] : 0.0);
         // boundary values the stencils read (both iterate buffers)
         auto put_bnd = [&](int bi, int bj) {
             const long long kb = (long long)bj * ld + bi;

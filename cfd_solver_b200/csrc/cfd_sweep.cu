@@ -111,14 +111,15 @@ __device__ __forceinline__ int sw_iter_plane(int f, int nxt) { return f < 2 ? P_
 // issue the tensor copies of field f of tile t into buffer `sm` (with alpha, beta, gamma)
 template <int MODE>
 __device__ __forceinline__ void sw_issue(const Tile& t, int f, int sweep, int nxt, const char* maps,
-                                         unsigned char* sm, unsigned char* met, uint64_t* bar) {
+                                         unsigned char* sm, unsigned char* met, uint64_t* bar, bool flip) {
     using L = SwLayout<MODE>;
     const int pa = sw_iter_plane(f, nxt);
     unsigned bytes = L::XBYTES + L::RBYTES + (met ? L::MBYTES : 0u);
     bool prev = false;
     int xs = 0, ps = 0;
     if (MODE == SW_F64) {
-        const int to_scratch = (sweep & 1) == 0;
+        // x_s is in the iterate plane when s is even, unless the solve started in the scratch plane
+        const bool to_scratch = ((sweep & 1) == 0) != flip;
         xs = to_scratch ? pa : P_BU + f;
         ps = to_scratch ? P_BU + f : pa;
         prev = sweep > 0;
@@ -179,13 +180,13 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
     using ST = typename C::ST;
     const Tile t = b.jtiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
-    const int* isc = b.iscal + (long long)t.c * NISCAL;
-    int mask = 0;
-#pragma unroll
-    for (int f = 0; f < NFIELD; f++) mask |= (isc[I_MDONE0 + f] == 0) << f;
+    // one word: the fields still iterating, those whose first iterate is in the scratch plane
+    // (FP64 form), and the sweeps done (the same for every still-active field of the case)
+    const int word = b.iscal[(long long)t.c * NISCAL + I_MWORD];
+    const int mask = word & ((1 << NFIELD) - 1);
     if (mask == 0) return;  // uniform over the case's CTAs
-    // every still-active field of the case has done the same number of sweeps
-    const int sweep = isc[I_MIT0 + (__ffs(mask) - 1)];
+    const int sweep = word >> (2 * NFIELD);
+    const int flipm = MODE == SW_F64 ? (word >> NFIELD) & ((1 << NFIELD) - 1) : 0;
     const int tid = threadIdx.x, lane = tid & 31, wrp = tid >> 5;
     const int nxt = b.cur ^ 1;
     const int nf = __popc(mask);
@@ -195,8 +196,12 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
         mbar_init(&bar[1], 1);
         fence_mbar_init();
         const int m1 = mask & (mask - 1);
-        sw_issue<MODE>(t, __ffs(mask) - 1, sweep, nxt, maps, sm, sm + L::MET, &bar[0]);
-        if (m1) sw_issue<MODE>(t, __ffs(m1) - 1, sweep, nxt, maps, sm + L::BUF, nullptr, &bar[1]);
+        const int f0 = __ffs(mask) - 1;
+        sw_issue<MODE>(t, f0, sweep, nxt, maps, sm, sm + L::MET, &bar[0], (flipm >> f0) & 1);
+        if (m1) {
+            const int f1 = __ffs(m1) - 1;
+            sw_issue<MODE>(t, f1, sweep, nxt, maps, sm + L::BUF, nullptr, &bar[1], (flipm >> f1) & 1);
+        }
     }
     // per-case constants (uniform)
     const double* sc = b.scal + (long long)t.c * NSCAL;
@@ -273,7 +278,10 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
         if (tid == 0) {
             int nx = fm & (fm - 1);
             nx &= nx - 1;
-            if (nx) sw_issue<MODE>(t, __ffs(nx) - 1, sweep, nxt, maps, sm + bi * L::BUF, nullptr, &bar[bi]);
+            if (nx) {
+                const int f2 = __ffs(nx) - 1;
+                sw_issue<MODE>(t, f2, sweep, nxt, maps, sm + bi * L::BUF, nullptr, &bar[bi], (flipm >> f2) & 1);
+            }
         }
 
         // off-centre sums: the 25-point form for every cell, then the few near-wall cells
@@ -302,7 +310,7 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
         float* res32 = nullptr;
         int dld = ld;
         if (MODE == SW_F64) {
-            dst64 = plane(b, c, (sweep & 1) == 0 ? P_BU + f : sw_iter_plane(f, nxt));
+            dst64 = plane(b, c, (((sweep & 1) == 0) != (((flipm >> f) & 1) != 0)) ? P_BU + f : sw_iter_plane(f, nxt));
         } else if (MODE == SW_MX0) {
             dst32 = xplane(b, c, X_DB + f);
             res32 = xplane(b, c, X_R + f);
@@ -421,24 +429,34 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
     if (tid != 0) return;
     double* scw = b.scal + (long long)cid * NSCAL;
     const int sweep = is[I_MIT0 + (__ffs(mask) - 1)];
-    const int decide = sweep & 1;
+    // the rule is tested after every sweep (on the residual of the sweep's input iterate; the
+    // sweep's output, one sweep further, is the result). After an odd number of sweeps the
+    // result sits in the scratch plane: the flag tells k_mom_fix / k_mom_update where
     for (int f = 0; f < NFIELD; f++) {
         if (!(mask & (1 << f))) continue;
-        if (sweep == 0) scw[S_MR0 + f] = (v[f] != 0.0) ? v[f] : 1.0;
+        if (sweep == 0) {
+            scw[S_MR0 + f] = (v[f] != 0.0) ? v[f] : 1.0;
+            is[I_MNEXT0 + f] = 0;  // next step: start in the iterate plane, unless this solve stops odd
+        }
         scw[S_MR + f] = v[f];
         is[I_MIT0 + f] += 1;
-        if (decide) {
-            bool done = (v[f] / scw[S_MR0 + f] < c.tol_mom) || (v[f] <= c.atol_mom);
-            if (!isfinite(v[f])) {
-                is[I_STATUS] |= ST_NAN;
-                done = true;
-            }
-            if (done) {
-                is[I_MDONE0 + f] = 1;
-                atomicSub(b.mactive, 1);
-            }
+        bool done = (v[f] / scw[S_MR0 + f] < c.tol_mom) || (v[f] <= c.atol_mom);
+        if (!isfinite(v[f])) {
+            is[I_STATUS] |= ST_NAN;
+            done = true;
+        }
+        if (done) {
+            // the result x_{sweep+1} is in the scratch plane when the sweep's parity equals
+            // the solve's start plane flag; predict the next step's start from this parity
+            is[I_MDONE0 + f] = 1;
+            is[I_MODD0 + f] = (sweep & 1) == (is[I_MFLIP0 + f] != 0);
+            is[I_MNEXT0 + f] = (sweep & 1) == 0;
+            atomicSub(b.mactive, 1);
         }
     }
+    int nmask = 0;  // the sweep kernel's word: fields still iterating, start planes, sweeps done
+    for (int f = 0; f < NFIELD; f++) nmask |= (is[I_MDONE0 + f] == 0) << f;
+    is[I_MWORD] = nmask | (is[I_MWORD] & (((1 << NFIELD) - 1) << NFIELD)) | ((sweep + 1) << (2 * NFIELD));
     for (int ty = 0; ty < 2; ty++) {  // Chebyshev weight of the next sweep
         const double ca = c.cheb_a[ty], cb = c.cheb_b[ty];
         const double s2 = ((cb + ca) / (cb - ca)) * ((cb + ca) / (cb - ca));
@@ -457,6 +475,32 @@ size_t sweep_smem_f64() { return (size_t)SwLayout<SW_F64>::TOTAL + 128; }
 size_t sweep_smem_mx() { return (size_t)max(SwLayout<SW_MX0>::TOTAL, SwLayout<SW_MX>::TOTAL) + 128; }
 
 // x0 += d for every field of the precision form (after the last sweep, d_final in X_DA)
+// A solve whose result is in the scratch plane (FP64 form; it stopped after a sweep count of
+// the other parity than predicted): copy it into the iterate plane. 32 x 16 tiles, two
+// cells per thread; the CTAs of a case with no such solve leave at once.
+__global__ void __launch_bounds__(NT) k_mom_fix(BatchDev b) {
+    const Tile t = b.jtiles[blockIdx.x];
+    const int* is = b.iscal + (long long)t.c * NISCAL;
+    int odd = 0;  // solves whose result is in the scratch plane: stopped there, or ran to the
+                  // sweep cap (an even count) after starting there
+#pragma unroll
+    for (int f = 0; f < NFIELD; f++) odd |= (is[I_MDONE0 + f] ? is[I_MODD0 + f] != 0 : is[I_MFLIP0 + f] != 0) << f;
+    if (!odd || !is[I_ACTIVE]) return;
+    const CaseDev& c = b.cases[t.c];
+    const int nxt = b.cur ^ 1;
+    const int i = t.i0 + (int)(threadIdx.x % TX);
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int j = t.j0 + (int)(threadIdx.x / TX) + h * TY;
+        if (i < c.ilo || i > c.ihi || j > c.n1 - 2) continue;
+        const long long k = (long long)j * c.ld + i;
+#pragma unroll
+        for (int f = 0; f < NFIELD; f++)
+            if (odd & (1 << f))
+                store_mirrored(plane(b, c, sw_iter_plane(f, nxt)), c.ld, i, j, c.W, c.periodic, plane(b, c, P_BU + f)[k]);
+    }
+}
+
 __global__ void __launch_bounds__(NT) k_mom_update(BatchDev b) {
     const Tile t = b.ftiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
@@ -470,7 +514,8 @@ __global__ void __launch_bounds__(NT) k_mom_update(BatchDev b) {
 #pragma unroll
     for (int f = 0; f < NFIELD; f++) {
         x[f] = plane(b, c, sw_iter_plane(f, nxt))[k];
-        d[f] = xplane(b, c, X_DA + f)[kx];
+        // the correction after an even number of sweeps is in X_DA, after an odd one in X_DB
+        d[f] = xplane(b, c, (b.iscal[(long long)t.c * NISCAL + I_MODD0 + f] ? X_DB : X_DA) + f)[kx];
     }
 #pragma unroll
     for (int f = 0; f < NFIELD; f++)

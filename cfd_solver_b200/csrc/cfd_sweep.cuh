@@ -13,6 +13,7 @@ __global__ void k_sweep_f64(BatchDev b);
 __global__ void k_sweep_mx(BatchDev b);
 __global__ void k_sweep_fin(BatchDev b);
 __global__ void k_mom_update(BatchDev b);
+__global__ void k_mom_fix(BatchDev b);
 size_t sweep_smem_f64();
 size_t sweep_smem_mx();
 }  // namespace cfd
