@@ -37,7 +37,7 @@ METRIC = "cell-updates/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--form", choices=["twin", "cavity"], default="twin")
@@ -166,6 +166,79 @@ def workload_config(args):
 
 
 # ------------------------------------------------------------------ clocks
+class NvmlClockSampler:
+    """SM clock and clock-event reasons read through NVML every 10 ms on a thread (reads only);
+    only the samples inside [mark_start, mark_end] count."""
+
+    HW, HW_THERMAL, SW_THERMAL, SW_POWER = 0x8, 0x40, 0x20, 0x4
+
+    def __init__(self, index: int):
+        import threading
+        import pynvml
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        self.h = None
+        try:  # the CUDA device's own NVML handle (CUDA and NVML orders can differ)
+            import torch
+            pr = torch.cuda.get_device_properties(index)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+        self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        self.samples = []
+        self.t0 = self.t1 = None
+        self.run = True
+
+        def poll():
+            while self.run:
+                try:
+                    mhz = pynvml.nvmlDeviceGetClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+                    rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                    self.samples.append((time.time(), mhz, rs))
+                except Exception:
+                    pass
+                time.sleep(0.01)
+
+        self.th = threading.Thread(target=poll, daemon=True)
+        self.th.start()
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+
+    def stop(self):
+        self.run = False
+        self.th.join(timeout=5)
+        sm, reasons = [], set()
+        names = {self.HW: "hw_slowdown", self.HW_THERMAL: "hw_thermal_slowdown",
+                 self.SW_THERMAL: "sw_thermal_slowdown", self.SW_POWER: "sw_power_cap"}
+        for ts, mhz, rs in self.samples:
+            if self.t0 is not None and not (self.t0 <= ts <= (self.t1 or ts)):
+                continue
+            sm.append(float(mhz))
+            for bit, n in names.items():
+                if rs & bit:
+                    reasons.add(n)
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(self.max_mhz), "reasons": sorted(reasons),
+                "samples": len(sm), "source": "nvml, 10 ms"}
+
+
+def clock_sampler(index: int):
+    try:
+        return NvmlClockSampler(index)
+    except Exception:
+        return ClockSampler(index)
+
+
 class ClockSampler:
     """nvidia-smi samples stamped on arrival; only those inside [mark_start, mark_end] count."""
 
@@ -288,7 +361,7 @@ def run_converged(args):
     n = len(cases)
     active = [True] * n
     steps_at, outcome, nu = [0] * n, [""] * n, [0.0] * n
-    clocks = ClockSampler(0)
+    clocks = clock_sampler(0)
     torch.cuda.synchronize()
     clocks.mark_start()
     t0 = time.perf_counter()
@@ -495,7 +568,7 @@ def main():
         b.set_mg(*mg)
     stream = torch.cuda.ExternalStream(b.stream())
 
-    clocks = ClockSampler(local)
+    clocks = clock_sampler(local)
     for _ in range(args.warmup):
         b.step(1)
     b.sync()
