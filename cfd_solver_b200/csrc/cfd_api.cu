@@ -173,6 +173,7 @@ struct cfd_batch {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int launches_per_pair = 2, launches_per_iter = 0, launches_per_half = 0, launches_fixed = 0;
     int flags_total0[3] = {0, 0, 0};
+    int* tword = nullptr;                // per tile: the case's momentum-loop word
     unsigned long long* work = nullptr;  // k_jac traffic counters
     long long launches = 0;              // kernels launched since creation
     int* h_flags = nullptr;
@@ -947,6 +948,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     ALLOC(b->counter, sizeof(unsigned) * ncases);
     ALLOC(b->flags, sizeof(int) * NFLAGS);
     ALLOC(b->work, sizeof(unsigned long long) * 4);
+    ALLOC(b->tword, sizeof(int) * std::max<size_t>(jtiles.size(), 1));
     ALLOC(b->dtmaps, (size_t)TMAP_STRIDE * ncases);
     ALLOC(b->dtiles, sizeof(Tile) * std::max<size_t>(ntl, 1));
     ALLOC(b->dcc, sizeof(int) * std::max<size_t>(ncc, 1));
@@ -1041,6 +1043,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     bd.mg_res = mg_res_plane(b->mg_pre, b->mg_post, b->mg_fused);
     bd.sweep_no = b->flags + 7;
     bd.mixed = b->precision == CFD_PRECISION_MIXED;
+    bd.tword = b->tword;
     for (int l = 0; l < MAXLEV; l++) {
         bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
         bd.mtiles[l] = b->dtiles + pos_mt[l]; bd.nmtiles[l] = (int)mt[l].size();
@@ -1115,7 +1118,7 @@ int cfd_batch_destroy(cfd_batch* b) {
     for (auto e : b->pool) cudaEventDestroy(e);
     cudaFree(b->f64); cudaFree(b->f32); cudaFree(b->dc); cudaFree(b->scal); cudaFree(b->iscal);
     cudaFree(b->stage); cudaFree(b->stage_off);
-    cudaFree(b->partial); cudaFree(b->counter); cudaFree(b->flags); cudaFree(b->work); cudaFree(b->dtiles); cudaFree(b->dcc); cudaFree(b->dtmaps);
+    cudaFree(b->partial); cudaFree(b->counter); cudaFree(b->flags); cudaFree(b->work); cudaFree(b->tword); cudaFree(b->dtiles); cudaFree(b->dcc); cudaFree(b->dtmaps);
     if (b->h_flags) cudaFreeHost(b->h_flags);
     if (b->st) cudaStreamDestroy(b->st);
     delete b;
@@ -1284,14 +1287,19 @@ int cfd_batch_work(cfd_batch* b, unsigned long long* out4) {
     return CFD_OK;
 }
 
-// the resident state of every case: u, v, p, T, up, vp (padded device planes, in case order)
+// the resident state of every case: u, v, p, T, up, vp (n1 rows of the stored columns each,
+// in case order) and 16 doubles of counters
 static const int kStatePlanes = 6;
+
+static long long state_doubles(const CaseDev& d) {
+    return (long long)kStatePlanes * d.n1 * (d.periodic ? d.W : d.n0) + 16;
+}
 
 size_t cfd_batch_state_bytes(cfd_batch* b) {
     if (!b) return 0;
     size_t s = 0;
-    for (auto& d : b->hc) s += (size_t)kStatePlanes * d.ps * sizeof(double);
-    return s + 16 * sizeof(double) * b->n;
+    for (auto& d : b->hc) s += (size_t)state_doubles(d) * sizeof(double);
+    return s;
 }
 
 // The state crosses PCIe as one copy per direction: a kernel packs (or unpacks) every
@@ -1305,7 +1313,7 @@ static int state_copy(cfd_batch* b, void* host, size_t bytes, bool to_host) {
         long long o = 0;
         for (int c = 0; c < b->n; c++) {
             off[c] = o;
-            o += (long long)kStatePlanes * b->hc[c].ps + 16;
+            o += state_doubles(b->hc[c]);
         }
         CK(cudaMalloc((void**)&b->stage, need));
         CK(cudaMalloc((void**)&b->stage_off, sizeof(long long) * b->n));
@@ -1326,10 +1334,11 @@ static int state_copy(cfd_batch* b, void* host, size_t bytes, bool to_host) {
 }
 
 // Checkpoint file (replaces the reference's spa100.dat restart writer, PSolver.cpp:2006-2016):
-//   "CFDB200C" | u32 version 1 | u32 cases | per case i32 n0, n1, profile, precision |
+//   "CFDB200C" | u32 version 2 | u32 cases | per case i32 n0, n1, profile, precision |
 //   the state image of cfd_batch_get_state | u64 FNV-1a hash of all preceding bytes
 namespace {
 const char kCkptMagic[8] = {'C', 'F', 'D', 'B', '2', '0', '0', 'C'};
+const uint32_t kCkptVersion = 2;  // 1: padded device planes in the state image; 2: stored columns only
 uint64_t fnv1a(const unsigned char* p, size_t n, uint64_t h = 1469598103934665603ull) {
     for (size_t k = 0; k < n; k++) {
         h ^= p[k];
@@ -1345,7 +1354,7 @@ int cfd_batch_save(cfd_batch* b, const char* path) {
     std::vector<unsigned char> buf(8 + 8 + (size_t)16 * b->n + sb + 8);
     unsigned char* p = buf.data();
     memcpy(p, kCkptMagic, 8);
-    const uint32_t hdr[2] = {1u, (uint32_t)b->n};
+    const uint32_t hdr[2] = {kCkptVersion, (uint32_t)b->n};
     memcpy(p + 8, hdr, 8);
     for (int c = 0; c < b->n; c++) {
         const int32_t g[4] = {b->hc[c].n0, b->hc[c].n1, b->hc[c].profile, b->prm[c].precision};
@@ -1376,7 +1385,7 @@ int cfd_batch_load(cfd_batch* b, const char* path) {
     if (buf.size() < 16 || memcmp(buf.data(), kCkptMagic, 8) != 0) return fail(CFD_E_ARG, "not a checkpoint file");
     uint32_t hdr[2];
     memcpy(hdr, buf.data() + 8, 8);
-    if (hdr[0] != 1u) return fail(CFD_E_ARG, "unsupported checkpoint version");
+    if (hdr[0] != kCkptVersion) return fail(CFD_E_ARG, "unsupported checkpoint version");
     if ((int)hdr[1] != b->n || buf.size() != need)
         return fail(CFD_E_ARG, "checkpoint does not match the batch (number of cases or sizes)");
     uint64_t h;

@@ -137,6 +137,8 @@ struct BatchDev {
     int* error;            // set when a bounded wait in a kernel gives up
     int* sweep_no;         // momentum sweep launches of the current step (k_sweep_fin counts)
     int mixed;             // 1: the precision form (momentum iterates are FP32 corrections)
+    int* tword;            // per 32 x 16 tile: its case's I_MWORD, so the sweep kernel reads it
+                           // in the same round trip as the tile itself
     const Tile* ftiles;    // fine-grid tiles of every case (FP64 kernels, multigrid level 0)
     int nftiles;
     const Tile* jtiles;    // 32 x 16 tiles of every case (u/v/T sweeps)

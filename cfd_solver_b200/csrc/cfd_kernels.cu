@@ -243,6 +243,13 @@ __global__ void __launch_bounds__(NT, 2) k_rhs(BatchDev b) {
         if (active) atomicAdd(b.mactive, NFIELD);
         else is[I_PDONE] = 1;  // an empty slot takes no part in the step
     }
+    if (tid == 0) {  // the sweep kernel's word for this tile (I_MWORD of the case)
+        int word = active ? (1 << NFIELD) - 1 : 0;
+        if (active && !b.mixed)
+            for (int f = 0; f < NFIELD; f++)
+                word |= (b.iscal[(long long)t.c * NISCAL + I_MNEXT0 + f] != 0) << (NFIELD + f);
+        b.tword[blockIdx.x] = word;
+    }
     if (!active) return;
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -1643,14 +1650,16 @@ __global__ void k_if_cond(cudaGraphConditionalHandle h, const int* flag, int* to
 #undef AT
 // ---------------------------------------------------------------------------
 // Resident state <-> one contiguous staging buffer (so a state snapshot crosses PCIe as one
-// copy per direction). Per case: the six state planes u, v, p, T, up, vp (whole padded
-// planes, ps doubles each, in that order), then 16 doubles: int time and int steps taken,
-// then the first-step steady residual and continuity norm (the references of the relative
-// residuals). blockIdx.x = case * 7 + m (m = 6: the counter slot).
+// copy per direction). Per case: the six state planes u, v, p, T, up, vp, each n1 rows of the
+// stored columns (n0 for the cavity, W = n0 - 1 for the periodic O-grid), then 16 doubles:
+// int time and int steps taken, then the first-step steady residual and continuity norm (the
+// references of the relative residuals). Unpacking writes the periodic halo mirrors too.
+// blockIdx.x = case * 7 + m (m = 6: the counter slot); one warp per row.
 __global__ void __launch_bounds__(256) k_state_pack(BatchDev b, double* stage, const long long* off, int to_stage) {
     const int c = blockIdx.x / 7, m = blockIdx.x % 7;
     const CaseDev& d = b.cases[c];
-    double* dst = stage + off[c] + (long long)m * d.ps;
+    const int nc = d.periodic ? d.W : d.n0;
+    double* dst = stage + off[c] + (long long)m * d.n1 * nc;
     if (m == 6) {
         // the case's counters: the reference's int time, the steps taken, and the
         // first-step references of the relative residuals
@@ -1663,6 +1672,7 @@ __global__ void __launch_bounds__(256) k_state_pack(BatchDev b, double* stage, c
                 di[1] = is[I_NSTEP];
                 dst[1] = sc[S_SR0];
                 dst[2] = sc[S_QL2_0];
+                for (int k = 3; k < 16; k++) dst[k] = 0.0;
             } else {
                 is[I_TIME] = di[0];
                 is[I_NSTEP] = di[1];
@@ -1673,11 +1683,17 @@ __global__ void __launch_bounds__(256) k_state_pack(BatchDev b, double* stage, c
         return;
     }
     const int ids[6] = {P_U, P_V, P_P, P_T0 + b.cur, P_UP0 + b.cur, P_VP0 + b.cur};
-    double* src = b.f64 + d.base + H - 16 + (long long)ids[m] * d.ps;  // 128-byte aligned plane start
-    const long long n2 = d.ps / 2;                                       // ps is a multiple of 16
-    double2* a = reinterpret_cast<double2*>(to_stage ? dst : src);
-    const double2* s2 = reinterpret_cast<const double2*>(to_stage ? src : dst);
-    for (long long e = threadIdx.x; e < n2; e += blockDim.x) a[e] = s2[e];
+    double* P = plane(b, d, ids[m]);
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int j = threadIdx.x >> 5; j < d.n1; j += nw) {
+        double* row = P + (long long)j * d.ld;
+        double* srow = dst + (long long)j * nc;
+        if (to_stage) {
+            for (int i = lane; i < nc; i += 32) srow[i] = row[i];
+        } else {
+            for (int i = lane; i < nc; i += 32) store_mirrored(row, 0, i, 0, d.W, d.periodic, srow[i]);
+        }
+    }
 }
 
 }  // namespace cfd

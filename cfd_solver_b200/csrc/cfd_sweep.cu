@@ -180,9 +180,10 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
     using ST = typename C::ST;
     const Tile t = b.jtiles[blockIdx.x];
     const CaseDev& c = b.cases[t.c];
-    // one word: the fields still iterating, those whose first iterate is in the scratch plane
+    // one word (the case's I_MWORD, kept per tile so that it is read in the same round trip as
+    // the tile): the fields still iterating, those whose first iterate is in the scratch plane
     // (FP64 form), and the sweeps done (the same for every still-active field of the case)
-    const int word = b.iscal[(long long)t.c * NISCAL + I_MWORD];
+    const int word = b.tword[blockIdx.x];
     const int mask = word & ((1 << NFIELD) - 1);
     if (mask == 0) return;  // uniform over the case's CTAs
     const int sweep = word >> (2 * NFIELD);
@@ -456,7 +457,9 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
     }
     int nmask = 0;  // the sweep kernel's word: fields still iterating, start planes, sweeps done
     for (int f = 0; f < NFIELD; f++) nmask |= (is[I_MDONE0 + f] == 0) << f;
-    is[I_MWORD] = nmask | (is[I_MWORD] & (((1 << NFIELD) - 1) << NFIELD)) | ((sweep + 1) << (2 * NFIELD));
+    const int nword = nmask | (is[I_MWORD] & (((1 << NFIELD) - 1) << NFIELD)) | ((sweep + 1) << (2 * NFIELD));
+    is[I_MWORD] = nword;
+    for (int k = 0; k < c.jt_count; k++) b.tword[c.jt_begin + k] = nword;
     for (int ty = 0; ty < 2; ty++) {  // Chebyshev weight of the next sweep
         const double ca = c.cheb_a[ty], cb = c.cheb_b[ty];
         const double s2 = ((cb + ca) / (cb - ca)) * ((cb + ca) / (cb - ca));

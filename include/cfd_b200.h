@@ -232,15 +232,18 @@ int cfd_gauss_solve_noalloc(int n0, int n1, int periodic, const double* const* c
                             const double* q, double tol, int maxit, int* sweeps, void* stream);
 
 /* ---- resident state snapshot (checkpoint / restart, host-owned stepping) ----
- * An opaque image of every case's u, v, p, T, up, vp, int time, steps taken and the
- * first-step references of the relative residuals, in the device layout;
- * cfd_batch_state_bytes() gives its size. Use pinned host memory for speed. Restoring an
- * image and stepping gives the same bits as the steps taken from it. */
+ * An image of every case's u, v, p, T, up, vp, int time, steps taken and the first-step
+ * references of the relative residuals. Per case, in case order: the six fields as
+ * row-major doubles, n1 rows of the stored columns (n0 for the cavity; n0 - 1 for the
+ * periodic O-grid, whose column n0 - 1 repeats column 0), then 16 doubles (int time and
+ * int steps in the first, the two references in the next two). cfd_batch_state_bytes()
+ * gives its size. Use pinned host memory for speed. Restoring an image and stepping gives
+ * the same bits as the steps taken from it. */
 size_t cfd_batch_state_bytes(cfd_batch* b);
 int cfd_batch_get_state(cfd_batch* b, void* host, size_t bytes);
 int cfd_batch_set_state(cfd_batch* b, const void* host, size_t bytes);
 /* Checkpoint files, in place of the reference's restart file spa100.dat (PSolver.cpp:2006-2016,
- * whose C++ writer dumps pointers): "CFDB200C", u32 version (1), u32 number of cases, per
+ * whose C++ writer dumps pointers): "CFDB200C", u32 version (2), u32 number of cases, per
  * case i32 n0, n1, profile, precision, the state image above, u64 FNV-1a hash of all
  * preceding bytes (little-endian). cfd_batch_load() checks magic, version, every case's
  * geometry and precision against the batch, and the hash, and fails with CFD_E_ARG

@@ -86,3 +86,27 @@ def test_checkpoint_file_restart_is_exact(tmp_path):
     with Batch(gs[:2], ps[:2]) as other:
         with pytest.raises(_lib.CfdError, match="does not match"):
             other.load(ck)
+
+
+def test_state_image_layout():
+    """The image holds, per case, u, v, p, T, up, vp as n1 rows of the stored columns (n0 - 1
+    for the periodic O-grid, n0 for the cavity), then 16 doubles of counters."""
+    from cfd_solver_b200.solver import Batch
+    gs, ps = _cases()
+    with Batch(gs, ps) as a:
+        a.step(3)
+        img = np.empty(a.state_bytes(), dtype=np.uint8)
+        a.get_state(img)
+        fields = _fields(a, len(gs))
+    words = img.view(np.float64)
+    o = 0
+    for g, f in zip(gs, fields):
+        nc = g.n0 - 1 if g.kind == "ogrid" else g.n0
+        for k in FIELDS:
+            got = words[o:o + g.n1 * nc].reshape(g.n1, nc)
+            np.testing.assert_array_equal(got, f[k][:, :nc], err_msg=k)
+            o += g.n1 * nc
+        counters = words[o:o + 16]
+        assert counters[:1].view(np.int32)[1] == 3  # steps taken
+        o += 16
+    assert o * 8 == img.size
