@@ -1306,7 +1306,7 @@ __global__ void __launch_bounds__(NT, 4) k_correct(BatchDev b) {
 // ---------------------------------------------------------------------------
 // boundary update, boundary pressure and wall integrals: one CTA per case
 // (O-grid: PSolver.cpp:1549-1783 and 1855-1983; cavity: this project's walls)
-__global__ void __launch_bounds__(BC_THREADS) k_bc(BatchDev b) {
+__global__ void __launch_bounds__(BC_THREADS, 2) k_bc(BatchDev b) {
     const int cid = blockIdx.x;
     const CaseDev& c = b.cases[cid];
     if (!b.iscal[(long long)cid * NISCAL + I_ACTIVE]) return;
