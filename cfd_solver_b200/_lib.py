@@ -49,7 +49,8 @@ class CfdParams(ctypes.Structure):
                 ("tol_mom", _D), ("atol_mom", _D), ("tol_p", _D), ("atol_p", _D),
                 ("maxit_mom", ctypes.c_int), ("maxit_p", ctypes.c_int), ("profile", ctypes.c_int),
                 ("fix_T_annw", ctypes.c_int), ("fix_circ_de", ctypes.c_int),
-                ("warm_start", ctypes.c_int), ("omega_p", _D), ("lid_u", _D), ("precision", ctypes.c_int)]
+                ("warm_start", ctypes.c_int), ("omega_p", _D), ("lid_u", _D), ("precision", ctypes.c_int),
+                ("time_accurate", ctypes.c_int)]
 
 
 class CfdStepStats(ctypes.Structure):
@@ -58,7 +59,7 @@ class CfdStepStats(ctypes.Structure):
                 ("nu", _D), ("circ", _D), ("cl_pr", _D), ("cd_pr", _D), ("cl_vor", _D),
                 ("cd_vor", _D), ("q_l1", _D), ("q_l2", _D), ("q_max", _D), ("dT_l1", _D),
                 ("dT_max", _D), ("p_res_rel", _D), ("mass_res_rel", _D), ("steady_res", _D),
-                ("steady_res_rel", _D)]
+                ("steady_res_rel", _D), ("time", _D)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "it_mom"}

@@ -391,6 +391,7 @@ void cheb_bounds(const cfd_grid& g, const cfd_params& p, CaseDev& d) {
 // physics, numerics and Chebyshev bounds of one case into its descriptor
 void case_params_to_dev(CaseDev& d, const cfd_grid& g, const cfd_params& p) {
     d.fix_T_annw = p.fix_T_annw; d.fix_circ_de = p.fix_circ_de; d.warm_up = p.warm_start;
+    d.time_accurate = p.time_accurate != 0;
     d.d0 = g.dxi0; d.d1 = g.dxi1; d.dt = p.dt; d.Re = p.Re; d.Pr = p.Pr; d.Ri = p.Ri; d.F = p.F;
     d.Pi = acos(-1.0);
     const double thetamax = d.Pi / 12.0;
@@ -746,6 +747,7 @@ void fill_stats(cfd_batch* b, int c, cfd_step_stats* s) {
     const double r0 = sc[S_SR0];
     s->steady_res_rel = r0 > 0 ? s->steady_res / r0 : (s->steady_res == 0 ? 0.0 : 1.0);
     s->steps = is[I_NSTEP];
+    s->time = b->prm[c].time_accurate ? sc[S_TIME] : (double)is[I_TIME];
 }
 
 int plane_id(const char* name, int cur) {
@@ -821,6 +823,7 @@ void cfd_params_default(cfd_params* p) {
     p->fix_T_annw = 0; p->fix_circ_de = 0; p->warm_start = 1;
     p->omega_p = 1.0; p->lid_u = 1.0;
     p->precision = CFD_PRECISION_FP64;
+    p->time_accurate = 0;
 }
 
 const char* cfd_last_error(void) { return g_err.c_str(); }

@@ -71,7 +71,8 @@ enum Scalar {
     S_QL2_0, S_SR, S_SR0,                   // first-step q_l2; steady residual (now, first step)
     S_MR0 = 29,           // 5 initial momentum residuals (L1)
     S_MR = S_MR0 + NFIELD,  // 5 latest momentum residuals
-    NSCAL = S_MR + NFIELD + 2
+    S_TIME = S_MR + NFIELD,  // time as a double (time-accurate mode)
+    NSCAL = S_TIME + 2
 };
 
 // per-case integer slots
@@ -110,6 +111,7 @@ struct CaseDev {
     int xld;                        // FP32 precision-form planes: pitch, base, stride
     long long xbase, xps;
     int fix_T_annw, fix_circ_de, warm_up;
+    int time_accurate;              // 1: time is a double (t = n dt), 0: the reference's int
     double d0, d1, dt, Re, Pr, Ri, F;
     double uinf, vinf, speed_amp, accn_amp, Pi, ar, omega_p, lid_u, sa, ca;
     double tol_mom, atol_mom, tol_p, atol_p;

@@ -6,7 +6,7 @@
 // and COEFF_HIS_pr_vor.dat (PSolver.cpp:1989-2040). This program does the same through the
 // C ABI of include/cfd_b200.h; the physics constants the reference hard-codes are options.
 //
-//   cfd_b200_solver [INP.DAT] [--steps N] [--Re x] [--Ri x] [--Pr x] [--F x] [--alpha deg]
+//   cfd_b200_solver [INP.DAT] [--steps N] [--Re x] [--Ri x] [--Pr x] [--F x] [--time-accurate] [--alpha deg]
 //                   [--dt x] [--profile ogrid|cavity] [--precision fp64|mixed]
 //                   [--tol-mom x] [--tol-p x] [--out-every N] [--solve-to tol] [--quiet]
 //                   [--dir DIR]
@@ -142,11 +142,12 @@ bool write_spt(const std::string& path, const Grid& g, const std::vector<double>
 }
 
 // COEFF_HIS.dat / COEFF_HIS_pr_vor.dat: appended, the int time and four fixed 8-decimal
-// values (PSolver.cpp:2018-2026)
-bool append_his(const std::string& path, int time, double a, double b, double c, double d) {
+// values (PSolver.cpp:2018-2026); in time-accurate mode the time as a fixed 8-decimal value
+bool append_his(const std::string& path, double time, bool as_int, double a, double b, double c, double d) {
     FILE* o = std::fopen(path.c_str(), "a");
     if (!o) return false;
-    std::fprintf(o, "%d %.8f %.8f %.8f %.8f\n", time, a, b, c, d);
+    if (as_int) std::fprintf(o, "%d %.8f %.8f %.8f %.8f\n", (int)time, a, b, c, d);
+    else std::fprintf(o, "%.8f %.8f %.8f %.8f %.8f\n", time, a, b, c, d);
     return std::fclose(o) == 0;
 }
 
@@ -167,7 +168,7 @@ bool write_surf(const std::string& path, const Grid& g, const std::vector<double
 
 int usage() {
     std::fprintf(stderr,
-                 "usage: cfd_b200_solver [INP.DAT] [--steps N] [--Re x] [--Ri x] [--Pr x] [--F x] [--alpha deg]\n"
+                 "usage: cfd_b200_solver [INP.DAT] [--steps N] [--Re x] [--Ri x] [--Pr x] [--F x] [--time-accurate] [--alpha deg]\n"
                  "       [--dt x] [--profile ogrid|cavity] [--precision fp64|mixed] [--tol-mom x] [--tol-p x]\n"
                  "       [--out-every N] [--solve-to tol] [--quiet] [--dir DIR]\n");
     return 1;
@@ -206,6 +207,7 @@ int main(int argc, char** argv) {
         else if (k == "--out-every") { if (!num(d)) return usage(); out_every = (int)d; }
         else if (k == "--solve-to") { if (!num(solve_to)) return usage(); }
         else if (k == "--quiet") quiet = true;
+        else if (k == "--time-accurate") prm.time_accurate = 1;
         else if (k == "--dir") { const char* v = val(); if (!v) return usage(); dir = v; }
         else if (k == "--profile") {
             const char* v = val();
@@ -240,13 +242,14 @@ int main(int argc, char** argv) {
     const size_t np = (size_t)g.n0 * g.n1;
     std::vector<double> f[6];
     for (auto& v : f) v.resize(np);
-    int time = 0;  // the reference's time is an int (PSolver.cpp:186)
+    double time = 0;  // the reference's time is an int (PSolver.cpp:186), unless time-accurate
+    const bool int_time = !prm.time_accurate;
     auto outputs = [&](const cfd_step_stats& st) -> bool {
         if (cfd_case_get_fields(c, f[0].data(), f[1].data(), f[2].data(), f[3].data(), f[4].data(), f[5].data()))
             return false;
         return write_spt(dir + "/spt100.dat", g, f) &&
-               append_his(dir + "/COEFF_HIS.dat", time, st.cl, st.cd, st.cm, st.nu) &&
-               append_his(dir + "/COEFF_HIS_pr_vor.dat", time, st.cl_pr, st.cd_pr, st.cl_vor, st.cd_vor) &&
+               append_his(dir + "/COEFF_HIS.dat", time, int_time, st.cl, st.cd, st.cm, st.nu) &&
+               append_his(dir + "/COEFF_HIS_pr_vor.dat", time, int_time, st.cl_pr, st.cd_pr, st.cl_vor, st.cd_vor) &&
                write_surf(dir + "/SURF_DIST.dat", g, f);
     };
     int rc = 0;
@@ -263,7 +266,7 @@ int main(int argc, char** argv) {
         for (long long loop = 0; loop < steps && rc == CFD_OK; loop++) {
             rc = cfd_case_step(c, 1, &st);
             if (rc) break;
-            time = (int)(time + prm.dt);
+            time = st.time;  // (int)(time + dt) in the reference's int mode
             if (!quiet) std::printf("%lld %g\n", loop, st.dmax);  // "loop dmax", PSolver.cpp:1890
             if (out_every > 0 && loop % out_every == 0 && !outputs(st)) rc = CFD_E_ARG;
         }

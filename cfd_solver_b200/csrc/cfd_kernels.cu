@@ -1338,6 +1338,8 @@ __global__ void __launch_bounds__(BC_THREADS, 2) k_bc(BatchDev b) {
     int* is = b.iscal + (long long)cid * NISCAL;
     double* sc = b.scal + (long long)cid * NSCAL;
     const int time_new = (int)((double)is[I_TIME] + dt);
+    // the time the wall motion sees: the reference's int (PSolver.cpp:186), or t = n dt
+    const double t_new = c.time_accurate ? sc[S_TIME] + dt : (double)time_new;
     const int jf = n1 - 1;
     // far-field u/v before this update (uold of PSolver.cpp:1456); W <= 4096
     extern __shared__ double s_old[];  // 2 * (W + 1)
@@ -1362,7 +1364,7 @@ __global__ void __launch_bounds__(BC_THREADS, 2) k_bc(BatchDev b) {
             __syncthreads();
         }
         const double circ = s_circ;
-        const double cwall = cos(2.0 * Pi * c.F * time_new);
+        const double cwall = cos(2.0 * Pi * c.F * t_new);
         for (int i = threadIdx.x; i < W; i += blockDim.x) {
             // vr/vth just inside (PSolver.cpp:1549-1562) and their far-field prediction (:1582-1609)
             const long long kb = (long long)(jf - 1) * ld + i, k = (long long)jf * ld + i;
@@ -1403,7 +1405,7 @@ __global__ void __launch_bounds__(BC_THREADS, 2) k_bc(BatchDev b) {
         }
         __syncthreads();
         // boundary pressure (PSolver.cpp:1668-1783)
-        const double swall = sin(2.0 * Pi * c.F * time_new);
+        const double swall = sin(2.0 * Pi * c.F * t_new);
         const double* Fl[2] = {U, V};
         for (int i = threadIdx.x; i < W; i += blockDim.x) {
             {   // wall, j = 0
@@ -1536,6 +1538,7 @@ __global__ void __launch_bounds__(BC_THREADS, 2) k_bc(BatchDev b) {
             sc[S_NU] = -acc[6];
         sc[S_CIRC] = cav ? 0.0 : s_circ;
         is[I_TIME] = time_new;
+        sc[S_TIME] = t_new;
     }
 }
 
@@ -1653,7 +1656,7 @@ __global__ void k_if_cond(cudaGraphConditionalHandle h, const int* flag, int* to
 // copy per direction). Per case: the six state planes u, v, p, T, up, vp, each n1 rows of the
 // stored columns (n0 for the cavity, W = n0 - 1 for the periodic O-grid), then 16 doubles:
 // int time and int steps taken, then the first-step steady residual and continuity norm (the
-// references of the relative residuals). Unpacking writes the periodic halo mirrors too.
+// references of the relative residuals), then the time as a double. Unpacking writes the periodic halo mirrors too.
 // blockIdx.x = case * 7 + m (m = 6: the counter slot); one warp per row.
 __global__ void __launch_bounds__(256) k_state_pack(BatchDev b, double* stage, const long long* off, int to_stage) {
     const int c = blockIdx.x / 7, m = blockIdx.x % 7;
@@ -1672,12 +1675,14 @@ __global__ void __launch_bounds__(256) k_state_pack(BatchDev b, double* stage, c
                 di[1] = is[I_NSTEP];
                 dst[1] = sc[S_SR0];
                 dst[2] = sc[S_QL2_0];
-                for (int k = 3; k < 16; k++) dst[k] = 0.0;
+                dst[3] = sc[S_TIME];
+                for (int k = 4; k < 16; k++) dst[k] = 0.0;
             } else {
                 is[I_TIME] = di[0];
                 is[I_NSTEP] = di[1];
                 sc[S_SR0] = dst[1];
                 sc[S_QL2_0] = dst[2];
+                sc[S_TIME] = dst[3];
             }
         }
         return;

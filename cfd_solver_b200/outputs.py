@@ -35,9 +35,12 @@ def write_spt(path, grid, f: dict) -> None:
     Path(path).write_text("\n".join(lines) + "\n")
 
 
-def write_coeff_his(path, time: int, a: float, b: float, c: float, d: float) -> None:
+def write_coeff_his(path, time, a: float, b: float, c: float, d: float) -> None:
+    """One line: the reference's int time (PSolver.cpp:2018-2026), or the time as a fixed
+    8-decimal value when it is a float (time-accurate mode)."""
+    t = f"{time:.8f}" if isinstance(time, float) else f"{int(time)}"
     with open(path, "a") as fh:
-        fh.write(f"{int(time)} {a:.8f} {b:.8f} {c:.8f} {d:.8f}\n")
+        fh.write(f"{t} {a:.8f} {b:.8f} {c:.8f} {d:.8f}\n")
 
 
 def write_surf_dist(path, grid, f: dict) -> None:

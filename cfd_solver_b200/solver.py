@@ -227,7 +227,8 @@ class Solver:
         self.params = case_params(self.grid, **params)
         self.batch = Batch([self.grid], [self.params])
         self.loop = 0
-        self.time = 0  # the reference keeps time as an int (PSolver.cpp:186)
+        # the reference keeps time as an int (PSolver.cpp:186); time-accurate mode, a float
+        self.time = 0.0 if self.params.time_accurate else 0
         self.history = []
 
     def fields(self) -> dict:
@@ -237,8 +238,8 @@ class Solver:
         """Advance nsteps; write spt100.dat / COEFF_HIS*.dat / SURF_DIST.dat when loop % 100 == 0."""
         for _ in range(nsteps):
             self.batch.step(1)
-            self.time = int(self.time + self.params.dt)
             st = self.batch.stats(0)
+            self.time = st["time"] if self.params.time_accurate else int(self.time + self.params.dt)
             self.history.append(st)
             if write and output_every and self.loop % output_every == 0:
                 self.write_outputs(st)
@@ -249,9 +250,13 @@ class Solver:
         """Advance nsteps without per-step host work (throughput path)."""
         self.batch.step(nsteps)
         self.loop += nsteps
-        for _ in range(nsteps):
-            self.time = int(self.time + self.params.dt)
-        return self.batch.stats(0)
+        st = self.batch.stats(0)
+        if self.params.time_accurate:
+            self.time = st["time"]
+        else:
+            for _ in range(nsteps):
+                self.time = int(self.time + self.params.dt)
+        return st
 
     def write_outputs(self, st: dict):
         f = self.fields()

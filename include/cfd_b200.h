@@ -72,6 +72,10 @@ typedef struct cfd_params {
     double omega_p;            /* p += omega_p * pcor (reference: 1) */
     double lid_u;              /* cavity lid velocity */
     int precision;             /* CFD_PRECISION_FP64 (plain) or CFD_PRECISION_MIXED; one per batch */
+    int time_accurate;         /* 0: time is the reference's int (PSolver.cpp:186; the oscillating
+                                  wall of PSolver.cpp:1617-1630 then sees t = 0 while dt < 1);
+                                  1: time is a double, t = n dt, for unsteady oscillating-cylinder
+                                  runs (F != 0) */
 } cfd_params;
 
 /* Statistics of the last completed step of a case. */
@@ -89,6 +93,7 @@ typedef struct cfd_step_stats {
     double mass_res_rel;      /* q_l2 / q_l2 of the case's first step */
     double steady_res;        /* mean (|du| + |dv| + |dT|) / dt over the unknown cells */
     double steady_res_rel;    /* steady_res / steady_res of the case's first step */
+    double time;              /* the case's time after the step (an integer unless time_accurate) */
 } cfd_step_stats;
 
 typedef struct cfd_batch cfd_batch;
@@ -236,7 +241,8 @@ int cfd_gauss_solve_noalloc(int n0, int n1, int periodic, const double* const* c
  * references of the relative residuals. Per case, in case order: the six fields as
  * row-major doubles, n1 rows of the stored columns (n0 for the cavity; n0 - 1 for the
  * periodic O-grid, whose column n0 - 1 repeats column 0), then 16 doubles (int time and
- * int steps in the first, the two references in the next two). cfd_batch_state_bytes()
+ * int steps in the first, the two references in the next two, the time as a double in the
+ * fourth). cfd_batch_state_bytes()
  * gives its size. Use pinned host memory for speed. Restoring an image and stepping gives
  * the same bits as the steps taken from it. */
 size_t cfd_batch_state_bytes(cfd_batch* b);

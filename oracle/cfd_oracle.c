@@ -60,6 +60,7 @@ typedef struct {
     int fix_circ_de;
     double omega_p; /* p += omega_p * pcor (the reference: 1) */
     double lid_u;   /* cavity lid velocity */
+    int time_accurate; /* 1: the wall motion sees t = n dt (a double); 0: the reference's int time */
 } orc_params;
 
 /* per-step diagnostics record */
@@ -83,6 +84,7 @@ typedef struct {
     orc_params prm;
     double Pi, uinf, vinf, speed_amp, accn_amp, thetamax;
     int loop, time;
+    double timed; /* time as a double (time-accurate mode) */
     /* grid */
     double *x, *y, *xix, *xiy, *etx, *ety, *alph, *beta, *gam, *jac;
     double *xnix, *xniy, *xnox, *xnoy;
@@ -449,6 +451,7 @@ static void initial_state(orc_case* c) {
     const size_t N = (size_t)n0 * n1;
     c->loop = 1;
     c->time = 0;
+    c->timed = 0.0;
     for (size_t k = 0; k < N; k++) {
         if (is_cav(c)) {
             c->u[k] = 0.0; c->v[k] = 0.0; c->T[k] = 0.0;
@@ -516,6 +519,9 @@ static void time_step(orc_case* c) {
     memcpy(c->vprev, c->v, N * sizeof(double));
 
     c->time = (int)((double)c->time + dt);
+    c->timed = c->timed + dt;
+    /* the time the wall motion sees: the reference's int (PSolver.cpp:186), or t = n dt */
+    const double tw = c->prm.time_accurate ? c->timed : (double)c->time;
 
     /* contravariant velocities, PSolver.cpp:1063-1069 */
     for (size_t k = 0; k < N; k++) {
@@ -827,9 +833,9 @@ static void time_step(orc_case* c) {
         /* wall velocity, PSolver.cpp:1617-1630 */
         for (int i = 0; i < n0; i++) {
             const size_t k = IX(i, 0);
-            c->u[k] = -c->speed_amp * cos(2.0 * Pi * c->prm.F * c->time) * c->y[k];
+            c->u[k] = -c->speed_amp * cos(2.0 * Pi * c->prm.F * tw) * c->y[k];
             c->up[k] = c->u[k];
-            c->v[k] = c->speed_amp * cos(2.0 * Pi * c->prm.F * c->time) * c->x[k];
+            c->v[k] = c->speed_amp * cos(2.0 * Pi * c->prm.F * tw) * c->x[k];
             c->vp[k] = c->v[k];
         }
         /* far-field u/v/T, PSolver.cpp:1632-1656 */
@@ -883,8 +889,8 @@ static void time_step(orc_case* c) {
                 double cv = c->uxi[k] * 0.5 * (f[IX(ipp, j)] - f[IX(inn, j)]) / d0;
                 cv = cv + c->uet[k] * (f[IX(i, jpp)] - f[k]) / d1;
                 double alc;
-                if (m == 0) alc = c->accn_amp * sin(2.0 * Pi * c->prm.F * c->time) * c->y[k];
-                else alc = -c->accn_amp * sin(2.0 * Pi * c->prm.F * c->time) * c->x[k];
+                if (m == 0) alc = c->accn_amp * sin(2.0 * Pi * c->prm.F * tw) * c->y[k];
+                else alc = -c->accn_amp * sin(2.0 * Pi * c->prm.F * tw) * c->x[k];
                 if (m == 0) dp_dx = 1.0 * d2u / Re - cv - alc;
                 if (m == 1) dp_dy = 1.0 * d2u / Re - cv - alc + Ri * c->T[k];
             }
@@ -1125,7 +1131,7 @@ int orc_step(orc_case* c, int nsteps, double* hist) {
     for (int s = 0; s < nsteps; s++) {
         time_step(c);
         c->diag[D_LOOP] = c->loop;
-        c->diag[D_TIME] = c->time;
+        c->diag[D_TIME] = c->prm.time_accurate ? c->timed : (double)c->time;
         c->loop++;
         if (hist) memcpy(hist + (size_t)s * D_COUNT, c->diag, D_COUNT * sizeof(double));
     }
