@@ -180,6 +180,30 @@ def cavity(n0: int, n1: int | None = None, skew: float = 0.1) -> Grid:
                 xnox=xnox, xnoy=xnoy, kind="cavity")
 
 
+def generate_on_device(kind: str, n0: int, n1: int | None = None, ar: float = 2.0,
+                       r_outer: float = 20.0, skew: float = 0.0) -> Grid:
+    """The grid of ogrid() / cavity(), generated on the GPU (cfd_grid_generate): the same
+    analytic map and metric formulas, evaluated by one thread per point."""
+    import ctypes
+    from . import _lib
+    n1 = n0 if n1 is None else n1
+    prof = _lib.PROFILE_OGRID if kind == "ogrid" else _lib.PROFILE_CAVITY
+    spec = _lib.CfdGridSpec(profile=prof, n0=n0, n1=n1, ar=ar, r_outer=r_outer, skew=skew)
+    planes = np.empty((10, n1, n0), dtype=np.float64)
+    normals = np.empty((4, n0), dtype=np.float64)
+    pd = ctypes.POINTER(ctypes.c_double)
+    _lib.check(_lib.lib().cfd_grid_generate(ctypes.byref(spec), planes.ctypes.data_as(pd),
+                                            normals.ctypes.data_as(pd)), "cfd_grid_generate")
+    f = {k: planes[q] for q, k in enumerate(FIELD_ORDER)}
+    if kind == "ogrid":
+        return Grid(n0=n0, n1=n1, dxi0=1.0 / (n0 - 1), dxi1=1.0 / (n1 - 1), p_grid=0.0,
+                    a_grid=float(r_outer), ar=float(ar), xnix=normals[0], xniy=normals[1],
+                    xnox=normals[2], xnoy=normals[3], kind="ogrid", **f)
+    return Grid(n0=n0, n1=n1, dxi0=1.0 / (n0 - 1), dxi1=1.0 / (n1 - 1), p_grid=0.0, a_grid=0.0,
+                ar=1.0, xnix=normals[0], xniy=normals[1], xnox=normals[2], xnoy=normals[3],
+                kind="cavity", **f)
+
+
 def write_inp(g: Grid, path: str | Path) -> None:
     """Write INP.DAT with round-trip (%.17g) precision."""
     n0, n1 = g.n0, g.n1

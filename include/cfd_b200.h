@@ -59,6 +59,17 @@ typedef struct cfd_grid {
     const double *xnix, *xniy, *xnox, *xnoy; /* n0 each */
 } cfd_grid;
 
+/* Analytic grid of a case, generated on the GPU by cfd_grid_generate (the reference reads
+ * its grid from INP.DAT, written by an external generator). */
+typedef struct cfd_grid_spec {
+    int profile;           /* CFD_PROFILE_OGRID: elliptic-cylinder O-grid; CFD_PROFILE_CAVITY */
+    int n0, n1;            /* grid points (O-grid: n0 >= 8, n1 >= 6; cavity: both >= 7) */
+    double ar;             /* O-grid semi-axis ratio (>= 1; 1 = circle): semi-axes 1 and 1/ar */
+    double r_outer;        /* O-grid far-field radius */
+    double skew;           /* skew amplitude s: O-grid mu = mu0 + L[eta + s eta(1-eta) sin 2 pi xi];
+                              cavity x = xi + s xi(1-xi) sin 2 pi eta, y = eta + s eta(1-eta) sin 2 pi xi */
+} cfd_grid_spec;
+
 /* Per-case parameters. cfd_params_default() gives the reference's values. */
 typedef struct cfd_params {
     double Re, Ri, Pr, F, alpha_deg, dt;  /* PSolver.cpp:160-174 */
@@ -235,6 +246,15 @@ int cfd_gauss_solve(int n0, int n1, int periodic, const double* const* coef, dou
 #define CFD_NOALLOC_MAX_POINTS (1 << 20)
 int cfd_gauss_solve_noalloc(int n0, int n1, int periodic, const double* const* coef, double* phi,
                             const double* q, double tol, int maxit, int* sweeps, void* stream);
+
+/* ---- grid generation on the GPU
+ * Generates the grid of `spec` on the current device (coordinates and metrics from the
+ * analytic map and its derivatives; the O-grid's seam column n0 - 1 repeats column 0) and
+ * copies it to host memory: `planes` gets 10 * n1 * n0 doubles, the planes x, y, xi_x, xi_y,
+ * eta_x, eta_y, alpha, beta, gamma, J in that order, each [j][i]; `normals` gets 4 * n0
+ * doubles: the inner and outer boundary normals xnix, xniy, xnox, xnoy (the INP.DAT blocks,
+ * PSolver.cpp:517-547). CFD_E_ARG for an invalid spec. */
+int cfd_grid_generate(const cfd_grid_spec* spec, double* planes, double* normals);
 
 /* ---- resident state snapshot (checkpoint / restart, host-owned stepping) ----
  * An image of every case's u, v, p, T, up, vp, int time, steps taken and the first-step
