@@ -4,9 +4,10 @@
 //   k_assemble_p     pressure 9-point stencil            PSolver.cpp:944-1040
 //   k_rhs            contravariant velocities,           PSolver.cpp:1063-1069
 //                    convection + predictor RHS          PSolver.cpp:1075-1237
-//   k_jac            the five gauss() systems            PSolver.cpp:1241-1350, 2280-2446
-//                    (u/v/T coefficients assembled in     PSolver.cpp:752-940
-//                     registers from alpha, beta, gamma)
+//   k_sweep_*        the five gauss() systems            PSolver.cpp:1241-1350, 2280-2446
+//   (cfd_sweep.cu)   (u/v/T coefficients assembled in     PSolver.cpp:752-940
+//                     shared memory from alpha, beta, gamma; k_sweep_fin, k_mom_fix,
+//                     k_mom_update finish each sweep / solve)
 //   k_upbc           up/vp far-field condition           PSolver.cpp:1356-1382
 //   k_face_q         face velocities -> continuity q     PSolver.cpp:1390-1449
 //   k_bicg_* / k_mg_*  pressure correction (replaces      PSolver.cpp:1453-1466, 2067-2278
@@ -731,14 +732,16 @@ __global__ void __launch_bounds__(NT, 5) k_bicg_x(BatchDev b, int maxit) {
 // ---------------------------------------------------------------------------
 // multigrid preconditioner, FP32, level tiles.
 //
-// One V-cycle: on the way down, level l is pre-smoothed from zero (k_mg_gs, post = 0:
-// writes x_l), then its residual is formed and restricted in one pass (k_mg_rr: writes
-// b_{l+1}); the coarsest level of each case is smoothed by one CTA (k_mg_coarse, in place
-// in x); on the way up, k_mg_gs (post = 1) adds the prolonged coarse result and
-// post-smooths in one pass, writing the level's result into its r plane. No kernel reads a
-// plane that another CTA of the same launch writes, so the V-cycle is a fixed linear map
-// (the same bits whatever the CTA schedule), as the Krylov method needs. The level's
-// final result lives in r (x for a case whose coarsest level it is).
+// One V-cycle: on the way down, level l is pre-smoothed from zero and its residual formed
+// and restricted into b_{l+1} -- either by k_mg_gs (mode 0: writes x_l) followed by
+// k_mg_rr, or (schedule form 2) by k_mg_prr in one pass over overlapping regions; then one
+// k_mg_coarse launch smooths every case's coarsest level (one CTA per case, in place in x);
+// on the way up, k_mg_gs (mode 2) adds the prolonged coarse result and post-smooths,
+// writing the level's result into its r plane. No kernel reads a plane that another CTA of
+// the same launch writes, so the V-cycle is a fixed linear map (the same bits whatever the
+// CTA schedule), as the Krylov method needs. The level's final result lives in r (x for a
+// case whose coarsest level it is).
+
 // stored column of level column gi, gi in [-W, inf): the periodic wrap without a division
 // in the common case (gi within one width of the level)
 __device__ __forceinline__ int mg_wrap(int gi, int W) {
