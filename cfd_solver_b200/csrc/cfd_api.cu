@@ -505,7 +505,8 @@ void enq_mid(cfd_batch* b, BatchDev& bd) {
     k_face_q<<<bd.njtiles, NT, kFaceQSmem, b->st>>>(bd);
 }
 // one BiCGStab iteration in two halves: up to the half-step exit (k_bicg_s), and the rest,
-// which the step graph skips when every case stopped at the half step
+// which the step graph skips when every case stopped at the half step. k_bicg_p forms the
+// iteration's direction (the first one, p_1 = r_0, is written by k_face_q).
 void enq_p_first(cfd_batch* b, BatchDev& bd) {
     const int nf = bd.njtiles;  // the BiCGStab kernels run on the 32 x 16 tiles
     { Prof pr(b, K_BICG_P); k_bicg_p<<<nf, NT, 0, b->st>>>(bd); }

@@ -489,6 +489,9 @@ __global__ void __launch_bounds__(NT, 4) k_face_q(BatchDev b) {
         const long long kg = (long long)j * ld + i;
         plane(b, c, P_Q)[kg] = q;
         plane(b, c, P_KR)[kg] = q;
+        // the first iteration's p = r_0 = q, as the preconditioner's right-hand side (k_bicg_p
+        // has nothing to do in the first iteration; the second reads p_1 from the q plane)
+        mplane(b, c.lev[0], M_B)[(long long)j * c.lev[0].ld + i] = (float)q;
         red[0] += fabs(q);
         red[1] += q * q;
         red[2] = fmax(red[2], fabs(q));
@@ -525,12 +528,17 @@ __global__ void __launch_bounds__(NT, 4) k_face_q(BatchDev b) {
 __global__ void __launch_bounds__(NT, 3) k_bicg_p(BatchDev b) {
     const Tile t = b.jtiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
-    const bool first = b.iscal[(long long)t.c * NISCAL + I_PIT] == 0;
+    // p_{k+1} = r_k + beta (p_k - omega v_k). In the first iteration there is nothing to do:
+    // p_1 = r_0 = q, which k_face_q has written as the preconditioner's right-hand side; the
+    // second iteration reads p_1 from the q plane.
+    const int it = b.iscal[(long long)t.c * NISCAL + I_PIT];
+    if (it == 0) return;
     const CaseDev& c = b.cases[t.c];
     const int i = t.i0 + (int)(threadIdx.x % TX), j0 = t.j0 + (int)(threadIdx.x / TX);
     const double* sc = b.scal + (long long)t.c * NSCAL;
     const double beta = sc[S_BETA], omega = sc[S_OMEGA];
     double* Pv = plane(b, c, P_KP);
+    const double* Pold = it == 1 ? plane(b, c, P_Q) : Pv;
     const double* R = plane(b, c, P_KR);
     const double* Vv = plane(b, c, P_KV);
     const LevelDev& L = c.lev[0];
@@ -543,14 +551,14 @@ __global__ void __launch_bounds__(NT, 3) k_bicg_p(BatchDev b) {
         in[h] = i >= c.ilo && i <= c.ihi && j <= c.n1 - 2;
         k[h] = in[h] ? (long long)j * c.ld + i : (long long)c.ld + c.ilo;
         r[h] = R[k[h]];
-        po[h] = first ? 0.0 : Pv[k[h]];
-        v[h] = first ? 0.0 : Vv[k[h]];
+        po[h] = Pold[k[h]];
+        v[h] = Vv[k[h]];
     }
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         if (!in[h]) continue;
         const int j = j0 + h * TY;
-        const double p = first ? r[h] : r[h] + beta * (po[h] - omega * v[h]);
+        const double p = r[h] + beta * (po[h] - omega * v[h]);
         Pv[k[h]] = p;
         mplane(b, L, M_B)[(long long)j * L.ld + i] = (float)p;
         store_mirrored(mplane(b, L, M_X), L.ld, i, j, L.W, c.periodic, 0.0f);
