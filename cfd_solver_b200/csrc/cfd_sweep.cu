@@ -406,28 +406,10 @@ __global__ void __launch_bounds__(SW_THREADS, 4) k_sweep_mx(BatchDev b) {
     else sweep_tile<SW_MX>(b, sm, bar);
 }
 
-// per case after every sweep launch: sum the tile partials in a fixed order, count the
-// sweep, decide the stop (after odd sweeps) and advance the Chebyshev weights
-__global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
-    __shared__ double red[NFIELD * 32];
-    const int cid = blockIdx.x;
-    const CaseDev& c = b.cases[cid];
-    int* is = b.iscal + (long long)cid * NISCAL;
-    int mask = 0;
-#pragma unroll
-    for (int f = 0; f < NFIELD; f++) mask |= (is[I_MDONE0 + f] == 0) << f;
-    if (cid == 0 && threadIdx.x == 0) atomicAdd(b.sweep_no, 1);  // read by the next sweep launch
-    if (!mask) return;
-    const int tid = threadIdx.x;
-    double v[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const int np = c.jt_count * SW_WARPS;
-    for (int e = tid; e < np; e += SWF_THREADS) {
-        const double* src = b.partial + ((long long)c.jt_begin * SW_WARPS + e) * PSTRIDE;
-#pragma unroll
-        for (int f = 0; f < NFIELD; f++) v[f] += src[f];
-    }
-    block_sum<NFIELD>(v, red);
-    if (tid != 0) return;
+// the case's bookkeeping after a sweep (thread 0 of k_sweep_fin): stop decisions, the next
+// Chebyshev weights, the sweep kernel's word (returned through *word) and the traffic counters
+__device__ __noinline__ void fin_case(const BatchDev& b, const CaseDev& c, int cid, int* is, int mask,
+                                      const double (&v)[NFIELD], int* word) {
     double* scw = b.scal + (long long)cid * NSCAL;
     const int sweep = is[I_MIT0 + (__ffs(mask) - 1)];
     // the rule is tested after every sweep (on the residual of the sweep's input iterate; the
@@ -459,7 +441,7 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
     for (int f = 0; f < NFIELD; f++) nmask |= (is[I_MDONE0 + f] == 0) << f;
     const int nword = nmask | (is[I_MWORD] & (((1 << NFIELD) - 1) << NFIELD)) | ((sweep + 1) << (2 * NFIELD));
     is[I_MWORD] = nword;
-    for (int k = 0; k < c.jt_count; k++) b.tword[c.jt_begin + k] = nword;
+    *word = nword;
     for (int ty = 0; ty < 2; ty++) {  // Chebyshev weight of the next sweep
         const double ca = c.cheb_a[ty], cb = c.cheb_b[ty];
         const double s2 = ((cb + ca) / (cb - ca)) * ((cb + ca) / (cb - ca));
@@ -473,6 +455,38 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
     if (sweep == 0) atomicAdd(&b.work[2], nf);
     if (sweep == 1) atomicAdd(&b.work[3], nf);
 }
+
+// per case after every sweep launch: sum the tile partials in a fixed order, count the
+// sweep, decide the stop (after every sweep), advance the Chebyshev weights, and hand every
+// tile of the case the sweep kernel's new word (the stores spread over the CTA's threads:
+// a 1025 x 1025 case has 2,048 tiles)
+__global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
+    __shared__ double red[NFIELD * 32];
+    __shared__ int s_word;
+    const int cid = blockIdx.x;
+    const CaseDev& c = b.cases[cid];
+    int* is = b.iscal + (long long)cid * NISCAL;
+    int mask = 0;
+#pragma unroll
+    for (int f = 0; f < NFIELD; f++) mask |= (is[I_MDONE0 + f] == 0) << f;
+    if (cid == 0 && threadIdx.x == 0) atomicAdd(b.sweep_no, 1);  // read by the next sweep launch
+    if (!mask) return;
+    const int tid = threadIdx.x;
+    double v[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const int np = c.jt_count * SW_WARPS;
+    for (int e = tid; e < np; e += SWF_THREADS) {
+        const double* src = b.partial + ((long long)c.jt_begin * SW_WARPS + e) * PSTRIDE;
+#pragma unroll
+        for (int f = 0; f < NFIELD; f++) v[f] += src[f];
+    }
+    block_sum<NFIELD>(v, red);
+    if (tid == 0) fin_case(b, c, cid, is, mask, v, &s_word);
+    __syncthreads();
+    // the new word into every tile of the case, by all threads
+    const int nword = s_word;
+    for (int k = tid; k < c.jt_count; k += SWF_THREADS) b.tword[c.jt_begin + k] = nword;
+}
+
 
 size_t sweep_smem_f64() { return (size_t)SwLayout<SW_F64>::TOTAL + 128; }
 size_t sweep_smem_mx() { return (size_t)max(SwLayout<SW_MX0>::TOTAL, SwLayout<SW_MX>::TOTAL) + 128; }
