@@ -193,6 +193,7 @@ struct cfd_batch {
     int mg_pre = 1, mg_post = 3;  // multigrid sweeps before / after the coarse correction
     int mg_fused = 2;             // 1: a smoothing phase's sweeps in one launch; 2: and the
                                   // pre-smoothing inside the residual + restriction launch
+    int swf_threads = 128;  // k_sweep_fin CTA size: 512 when a case has >= 1024 tiles
     int max_W = 0;
     int cur = 0;
     long long steps_done = 0;
@@ -486,7 +487,7 @@ void enq_mom_pair(cfd_batch* b, BatchDev& bd) {
             else k_sweep_f64<<<b->sw_grid, SW_THREADS, b->sw_smem, b->st>>>(bd);
         }
         Prof pr(b, K_SWEEP_FIN);
-        k_sweep_fin<<<b->n, SWF_THREADS, 0, b->st>>>(bd);
+        k_sweep_fin<<<b->n, b->swf_threads, 0, b->st>>>(bd);
     }
 }
 void enq_mid(cfd_batch* b, BatchDev& bd) {
@@ -976,6 +977,9 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         CK(cudaFuncSetAttribute(swk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->sw_smem));
         CK(cudaFuncSetAttribute(swk, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         b->sw_grid = (int)jtiles.size();  // one CTA per 32 x 16 tile
+        int jt_max = 0;
+        for (const auto& d : b->hc) jt_max = std::max(jt_max, d.jt_count);
+        b->swf_threads = jt_max >= 1024 ? SWF_THREADS : 128;
         CK(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem));
         CK(cudaFuncSetAttribute(k_face_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFaceQSmem));
     }

@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
     const int tid = threadIdx.x;
     double v[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const int np = c.jt_count * SW_WARPS;
-    for (int e = tid; e < np; e += SWF_THREADS) {
+    for (int e = tid; e < np; e += blockDim.x) {
         const double* src = b.partial + ((long long)c.jt_begin * SW_WARPS + e) * PSTRIDE;
 #pragma unroll
         for (int f = 0; f < NFIELD; f++) v[f] += src[f];
@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
     __syncthreads();
     // the new word into every tile of the case, by all threads
     const int nword = s_word;
-    for (int k = tid; k < c.jt_count; k += SWF_THREADS) b.tword[c.jt_begin + k] = nword;
+    for (int k = tid; k < c.jt_count; k += blockDim.x) b.tword[c.jt_begin + k] = nword;
 }
 
 

@@ -7,7 +7,8 @@ enum SweepMode { SW_F64 = 0, SW_MX0 = 1, SW_MX = 2 };
 constexpr int SW_WARPS = 4;                       // warps per CTA (one 32 x 16 tile)
 constexpr int SW_THREADS = 32 * SW_WARPS;
 constexpr int SW_ROWS = TYJ / SW_WARPS;           // rows of the tile per thread
-constexpr int SWF_THREADS = 128;                  // per-case finalisation
+constexpr int SWF_THREADS = 512;                  // per-case finalisation, most threads (a batch with a
+                                                   // case of >= 1024 tiles; 128 otherwise)
 
 __global__ void k_sweep_f64(BatchDev b);
 __global__ void k_sweep_mx(BatchDev b);
