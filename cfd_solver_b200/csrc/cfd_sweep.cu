@@ -406,24 +406,53 @@ __global__ void __launch_bounds__(SW_THREADS, 4) k_sweep_mx(BatchDev b) {
     else sweep_tile<SW_MX>(b, sm, bar);
 }
 
+// What the case's bookkeeping after a sweep reads, loaded by thread 0 of k_sweep_fin at its
+// start so that the loads overlap the partial sums (the sweep count, the fields still
+// iterating and their start planes come from the case's packed word).
+struct FinIn {
+    double mr0[NFIELD];   // first-sweep residuals (the rule's reference)
+    double cw[2];         // Chebyshev weights of the sweep just done
+    double ca[2], cb[2];  // eigenvalue bounds (u-type, T)
+    double tol, atol;
+    unsigned long long ncell;
+};
+
+__device__ __forceinline__ void fin_load(const BatchDev& b, const CaseDev& c, int cid, FinIn& in) {
+    const double* scw = b.scal + (long long)cid * NSCAL;
+#pragma unroll
+    for (int f = 0; f < NFIELD; f++) in.mr0[f] = scw[S_MR0 + f];
+#pragma unroll
+    for (int ty = 0; ty < 2; ty++) {
+        in.cw[ty] = scw[S_CW0 + ty];
+        in.ca[ty] = c.cheb_a[ty];
+        in.cb[ty] = c.cheb_b[ty];
+    }
+    in.tol = c.tol_mom;
+    in.atol = c.atol_mom;
+    in.ncell = (unsigned long long)(c.ihi - c.ilo + 1) * (c.n1 - 2);
+}
+
 // the case's bookkeeping after a sweep (thread 0 of k_sweep_fin): stop decisions, the next
-// Chebyshev weights, the sweep kernel's word (returned through *word) and the traffic counters
-__device__ __noinline__ void fin_case(const BatchDev& b, const CaseDev& c, int cid, int* is, int mask,
-                                      const double (&v)[NFIELD], int* word) {
+// Chebyshev weights, the sweep kernel's new word (returned) and the traffic counters
+__device__ __forceinline__ int fin_case(const BatchDev& b, int cid, int* is, int word, const double (&v)[NFIELD],
+                                        const FinIn& in) {
     double* scw = b.scal + (long long)cid * NSCAL;
-    const int sweep = is[I_MIT0 + (__ffs(mask) - 1)];
+    const int mask = word & ((1 << NFIELD) - 1), flipm = (word >> NFIELD) & ((1 << NFIELD) - 1);
+    const int sweep = word >> (2 * NFIELD);
+    int nmask = mask;
     // the rule is tested after every sweep (on the residual of the sweep's input iterate; the
-    // sweep's output, one sweep further, is the result). After an odd number of sweeps the
-    // result sits in the scratch plane: the flag tells k_mom_fix / k_mom_update where
+    // sweep's output, one sweep further, is the result)
+#pragma unroll
     for (int f = 0; f < NFIELD; f++) {
         if (!(mask & (1 << f))) continue;
+        const double mr0 = sweep == 0 ? ((v[f] != 0.0) ? v[f] : 1.0) : in.mr0[f];
         if (sweep == 0) {
-            scw[S_MR0 + f] = (v[f] != 0.0) ? v[f] : 1.0;
+            scw[S_MR0 + f] = mr0;
             is[I_MNEXT0 + f] = 0;  // next step: start in the iterate plane, unless this solve stops odd
         }
         scw[S_MR + f] = v[f];
-        is[I_MIT0 + f] += 1;
-        bool done = (v[f] / scw[S_MR0 + f] < c.tol_mom) || (v[f] <= c.atol_mom);
+        is[I_MIT0 + f] = sweep + 1;
+        bool done = (v[f] / mr0 < in.tol) || (v[f] <= in.atol);
         if (!isfinite(v[f])) {
             is[I_STATUS] |= ST_NAN;
             done = true;
@@ -432,28 +461,27 @@ __device__ __noinline__ void fin_case(const BatchDev& b, const CaseDev& c, int c
             // the result x_{sweep+1} is in the scratch plane when the sweep's parity equals
             // the solve's start plane flag; predict the next step's start from this parity
             is[I_MDONE0 + f] = 1;
-            is[I_MODD0 + f] = (sweep & 1) == (is[I_MFLIP0 + f] != 0);
+            is[I_MODD0 + f] = (sweep & 1) == ((flipm >> f) & 1);
             is[I_MNEXT0 + f] = (sweep & 1) == 0;
             atomicSub(b.mactive, 1);
+            nmask &= ~(1 << f);
         }
     }
-    int nmask = 0;  // the sweep kernel's word: fields still iterating, start planes, sweeps done
-    for (int f = 0; f < NFIELD; f++) nmask |= (is[I_MDONE0 + f] == 0) << f;
-    const int nword = nmask | (is[I_MWORD] & (((1 << NFIELD) - 1) << NFIELD)) | ((sweep + 1) << (2 * NFIELD));
+    const int nword = nmask | (flipm << NFIELD) | ((sweep + 1) << (2 * NFIELD));
     is[I_MWORD] = nword;
-    *word = nword;
+#pragma unroll
     for (int ty = 0; ty < 2; ty++) {  // Chebyshev weight of the next sweep
-        const double ca = c.cheb_a[ty], cb = c.cheb_b[ty];
+        const double ca = in.ca[ty], cb = in.cb[ty];
         const double s2 = ((cb + ca) / (cb - ca)) * ((cb + ca) / (cb - ca));
-        scw[S_CW0 + ty] = (sweep == 0) ? 1.0 / (1.0 - 1.0 / (2.0 * s2)) : 1.0 / (1.0 - scw[S_CW0 + ty] / (4.0 * s2));
+        scw[S_CW0 + ty] = (sweep == 0) ? 1.0 / (1.0 - 1.0 / (2.0 * s2)) : 1.0 / (1.0 - in.cw[ty] / (4.0 * s2));
     }
     // algorithmic-traffic counters (cells and field-cells swept)
-    const unsigned long long ncell = (unsigned long long)(c.ihi - c.ilo + 1) * (c.n1 - 2);
-    const unsigned long long nf = (unsigned long long)__popc(mask) * ncell;
+    const unsigned long long nf = (unsigned long long)__popc(mask) * in.ncell;
     atomicAdd(&b.work[0], nf);
-    atomicAdd(&b.work[1], ncell);
+    atomicAdd(&b.work[1], in.ncell);
     if (sweep == 0) atomicAdd(&b.work[2], nf);
     if (sweep == 1) atomicAdd(&b.work[3], nf);
+    return nword;
 }
 
 // per case after every sweep launch: sum the tile partials in a fixed order, count the
@@ -466,12 +494,12 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
     const int cid = blockIdx.x;
     const CaseDev& c = b.cases[cid];
     int* is = b.iscal + (long long)cid * NISCAL;
-    int mask = 0;
-#pragma unroll
-    for (int f = 0; f < NFIELD; f++) mask |= (is[I_MDONE0 + f] == 0) << f;
+    const int word = is[I_MWORD];
     if (cid == 0 && threadIdx.x == 0) atomicAdd(b.sweep_no, 1);  // read by the next sweep launch
-    if (!mask) return;
+    if (!(word & ((1 << NFIELD) - 1))) return;
     const int tid = threadIdx.x;
+    FinIn in;
+    if (tid == 0) fin_load(b, c, cid, in);
     double v[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const int np = c.jt_count * SW_WARPS;
     for (int e = tid; e < np; e += blockDim.x) {
@@ -480,7 +508,7 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
         for (int f = 0; f < NFIELD; f++) v[f] += src[f];
     }
     block_sum<NFIELD>(v, red);
-    if (tid == 0) fin_case(b, c, cid, is, mask, v, &s_word);
+    if (tid == 0) s_word = fin_case(b, cid, is, word, v, in);
     __syncthreads();
     // the new word into every tile of the case, by all threads
     const int nword = s_word;
