@@ -371,7 +371,9 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
         }
         return;
     }
-    // the warp's partial L1 residuals of this tile (summed per case by k_sweep_fin)
+    // the tile's partial L1 residuals, one row per tile (summed per case by k_sweep_fin):
+    // warps, then the tile's four warps in a fixed order through the first field buffer,
+    // free once every field has been read and no copy is in flight
 #pragma unroll
     for (int ff = 0; ff < NFIELD; ff++) {
         double x = r[ff];
@@ -379,10 +381,18 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         r[ff] = x;
     }
+    double* red = reinterpret_cast<double*>(sm);
+    __syncthreads();
     if (lane == 0) {
-        double* dstp = b.partial + ((long long)blockIdx.x * SW_WARPS + wrp) * PSTRIDE;
 #pragma unroll
-        for (int ff = 0; ff < NFIELD; ff++) dstp[ff] = r[ff];
+        for (int ff = 0; ff < NFIELD; ff++) red[wrp * NFIELD + ff] = r[ff];
+    }
+    __syncthreads();
+    if (tid < NFIELD) {
+        double x = 0.0;
+#pragma unroll
+        for (int w = 0; w < SW_WARPS; w++) x += red[w * NFIELD + tid];
+        b.partial[(long long)blockIdx.x * PSTRIDE + tid] = x;
     }
 }
 
@@ -484,7 +494,7 @@ __device__ __forceinline__ int fin_case(const BatchDev& b, int cid, int* is, int
     return nword;
 }
 
-// per case after every sweep launch: sum the tile partials in a fixed order, count the
+// per case after every sweep launch: sum the tile rows in a fixed order, count the
 // sweep, decide the stop (after every sweep), advance the Chebyshev weights, and hand every
 // tile of the case the sweep kernel's new word (the stores spread over the CTA's threads:
 // a 1025 x 1025 case has 2,048 tiles)
@@ -501,9 +511,9 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
     FinIn in;
     if (tid == 0) fin_load(b, c, cid, in);
     double v[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const int np = c.jt_count * SW_WARPS;
+    const int np = c.jt_count;  // one row per tile
     for (int e = tid; e < np; e += blockDim.x) {
-        const double* src = b.partial + ((long long)c.jt_begin * SW_WARPS + e) * PSTRIDE;
+        const double* src = b.partial + ((long long)c.jt_begin + e) * PSTRIDE;
 #pragma unroll
         for (int f = 0; f < NFIELD; f++) v[f] += src[f];
     }
