@@ -769,7 +769,11 @@ int plane_id(const char* name, int cur) {
 }  // namespace
 
 // Grid, normals, initial state, descriptor and per-case scalars of case `c` (a slot of the
-// batch); with `setup` also its pressure stencil and multigrid hierarchy.
+// batch); with `setup` also its pressure stencil and multigrid hierarchy. Every copy goes on
+// the batch's stream: that stream is non-blocking, so a copy on the legacy default stream
+// would not be ordered before the kernels that read it (a synchronous copy from pageable
+// memory may return before its DMA lands). From pageable memory the call returns once the
+// source is staged, so the host vectors may be reused or freed right after it.
 int upload_case(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, bool setup) {
     CaseDev& d = b->hc[c];
     case_params_to_dev(d, g, p);
@@ -777,8 +781,8 @@ int upload_case(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, boo
     std::vector<double> pad;
     auto put = [&](int plane_id, const double* src) -> int {
         pad_plane(d, src, pad);
-        CK(cudaMemcpy(b->f64 + d.base + H - 16 + (long long)plane_id * d.ps, pad.data(), sizeof(double) * d.ps,
-                      cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(b->f64 + d.base + H - 16 + (long long)plane_id * d.ps, pad.data(), sizeof(double) * d.ps,
+                           cudaMemcpyHostToDevice, b->st));
         return CFD_OK;
     };
     const double* gp[10] = {g.x, g.y, g.xix, g.xiy, g.etx, g.ety, g.alph, g.beta, g.gam, g.jac};
@@ -795,12 +799,12 @@ int upload_case(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, boo
     const int sid[6] = {P_U, P_V, P_T0 + b->cur, P_UP0 + b->cur, P_VP0 + b->cur, P_P};
     for (int m = 0; m < 6; m++)
         if (int rc = put(sid[m], st[m].data())) return rc;
-    CK(cudaMemcpy(b->dc + c, &d, sizeof(CaseDev), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(b->dc + c, &d, sizeof(CaseDev), cudaMemcpyHostToDevice, b->st));
     std::vector<double> sc(NSCAL, 0.0);
     std::vector<int> is(NISCAL, 0);
     is[I_ACTIVE] = 1;
-    CK(cudaMemcpy(b->scal + (size_t)c * NSCAL, sc.data(), sizeof(double) * NSCAL, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->iscal + (size_t)c * NISCAL, is.data(), sizeof(int) * NISCAL, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(b->scal + (size_t)c * NSCAL, sc.data(), sizeof(double) * NSCAL, cudaMemcpyHostToDevice, b->st));
+    CK(cudaMemcpyAsync(b->iscal + (size_t)c * NISCAL, is.data(), sizeof(int) * NISCAL, cudaMemcpyHostToDevice, b->st));
     if (setup) {
         BatchDev bd = b->bd;
         k_assemble_p<<<d.tile_count, NT, 0, b->st>>>(bd, d.tile_begin);
@@ -998,10 +1002,10 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         pos_cc[l] = allcc.size();
         allcc.insert(allcc.end(), cc[l].begin(), cc[l].end());
     }
-    CK(cudaMemcpy(b->dtiles, all.data(), sizeof(Tile) * all.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(b->dtiles, all.data(), sizeof(Tile) * all.size(), cudaMemcpyHostToDevice, b->st));
     if (!allcc.empty())
-        CK(cudaMemcpy(b->dcc, allcc.data(), sizeof(int) * allcc.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->dc, b->hc.data(), sizeof(CaseDev) * ncases, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(b->dcc, allcc.data(), sizeof(int) * allcc.size(), cudaMemcpyHostToDevice, b->st));
+    CK(cudaMemcpyAsync(b->dc, b->hc.data(), sizeof(CaseDev) * ncases, cudaMemcpyHostToDevice, b->st));
 
     BatchDev& bd = b->bd;
     bd.cases = b->dc; bd.ncases = ncases; bd.f64 = b->f64; bd.f32 = b->f32;
@@ -1043,7 +1047,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
             if (r != CUDA_SUCCESS)
                 return cleanup(fail(CFD_E_CUDA, "cuTensorMapEncodeTiled failed for case " + std::to_string(c)));
         }
-        CK(cudaMemcpy(b->dtmaps, maps.data(), maps.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(b->dtmaps, maps.data(), maps.size(), cudaMemcpyHostToDevice, b->st));
     }
     bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
     bd.jtiles = b->dtiles + pos_jt; bd.njtiles = (int)jtiles.size();
@@ -1325,7 +1329,7 @@ static int state_copy(cfd_batch* b, void* host, size_t bytes, bool to_host) {
         }
         CK(cudaMalloc((void**)&b->stage, need));
         CK(cudaMalloc((void**)&b->stage_off, sizeof(long long) * b->n));
-        CK(cudaMemcpy(b->stage_off, off.data(), sizeof(long long) * b->n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(b->stage_off, off.data(), sizeof(long long) * b->n, cudaMemcpyHostToDevice, b->st));
     }
     b->bd.cur = b->cur;
     if (to_host) {
