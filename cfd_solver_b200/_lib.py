@@ -30,7 +30,8 @@ SYMBOLS = ("cfd_params_default", "cfd_last_error", "cfd_device_count", "cfd_set_
            "cfd_batch_state_bytes", "cfd_batch_get_state", "cfd_batch_set_state",
            "cfd_gauss_solve", "cfd_gauss_solve_noalloc", "cfd_batch_fetch_stats", "cfd_batch_admit",
            "cfd_batch_set_active", "cfd_serve", "cfd_batch_set_mg", "cfd_batch_get_mg",
-           "cfd_batch_autotune", "cfd_batch_save", "cfd_batch_load", "cfd_grid_generate")
+           "cfd_batch_autotune", "cfd_batch_save", "cfd_batch_load", "cfd_grid_generate",
+           "cfd_batch_admit_spec")
 
 _D = ctypes.c_double
 _PD = ctypes.POINTER(ctypes.c_double)
@@ -160,6 +161,7 @@ def lib():
     L.cfd_batch_save.argtypes = [vp, ctypes.c_char_p]
     L.cfd_batch_load.argtypes = [vp, ctypes.c_char_p]
     L.cfd_grid_generate.argtypes = [ctypes.POINTER(CfdGridSpec), _PD, _PD]
+    L.cfd_batch_admit_spec.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CfdGridSpec), ctypes.POINTER(CfdParams)]
     L.cfd_serve.argtypes = [ctypes.POINTER(CfdServeConfig), ctypes.POINTER(CfdRequest), ctypes.c_int,
                             ctypes.POINTER(CfdResult), ctypes.POINTER(CfdServeStats)]
     special = {"cfd_params_default", "cfd_last_error", "cfd_case_bytes", "cfd_batch_stream",

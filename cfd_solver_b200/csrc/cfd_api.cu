@@ -301,20 +301,27 @@ void unpad_plane(const CaseDev& c, const double* padded, double* out) {
     }
 }
 
-int check_params(const cfd_grid* g, const cfd_params* p) {
-    if (!g || !p) return fail(CFD_E_ARG, "null grid or params");
+// the checks of a case's parameters that do not read its grid
+int check_case_params(const cfd_params* p) {
+    if (!p) return fail(CFD_E_ARG, "null params");
     if (p->profile != CFD_PROFILE_OGRID && p->profile != CFD_PROFILE_CAVITY)
         return fail(CFD_E_ARG, "unknown profile");
+    if (!(p->dt > 0) || !(p->Re > 0) || !(p->Pr > 0)) return fail(CFD_E_ARG, "dt, Re, Pr must be > 0");
+    if (p->maxit_mom < 2 || p->maxit_p < 1) return fail(CFD_E_ARG, "iteration caps too small");
+    if (p->precision != CFD_PRECISION_FP64 && p->precision != CFD_PRECISION_MIXED)
+        return fail(CFD_E_ARG, "unknown precision");
+    return CFD_OK;
+}
+
+int check_params(const cfd_grid* g, const cfd_params* p) {
+    if (!g || !p) return fail(CFD_E_ARG, "null grid or params");
+    if (int rc = check_case_params(p)) return rc;
     if (g->n0 < 8 || g->n1 < 6) return fail(CFD_E_ARG, "grid too small (need n0 >= 8, n1 >= 6)");
     if (g->n0 > 8192 || g->n1 > 8192) return fail(CFD_E_ARG, "grid too large (n0, n1 <= 8192)");
     if (!(g->dxi0 > 0) || !(g->dxi1 > 0)) return fail(CFD_E_ARG, "non-positive grid spacing");
     if (!g->x || !g->y || !g->xix || !g->xiy || !g->etx || !g->ety || !g->alph || !g->beta ||
         !g->gam || !g->jac || !g->xnix || !g->xniy || !g->xnox || !g->xnoy)
         return fail(CFD_E_ARG, "missing grid plane");
-    if (!(p->dt > 0) || !(p->Re > 0) || !(p->Pr > 0)) return fail(CFD_E_ARG, "dt, Re, Pr must be > 0");
-    if (p->maxit_mom < 2 || p->maxit_p < 1) return fail(CFD_E_ARG, "iteration caps too small");
-    if (p->precision != CFD_PRECISION_FP64 && p->precision != CFD_PRECISION_MIXED)
-        return fail(CFD_E_ARG, "unknown precision");
     const size_t N = (size_t)g->n0 * g->n1;
     for (size_t k = 0; k < N; k++) {
         if (!(g->alph[k] > 0) || !(g->gam[k] > 0) || !std::isfinite(g->beta[k]) || !std::isfinite(g->jac[k]))
@@ -370,27 +377,133 @@ void initial_state(const cfd_grid* g, const cfd_params* p, const CaseDev& c, std
 // bounds the top: 1 + ((17/6) E + 4.5 |beta| dt/(Re dxi0 dxi1)) / (1 + 2.5 E); the 9-point
 // rows lie inside both. Margins: 0.9 below, 1.05 above. T uses Re*Pr; the reference's T
 // slot bug (atnw for annw) adds 7/9 |beta| c to the off-diagonal sum.
-void cheb_bounds(const cfd_grid& g, const cfd_params& p, CaseDev& d) {
-    const int n0 = g.n0, n1 = g.n1;
+// Per-system constants of the bound scan: dt/scale, the cross-term factor, dt/(scale dxi0
+// dxi1), dxi0^2, dxi1^2 (index 0: u, v, up, vp with scale Re; 1: T with scale Re Pr).
+struct ChebScan {
+    double dts[2], cross[2], cc[2], d00, d11;
+};
+
+ChebScan cheb_consts(const cfd_params& p, double dxi0, double dxi1) {
+    ChebScan cs;
     for (int ty = 0; ty < 2; ty++) {
         const double scale = ty == 0 ? p.Re : p.Re * p.Pr;
-        const double cross = (ty == 1 && !p.fix_T_annw) ? 4.5 + 7.0 / 9.0 : 4.5;
-        const double cc = p.dt / (scale * g.dxi0 * g.dxi1);
-        double emax = 0.0, rmax = 0.0;
-        for (int j = 1; j < n1 - 1; j++)
-            for (int i = 0; i < n0; i++) {
-                const size_t k = (size_t)j * n0 + i;
-                const double E = p.dt / scale * (g.alph[k] / (g.dxi0 * g.dxi0) + g.gam[k] / (g.dxi1 * g.dxi1));
-                emax = std::max(emax, E);
-                rmax = std::max(rmax, ((17.0 / 6.0) * E + cross * std::fabs(g.beta[k]) * cc) / (1.0 + 2.5 * E));
-            }
-        d.cheb_a[ty] = 0.9 / (1.0 + 2.5 * emax);
-        d.cheb_b[ty] = 1.05 * (1.0 + rmax);
+        cs.dts[ty] = p.dt / scale;
+        cs.cross[ty] = (ty == 1 && !p.fix_T_annw) ? 4.5 + 7.0 / 9.0 : 4.5;
+        cs.cc[ty] = p.dt / (scale * dxi0 * dxi1);
+    }
+    cs.d00 = dxi0 * dxi0;
+    cs.d11 = dxi1 * dxi1;
+    return cs;
+}
+
+void cheb_finish(const double* emax, const double* rmax, CaseDev& d) {
+    for (int ty = 0; ty < 2; ty++) {
+        d.cheb_a[ty] = 0.9 / (1.0 + 2.5 * emax[ty]);
+        d.cheb_b[ty] = 1.05 * (1.0 + rmax[ty]);
     }
 }
 
-// physics, numerics and Chebyshev bounds of one case into its descriptor
-void case_params_to_dev(CaseDev& d, const cfd_grid& g, const cfd_params& p) {
+void cheb_bounds(const cfd_grid& g, const cfd_params& p, CaseDev& d) {
+    const int n0 = g.n0, n1 = g.n1;
+    const ChebScan cs = cheb_consts(p, g.dxi0, g.dxi1);
+    double emax[2], rmax[2];
+    for (int ty = 0; ty < 2; ty++) {
+        emax[ty] = 0.0;
+        rmax[ty] = 0.0;
+        for (int j = 1; j < n1 - 1; j++)
+            for (int i = 0; i < n0; i++) {
+                const size_t k = (size_t)j * n0 + i;
+                const double E = cs.dts[ty] * (g.alph[k] / cs.d00 + g.gam[k] / cs.d11);
+                emax[ty] = std::max(emax[ty], E);
+                rmax[ty] = std::max(rmax[ty], ((17.0 / 6.0) * E + cs.cross[ty] * std::fabs(g.beta[k]) * cs.cc[ty]) /
+                                                  (1.0 + 2.5 * E));
+            }
+    }
+    cheb_finish(emax, rmax, d);
+}
+
+// The bound scan of cheb_bounds() over a grid that is in device memory (the 10 planes
+// of a generated grid), with each product, quotient and sum rounded on its own as the
+// host evaluates them, so both give the same bits. Also counts the points whose metrics
+// are invalid (the test of check_params()). The maxima are of non-negative doubles, so
+// they are taken on the bit patterns as unsigned integers. out: emax[2], rmax[2] (bit
+// patterns), invalid points; zeroed by the caller.
+constexpr int SCAN_THREADS = 256;
+__global__ void __launch_bounds__(SCAN_THREADS) k_grid_scan(const double* planes, int n0, int n1, ChebScan cs,
+                                                            unsigned long long* out) {
+    const long long np = (long long)n0 * n1;
+    const double* alph = planes + (long long)P_ALPH * np;
+    const double* beta = planes + (long long)P_BETA * np;
+    const double* gam = planes + (long long)P_GAM * np;
+    const double* jac = planes + (long long)P_JAC * np;
+    double em[2] = {0.0, 0.0}, rm[2] = {0.0, 0.0};
+    unsigned long long bad = 0;
+    for (long long k = (long long)blockIdx.x * SCAN_THREADS + threadIdx.x; k < np;
+         k += (long long)gridDim.x * SCAN_THREADS) {
+        const double a = alph[k], g = gam[k], be = beta[k];
+        if (!(a > 0) || !(g > 0) || !isfinite(be) || !isfinite(jac[k])) bad++;
+        const int j = (int)(k / n0);
+        if (j < 1 || j > n1 - 2) continue;
+        const double sm = __dadd_rn(__ddiv_rn(a, cs.d00), __ddiv_rn(g, cs.d11));
+#pragma unroll
+        for (int ty = 0; ty < 2; ty++) {
+            const double E = __dmul_rn(cs.dts[ty], sm);
+            const double num = __dadd_rn(__dmul_rn(17.0 / 6.0, E), __dmul_rn(__dmul_rn(cs.cross[ty], fabs(be)), cs.cc[ty]));
+            const double r = __ddiv_rn(num, __dadd_rn(1.0, __dmul_rn(2.5, E)));
+            em[ty] = fmax(em[ty], E);
+            rm[ty] = fmax(rm[ty], r);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int ty = 0; ty < 2; ty++) {
+            em[ty] = fmax(em[ty], __shfl_xor_sync(0xffffffffu, em[ty], o));
+            rm[ty] = fmax(rm[ty], __shfl_xor_sync(0xffffffffu, rm[ty], o));
+        }
+        bad += __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int ty = 0; ty < 2; ty++) {
+            atomicMax(out + ty, (unsigned long long)__double_as_longlong(em[ty]));
+            atomicMax(out + 2 + ty, (unsigned long long)__double_as_longlong(rm[ty]));
+        }
+        if (bad) atomicAdd(out + 4, bad);
+    }
+}
+
+// Writes a generated grid (10 planes of [n1][n0], then 4 rows of n0 normals) into a case's
+// padded planes the way pad_plane() does on the host: `region` is the start of the case's
+// plane 0 (plane q at region + q * ps, point (j, i) at 16 + j * ld + i); for a periodic case
+// padded columns -H..W+H-1 take source column i mod W; normals go to rows 0..3 of P_VEC,
+// zero in the other rows. The planes' other entries are zeroed by the caller.
+__global__ void k_grid_to_slot(const double* gen, int n0, int n1, int W, int periodic, double* region,
+                               long long ps, int ld) {
+    const int ncols = periodic ? W + 2 * H : n0;
+    const long long per = (long long)n1 * ncols;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 11 * per) return;
+    const int q = (int)(e / per);
+    const long long r = e - q * per;
+    const int j = (int)(r / ncols), cpad = (int)(r % ncols);
+    const int col = periodic ? cpad - H : cpad;
+    const int i = col < 0 ? col + W : (col >= W ? col - W : col);
+    const long long np = (long long)n0 * n1;
+    double v;
+    if (q < 10)
+        v = gen[q * np + (long long)j * n0 + i];
+    else
+        v = j < 4 ? gen[10 * np + (long long)j * n0 + i] : 0.0;
+    const int pid = q < 10 ? q : P_VEC;
+    region[(long long)pid * ps + 16 + (long long)j * ld + col] = v;
+}
+
+static_assert(P_X == 0 && P_Y == 1 && P_XIX == 2 && P_XIY == 3 && P_ETX == 4 && P_ETY == 5 && P_ALPH == 6 &&
+                  P_BETA == 7 && P_GAM == 8 && P_JAC == 9,
+              "grid planes 0..9 in the order of cfd_grid_generate's planes");
+
+// physics and numerics of one case into its descriptor (all but the Chebyshev bounds)
+void case_scalars_to_dev(CaseDev& d, double dxi0, double dxi1, double ar, const cfd_params& p) {
+    const cfd_grid g{0, 0, dxi0, dxi1, 0.0, 0.0, ar};
     d.fix_T_annw = p.fix_T_annw; d.fix_circ_de = p.fix_circ_de; d.warm_up = p.warm_start;
     d.time_accurate = p.time_accurate != 0;
     d.d0 = g.dxi0; d.d1 = g.dxi1; d.dt = p.dt; d.Re = p.Re; d.Pr = p.Pr; d.Ri = p.Ri; d.F = p.F;
@@ -407,6 +520,11 @@ void case_params_to_dev(CaseDev& d, const cfd_grid& g, const cfd_params& p) {
     d.pc1 = 1.0 / (2.0 * g.dxi0 * g.dxi0);
     d.pc2 = 1.0 / (8.0 * g.dxi0 * g.dxi1);
     d.pc3 = 1.0 / (2.0 * g.dxi1 * g.dxi1);
+}
+
+// physics, numerics and Chebyshev bounds of one case into its descriptor
+void case_params_to_dev(CaseDev& d, const cfd_grid& g, const cfd_params& p) {
+    case_scalars_to_dev(d, g.dxi0, g.dxi1, g.ar, p);
     cheb_bounds(g, p, d);
 }
 
@@ -774,31 +892,26 @@ int plane_id(const char* name, int cur) {
 // would not be ordered before the kernels that read it (a synchronous copy from pageable
 // memory may return before its DMA lands). From pageable memory the call returns once the
 // source is staged, so the host vectors may be reused or freed right after it.
-int upload_case(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, bool setup) {
+namespace {
+// plane `plane_id` of case `d` from a host [n1][n0] array, padded
+int put_plane(cfd_batch* b, const CaseDev& d, int plane_id, const double* src, std::vector<double>& pad) {
+    pad_plane(d, src, pad);
+    CK(cudaMemcpyAsync(b->f64 + d.base + H - 16 + (long long)plane_id * d.ps, pad.data(), sizeof(double) * d.ps,
+                       cudaMemcpyHostToDevice, b->st));
+    return CFD_OK;
+}
+
+// Initial state, descriptor and per-case scalars of case `c` once its grid planes are in
+// place, and with `setup` its pressure stencil and multigrid hierarchy. The initial state
+// reads only n0, n1, row 0 of x and y and the outer normals xnox, xnoy of `g`.
+int upload_state(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, bool setup) {
     CaseDev& d = b->hc[c];
-    case_params_to_dev(d, g, p);
-    b->prm[c] = p;
     std::vector<double> pad;
-    auto put = [&](int plane_id, const double* src) -> int {
-        pad_plane(d, src, pad);
-        CK(cudaMemcpyAsync(b->f64 + d.base + H - 16 + (long long)plane_id * d.ps, pad.data(), sizeof(double) * d.ps,
-                           cudaMemcpyHostToDevice, b->st));
-        return CFD_OK;
-    };
-    const double* gp[10] = {g.x, g.y, g.xix, g.xiy, g.etx, g.ety, g.alph, g.beta, g.gam, g.jac};
-    const int gid[10] = {P_X, P_Y, P_XIX, P_XIY, P_ETX, P_ETY, P_ALPH, P_BETA, P_GAM, P_JAC};
-    for (int m = 0; m < 10; m++)
-        if (int rc = put(gid[m], gp[m])) return rc;
-    std::vector<double> vec((size_t)g.n0 * g.n1, 0.0);  // normals as rows 0..3 of P_VEC
-    const double* nv[4] = {g.xnix, g.xniy, g.xnox, g.xnoy};
-    for (int r = 0; r < 4 && r < g.n1; r++)
-        for (int i = 0; i < g.n0; i++) vec[(size_t)r * g.n0 + i] = nv[r][i];
-    if (int rc = put(P_VEC, vec.data())) return rc;
     std::vector<double> st[6];
     initial_state(&g, &p, d, st);
     const int sid[6] = {P_U, P_V, P_T0 + b->cur, P_UP0 + b->cur, P_VP0 + b->cur, P_P};
     for (int m = 0; m < 6; m++)
-        if (int rc = put(sid[m], st[m].data())) return rc;
+        if (int rc = put_plane(b, d, sid[m], st[m].data(), pad)) return rc;
     CK(cudaMemcpyAsync(b->dc + c, &d, sizeof(CaseDev), cudaMemcpyHostToDevice, b->st));
     std::vector<double> sc(NSCAL, 0.0);
     std::vector<int> is(NISCAL, 0);
@@ -814,6 +927,84 @@ int upload_case(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, boo
         CK(cudaStreamSynchronize(b->st));
     }
     return CFD_OK;
+}
+}  // namespace
+
+int upload_case(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, bool setup) {
+    CaseDev& d = b->hc[c];
+    case_params_to_dev(d, g, p);
+    b->prm[c] = p;
+    std::vector<double> pad;
+    auto put = [&](int plane_id, const double* src) -> int { return put_plane(b, d, plane_id, src, pad); };
+    const double* gp[10] = {g.x, g.y, g.xix, g.xiy, g.etx, g.ety, g.alph, g.beta, g.gam, g.jac};
+    const int gid[10] = {P_X, P_Y, P_XIX, P_XIY, P_ETX, P_ETY, P_ALPH, P_BETA, P_GAM, P_JAC};
+    for (int m = 0; m < 10; m++)
+        if (int rc = put(gid[m], gp[m])) return rc;
+    std::vector<double> vec((size_t)g.n0 * g.n1, 0.0);  // normals as rows 0..3 of P_VEC
+    const double* nv[4] = {g.xnix, g.xniy, g.xnox, g.xnoy};
+    for (int r = 0; r < 4 && r < g.n1; r++)
+        for (int i = 0; i < g.n0; i++) vec[(size_t)r * g.n0 + i] = nv[r][i];
+    if (int rc = put(P_VEC, vec.data())) return rc;
+    return upload_state(b, c, g, p, setup);
+}
+
+int cfd_internal_grid_gen(const cfd_grid_spec* spec, double* d_planes, double* d_normals, cudaStream_t stream);
+
+// Case `c` from a grid generated on the device into `gen` (10 planes, 4 normal rows, 5
+// scan words): the bound scan and metric check run on the device and only their results,
+// row 0 of x and y and the normals come back; the slot's grid planes are written from
+// `gen` on the device, and only after the check has passed.
+int upload_case_generated(cfd_batch* b, int c, const cfd_grid_spec& spec, const cfd_params& p, double* gen) {
+    CaseDev& d = b->hc[c];
+    const int n0 = spec.n0, n1 = spec.n1;
+    const long long np = (long long)n0 * n1;
+    double* nrm = gen + 10 * np;
+    unsigned long long* scan = reinterpret_cast<unsigned long long*>(nrm + 4LL * n0);
+    if (int rc = cfd_internal_grid_gen(&spec, gen, nrm, b->st)) return rc;
+    const double dxi0 = 1.0 / (n0 - 1), dxi1 = 1.0 / (n1 - 1);
+    const ChebScan cs = cheb_consts(p, dxi0, dxi1);
+    CK(cudaMemsetAsync(scan, 0, 5 * sizeof(unsigned long long), b->st));
+    const int sblocks = (int)std::min<long long>((np + SCAN_THREADS - 1) / SCAN_THREADS, 148LL * 8);
+    k_grid_scan<<<sblocks, SCAN_THREADS, 0, b->st>>>(gen, n0, n1, cs, scan);
+    CK(cudaGetLastError());
+    std::vector<double> x0(n0), y0(n0), nv(4 * (size_t)n0);
+    unsigned long long hs[5];
+    CK(cudaMemcpyAsync(x0.data(), gen + (long long)P_X * np, sizeof(double) * n0, cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(y0.data(), gen + (long long)P_Y * np, sizeof(double) * n0, cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(nv.data(), nrm, sizeof(double) * 4 * n0, cudaMemcpyDeviceToHost, b->st));
+    CK(cudaMemcpyAsync(hs, scan, sizeof(hs), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    if (hs[4] != 0) return fail(CFD_E_ARG, "grid metrics invalid (alpha, gamma must be > 0)");
+    double emax[2], rmax[2];
+    for (int ty = 0; ty < 2; ty++) {
+        memcpy(&emax[ty], &hs[ty], sizeof(double));
+        memcpy(&rmax[ty], &hs[2 + ty], sizeof(double));
+    }
+    // the slot's grid planes: zero (as pad_plane leaves every entry it does not set), then fill
+    double* region = b->f64 + d.base + H - 16;
+    CK(cudaMemsetAsync(region, 0, sizeof(double) * 10 * d.ps, b->st));
+    CK(cudaMemsetAsync(region + (long long)P_VEC * d.ps, 0, sizeof(double) * d.ps, b->st));
+    const long long nput = 11LL * n1 * (d.periodic ? d.W + 2 * H : n0);
+    k_grid_to_slot<<<(unsigned)((nput + 255) / 256), 256, 0, b->st>>>(gen, n0, n1, d.W, d.periodic, region, d.ps,
+                                                                      d.ld);
+    CK(cudaGetLastError());
+    const double ar = spec.profile == CFD_PROFILE_OGRID ? spec.ar : 1.0;
+    case_scalars_to_dev(d, dxi0, dxi1, ar, p);
+    cheb_finish(emax, rmax, d);
+    b->prm[c] = p;
+    cfd_grid g{};
+    g.n0 = n0;
+    g.n1 = n1;
+    g.dxi0 = dxi0;
+    g.dxi1 = dxi1;
+    g.ar = ar;
+    g.x = x0.data();
+    g.y = y0.data();
+    g.xnix = nv.data();
+    g.xniy = nv.data() + n0;
+    g.xnox = nv.data() + 2 * n0;
+    g.xnoy = nv.data() + 3 * n0;
+    return upload_state(b, c, g, p, true);
 }
 
 // ==========================================================================
@@ -1270,6 +1461,27 @@ int cfd_batch_admit(cfd_batch* b, int slot, const cfd_grid* g, const cfd_params*
     if (p->precision != b->precision) return fail(CFD_E_ARG, "case precision differs from the batch's");
     CK(cudaStreamSynchronize(b->st));
     return upload_case(b, slot, *g, *p, true);
+}
+
+int cfd_batch_admit_spec(cfd_batch* b, int slot, const cfd_grid_spec* spec, const cfd_params* p) {
+    if (!b || slot < 0 || slot >= b->n) return fail(CFD_E_ARG, "bad slot");
+    if (!spec) return fail(CFD_E_ARG, "null grid spec");
+    int rc = check_case_params(p);
+    if (rc) return rc;
+    const CaseDev& d = b->hc[slot];
+    if (spec->n0 != d.n0 || spec->n1 != d.n1 || spec->profile != d.profile || p->profile != d.profile)
+        return fail(CFD_E_ARG, "case does not match the slot's geometry (n0, n1, profile)");
+    if (p->precision != b->precision) return fail(CFD_E_ARG, "case precision differs from the batch's");
+    CK(cudaStreamSynchronize(b->st));
+    const long long np = (long long)spec->n0 * spec->n1;
+    double* gen = nullptr;
+    CK(cudaMallocAsync((void**)&gen, sizeof(double) * (size_t)(10 * np + 4LL * spec->n0 + 5), b->st));
+    rc = upload_case_generated(b, slot, *spec, *p, gen);
+    cudaFreeAsync(gen, b->st);
+    const cudaError_t e = cudaStreamSynchronize(b->st);
+    if (rc) return rc;
+    CK(e);
+    return CFD_OK;
 }
 
 int cfd_batch_set_active(cfd_batch* b, int slot, int active) {

@@ -104,19 +104,20 @@ __global__ void __launch_bounds__(GEN_THREADS) k_grid_gen(GenArgs a, double* pla
 
 using namespace cfd;
 
-extern "C" int cfd_grid_generate(const cfd_grid_spec* spec, double* planes, double* normals) {
-    if (!spec || !planes || !normals) {
-        set_last_error("cfd_grid_generate: null argument");
-        return CFD_E_ARG;
-    }
-    const cfd_grid_spec& s = *spec;
-    GenArgs a{};
+namespace {
+// Map parameters of `s`, or CFD_E_ARG (with the reason) for an invalid spec.
+int gen_args(const cfd_grid_spec& s, GenArgs& a) {
+    a = GenArgs{};
     a.n0 = s.n0;
     a.n1 = s.n1;
     a.skew = s.skew;
+    if (s.n0 > 65536 || s.n1 > 65536) {
+        set_last_error("grid generation: n0, n1 must be <= 65536");
+        return CFD_E_ARG;
+    }
     if (s.profile == CFD_PROFILE_OGRID) {
         if (s.n0 < 8 || s.n1 < 6 || !(s.ar >= 1.0) || !(s.r_outer > 1.0)) {
-            set_last_error("cfd_grid_generate: O-grid needs n0 >= 8, n1 >= 6, ar >= 1, r_outer > 1");
+            set_last_error("grid generation: O-grid needs n0 >= 8, n1 >= 6, ar >= 1, r_outer > 1");
             return CFD_E_ARG;
         }
         a.ogrid = 1;
@@ -125,7 +126,7 @@ extern "C" int cfd_grid_generate(const cfd_grid_spec* spec, double* planes, doub
             a.c = std::sqrt(A * A - B * B);
             a.mu0 = std::atanh(B / A);
             if (!(s.r_outer > a.c)) {
-                set_last_error("cfd_grid_generate: r_outer must exceed the focal distance");
+                set_last_error("grid generation: r_outer must exceed the focal distance");
                 return CFD_E_ARG;
             }
             a.L = std::acosh(s.r_outer / a.c) - a.mu0;
@@ -136,13 +137,46 @@ extern "C" int cfd_grid_generate(const cfd_grid_spec* spec, double* planes, doub
         }
     } else if (s.profile == CFD_PROFILE_CAVITY) {
         if (s.n0 < 7 || s.n1 < 7) {
-            set_last_error("cfd_grid_generate: the cavity needs n0, n1 >= 7");
+            set_last_error("grid generation: the cavity needs n0, n1 >= 7");
             return CFD_E_ARG;
         }
     } else {
-        set_last_error("cfd_grid_generate: unknown profile");
+        set_last_error("grid generation: unknown profile");
         return CFD_E_ARG;
     }
+    return CFD_OK;
+}
+}  // namespace
+
+// Checks `spec` and launches the generator on `stream`: 10 planes of n1 * n0 doubles into
+// d_planes, 4 rows of n0 normals into d_normals (device memory). CFD_E_ARG for an invalid
+// spec, before any device work. Also used by cfd_batch_admit_spec (cfd_api.cu).
+int cfd_internal_grid_gen(const cfd_grid_spec* spec, double* d_planes, double* d_normals, cudaStream_t stream) {
+    if (!spec) {
+        set_last_error("grid generation: null spec");
+        return CFD_E_ARG;
+    }
+    GenArgs a;
+    if (int rc = gen_args(*spec, a)) return rc;
+    const long long np = (long long)spec->n0 * spec->n1;
+    const int blocks = (int)((np + GEN_THREADS - 1) / GEN_THREADS);
+    k_grid_gen<<<blocks, GEN_THREADS, 0, stream>>>(a, d_planes, d_normals);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_last_error(std::string("grid generation: ") + cudaGetErrorString(e));
+        return CFD_E_CUDA;
+    }
+    return CFD_OK;
+}
+
+extern "C" int cfd_grid_generate(const cfd_grid_spec* spec, double* planes, double* normals) {
+    if (!spec || !planes || !normals) {
+        set_last_error("cfd_grid_generate: null argument");
+        return CFD_E_ARG;
+    }
+    const cfd_grid_spec& s = *spec;
+    GenArgs a;
+    if (int rc = gen_args(s, a)) return rc;  // an invalid spec touches no device
     const long long np = (long long)s.n0 * s.n1;
     const size_t nb = sizeof(double) * (size_t)(10 * np + 4LL * s.n0);
     double* d = nullptr;
@@ -150,10 +184,12 @@ extern "C" int cfd_grid_generate(const cfd_grid_spec* spec, double* planes, doub
         set_last_error("cfd_grid_generate: no device memory");
         return CFD_E_OOM;
     }
-    const int blocks = (int)((np + GEN_THREADS - 1) / GEN_THREADS);
-    k_grid_gen<<<blocks, GEN_THREADS>>>(a, d, d + 10 * np);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpy(planes, d, sizeof(double) * 10 * np, cudaMemcpyDeviceToHost);
+    const int rc = cfd_internal_grid_gen(spec, d, d + 10 * np, 0);
+    if (rc != CFD_OK) {
+        cudaFree(d);
+        return rc;
+    }
+    cudaError_t e = cudaMemcpy(planes, d, sizeof(double) * 10 * np, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(normals, d + 10 * np, sizeof(double) * 4 * s.n0, cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (e != cudaSuccess) {

@@ -82,6 +82,16 @@ class Batch:
         _lib.check(_lib.lib().cfd_batch_admit(self.h, slot, ctypes.byref(s), ctypes.byref(params)),
                    "cfd_batch_admit")
 
+    def admit_spec(self, slot: int, kind: str, params, ar: float = 2.0, r_outer: float = 20.0,
+                   skew: float = 0.0):
+        """admit() of the grid generate_on_device(kind, n0, n1, ...) would return, generated
+        straight into the slot's device planes (cfd_batch_admit_spec); n0, n1 are the slot's."""
+        g = self.grids[slot]
+        prof = _lib.PROFILE_OGRID if kind == "ogrid" else _lib.PROFILE_CAVITY
+        spec = _lib.CfdGridSpec(profile=prof, n0=g.n0, n1=g.n1, ar=ar, r_outer=r_outer, skew=skew)
+        _lib.check(_lib.lib().cfd_batch_admit_spec(self.h, slot, ctypes.byref(spec), ctypes.byref(params)),
+                   "cfd_batch_admit_spec")
+
     def set_active(self, slot: int, active: bool):
         _lib.check(_lib.lib().cfd_batch_set_active(self.h, slot, int(active)), "cfd_batch_set_active")
 

@@ -61,3 +61,47 @@ def test_case_on_device_grid_steps_like_host_grid():
     for k in out[0]:
         d = np.linalg.norm(out[0][k] - out[1][k]) / np.linalg.norm(out[1][k])
         assert d < 1e-10, (k, d)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,kw", [SHAPES[0], SHAPES[2], SHAPES[3]])
+def test_admit_spec_steps_like_admit_of_the_generated_grid(kind, kw):
+    """A case generated straight into a slot (cfd_batch_admit_spec) steps bit for bit like
+    cfd_batch_admit() of the grid cfd_grid_generate() returns: the same padded grid planes,
+    the same Chebyshev bounds (the device scan rounds every operation as the host loop
+    does) and the same initial state."""
+    from cfd_solver_b200.solver import Batch, case_params
+    spec_kw = {k: v for k, v in kw.items() if k not in ("n0", "n1")}
+    gdev = G.generate_on_device(kind, **kw)
+    first = G.generate_on_device(kind, **dict(kw, skew=0.05))  # the slots' first occupant
+    prm = case_params(gdev, Re=200.0, Ri=1.0, dt=1e-3)
+    with Batch([first, first], [prm, prm]) as b:
+        b.step(2)
+        b.admit_spec(0, kind, prm, **spec_kw)
+        b.admit(1, gdev, prm)
+        for name in ("x", "y", "xix", "ety", "alph", "beta", "gam", "jac", "u", "v", "T", "p"):
+            assert np.array_equal(b.plane(0, name), b.plane(1, name)), name
+        b.step(4)
+        for name in ("u", "v", "T", "p", "up", "vp"):
+            assert np.array_equal(b.plane(0, name), b.plane(1, name)), name
+        s0, s1 = b.stats(0), b.stats(1)
+        assert s0["it_mom"] == s1["it_mom"] and s0["it_p"] == s1["it_p"] and s0["nu"] == s1["nu"]
+
+
+@pytest.mark.gpu
+def test_admit_spec_rejects_a_mismatch_and_leaves_the_slot():
+    from cfd_solver_b200 import _lib
+    from cfd_solver_b200.solver import Batch, case_params
+    g = G.generate_on_device("ogrid", n0=65, n1=49)
+    prm = case_params(g, Re=200.0, dt=1e-3)
+    with Batch([g], [prm]) as b:
+        b.step(2)
+        before = {k: b.plane(0, k) for k in ("x", "alph", "u", "p")}
+        with pytest.raises(_lib.CfdError):  # another profile than the slot's
+            b.admit_spec(0, "cavity", case_params(g, Re=200.0, dt=1e-3, profile=_lib.PROFILE_CAVITY))
+        with pytest.raises(_lib.CfdError):  # an invalid spec (semi-axis ratio below 1)
+            b.admit_spec(0, "ogrid", prm, ar=0.5)
+        for k, v in before.items():
+            assert np.array_equal(b.plane(0, k), v), k
+        b.step(1)
+        assert b.stats(0)["status"] == 0
