@@ -718,9 +718,10 @@ def main():
                         "sub_batches": nsub},
                 "clocks": clk, "gpu_launches": launches, "kernels": kernels,
                 "dominant_kernel": dom[0],
-                "baseline_metric_note": ("BASELINE metric is converged cases/s; one case needs "
+                "baseline_metric_note": ("the headline metric is converged cases/s; one case needs "
                                          "1e4-1e5 steps to its steady state, so a bench step is one "
-                                         "outer step of the whole sweep (see DESIGN.md)"),
+                                         "outer step of the whole sweep (converged cases/s: "
+                                         "--workload converged)"),
                 "case0": {"it_mom": st0["it_mom"], "it_p": st0["it_p"], "status": st0["status"]}}
         print(json.dumps(line))
     if world > 1:
