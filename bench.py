@@ -427,19 +427,13 @@ def run_serve(args):
     the sweep) through the native serving loop, against a plain single-case FP64 server
     (FIFO, one case at a time) whose service times are measured per size."""
     import math as _m
-    import numpy as np
     from cfd_solver_b200.grid import cavity
     from cfd_solver_b200.solver import case_params, serve
-    from cfd_solver_b200.workloads import SWEEP_SEED, make_case, sweep_draws
-    rng = np.random.default_rng(SWEEP_SEED + 7)
-    sizes, probs = [129, 257, 513, 1025], [0.4, 0.3, 0.2, 0.1]
-    base = sweep_draws(args.requests, seed=SWEEP_SEED + 7)
+    from cfd_solver_b200.workloads import SERVE_PROBS, SERVE_SIZES, make_case, serve_stream
+    sizes, probs = list(SERVE_SIZES), list(SERVE_PROBS)
     prec = 1 if args.precision == "mixed" else 0
     reqs, cases = [], []
-    t = 0.0
-    for d in base:
-        d = dict(d, N=int(rng.choice(sizes, p=probs)))
-        t += float(rng.exponential(1.0 / args.rate))
+    for t, d in serve_stream(args.requests, args.rate):
         g, prm = make_case(d, "cavity")
         cases.append((g, prm))
         reqs.append((t, g, case_params(g, precision=prec, **prm), args.tol, args.max_steps))

@@ -33,6 +33,24 @@ def sweep_draws(ncases: int = 256, seed: int = SWEEP_SEED):
     return out
 
 
+SERVE_SIZES = (129, 257, 513, 1025)
+SERVE_PROBS = (0.4, 0.3, 0.2, 0.1)
+
+
+def serve_stream(nrequests: int, rate: float, seed: int = SWEEP_SEED + 7):
+    """The served request stream: Poisson arrivals at `rate` requests/s, N in
+    {129, 257, 513, 1025} with probability {.4, .3, .2, .1}, the other physics of the
+    sweep draws of the same seed. Returns [(arrival_s, draw)] in arrival order."""
+    rng = np.random.default_rng(seed)
+    out = []
+    t = 0.0
+    for d in sweep_draws(nrequests, seed=seed):
+        d = dict(d, N=int(rng.choice(list(SERVE_SIZES), p=list(SERVE_PROBS))))
+        t += float(rng.exponential(1.0 / rate))
+        out.append((t, d))
+    return out
+
+
 def cavity_dt(N: int, Ri: float, Re: float = 0.0, Pr: float = 1.0, cfl: float = 0.4) -> float:
     """Time step of the cavity form, velocity scale U = max(1, sqrt(Ri)) (lid speed or
     buoyant velocity). Two limits: CFL `cfl` on U, and the stability of explicit

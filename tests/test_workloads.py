@@ -56,3 +56,22 @@ def test_cavity_dt_limits():
         assert dt <= 1.0 / (Re * max(1.0, Pr) * U * U) * (1 + 1e-15)  # half the convective bound
         assert dt in (0.4 / (N - 1) / U, 1.0 / (Re * max(1.0, Pr) * U * U))
     assert W.cavity_dt(65, 1.0) == 0.4 / 64  # no Re: CFL only
+
+
+def test_serve_stream_is_a_seeded_poisson_stream_with_the_size_mix():
+    n, rate = 4096, 8.0  # the served configuration's request count
+    s = W.serve_stream(n, rate)
+    assert s == W.serve_stream(n, rate)
+    t = np.array([a for a, _ in s])
+    assert np.all(np.diff(t) > 0) and t[0] > 0
+    gaps = np.diff(np.concatenate([[0.0], t]))
+    # exponential gaps: mean 1/rate (4-sigma band of the sample mean), coefficient of variation ~1
+    assert abs(gaps.mean() * rate - 1.0) < 4.0 / math.sqrt(n)
+    assert abs(gaps.std() / gaps.mean() - 1.0) < 0.1
+    Ns = np.array([d["N"] for _, d in s])
+    for N, p in zip(W.SERVE_SIZES, W.SERVE_PROBS):
+        f = np.mean(Ns == N)
+        assert abs(f - p) < 4.0 * math.sqrt(p * (1 - p) / n), (N, f, p)
+    draws = W.sweep_draws(n, seed=W.SWEEP_SEED + 7)
+    for (_, d), b in zip(s, draws):  # everything but N is the sweep draw of the same seed
+        assert {k: v for k, v in d.items() if k != "N"} == {k: v for k, v in b.items() if k != "N"}
