@@ -1,0 +1,53 @@
+"""Host-side contract of the library on a machine without a GPU: the batch constructor
+fails loudly (there is no CPU path to fall back to), an invalid case is rejected before
+any device is looked for, and the admission budget (cfd_case_bytes) covers at least the
+case's FP64 planes and grows with the grid."""
+import pytest
+
+from cfd_solver_b200 import _lib
+from cfd_solver_b200 import grid as G
+
+NPLANES_FP64 = 54  # FP64 planes per case: grid 10, pressure stencil 9, state 9, u*/v* 2,
+#                    right-hand sides 5, sweep scratch 5, q/pcor/diagnostics 5, normals 1,
+#                    BiCGStab vectors 8
+
+
+def _no_gpu():
+    try:
+        import torch
+        return not torch.cuda.is_available()
+    except Exception:
+        return True
+
+
+pytestmark = pytest.mark.skipif(not _lib.LIB_PATH.exists(), reason="library not built")
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="a GPU is present")
+def test_batch_without_a_gpu_fails_loudly():
+    from cfd_solver_b200.solver import Batch, case_params
+    g = G.ogrid(33, 25)
+    with pytest.raises(_lib.CfdError, match="no CUDA device"):
+        Batch([g], [case_params(g)])
+
+
+def test_invalid_case_is_rejected_before_the_device_lookup():
+    from cfd_solver_b200.solver import Batch, case_params
+    g = G.ogrid(33, 25)
+    with pytest.raises(_lib.CfdError, match="dt, Re, Pr"):
+        Batch([g], [case_params(g, dt=0.0)])
+    with pytest.raises(_lib.CfdError, match="unknown precision"):
+        Batch([g], [case_params(g, precision=7)])
+
+
+def test_case_bytes_budget():
+    L = _lib.lib()
+    for prof in (_lib.PROFILE_OGRID, _lib.PROFILE_CAVITY):
+        prev = 0
+        for n in (65, 129, 257, 513, 1025):
+            b = L.cfd_case_bytes(n, n, prof)
+            assert b >= NPLANES_FP64 * n * n * 8, (prof, n, b)
+            assert b <= 2 * NPLANES_FP64 * n * n * 8 + (1 << 20), (prof, n, b)
+            assert b > prev
+            prev = b
+        assert L.cfd_case_bytes(7, 65, prof) == 0 and L.cfd_case_bytes(65, 5, prof) == 0
