@@ -37,6 +37,10 @@ extern "C" int cfd_serve(const cfd_serve_config* cfg, const cfd_request* reqs, i
     for (int k = 0; k < nc; k++) {
         if (cfg->class_slots) {
             nslots[k] = cfg->class_slots[k];
+            if (nslots[k] <= 0) {
+                cfd_internal_set_error("cfd_serve: class_slots must be > 0");
+                return CFD_E_ARG;
+            }
         } else {
             const size_t per = cfd_case_bytes(cfg->class_grids[k].n0, cfg->class_grids[k].n1, cfg->class_profile[k]);
             nslots[k] = per ? (int)std::min<size_t>(4096, (cfg->hbm_budget / nc) / per) : 0;
@@ -44,6 +48,28 @@ extern "C" int cfd_serve(const cfd_serve_config* cfg, const cfd_request* reqs, i
         if (nslots[k] <= 0) {
             cfd_internal_set_error("cfd_serve: a slot class gets no slot within the budget");
             return CFD_E_OOM;
+        }
+    }
+    auto class_of = [&](const cfd_request& r) {
+        for (int k = 0; k < nc; k++)
+            if (r.grid->n0 == cfg->class_grids[k].n0 && r.grid->n1 == cfg->class_grids[k].n1 &&
+                r.params.profile == cfg->class_profile[k])
+                return k;
+        return -1;
+    };
+    // every request names a grid of one of the slot classes, at the slots' precision; checked
+    // before any device work, so a bad request costs no batch
+    for (int i = 0; i < nreq; i++) {
+        const char* why = nullptr;
+        if (!reqs[i].grid)
+            why = "has no grid";
+        else if (class_of(reqs[i]) < 0)
+            why = "matches no slot class";
+        else if (reqs[i].params.precision != cfg->precision)
+            why = "has another precision than the slots";
+        if (why) {
+            cfd_internal_set_error(("cfd_serve: request " + std::to_string(i) + " " + why).c_str());
+            return CFD_E_ARG;
         }
     }
     std::vector<cfd_grid> tg;
@@ -68,13 +94,6 @@ extern "C" int cfd_serve(const cfd_serve_config* cfg, const cfd_request* reqs, i
         cfd_batch_destroy(b);
         return rc;
     }
-    auto class_of = [&](const cfd_request& r) {
-        for (int k = 0; k < nc; k++)
-            if (r.grid->n0 == cfg->class_grids[k].n0 && r.grid->n1 == cfg->class_grids[k].n1 &&
-                r.params.profile == cfg->class_profile[k])
-                return k;
-        return -1;
-    };
     std::vector<int> order(nreq);
     for (int i = 0; i < nreq; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return reqs[a].arrival_s < reqs[c].arrival_s; });
@@ -83,11 +102,6 @@ extern "C" int cfd_serve(const cfd_serve_config* cfg, const cfd_request* reqs, i
         results[i].status = CFD_E_NOTCONV;
         results[i].slot = -1;
         results[i].arrival_s = reqs[i].arrival_s;
-        if (class_of(reqs[i]) < 0) {
-            cfd_batch_destroy(b);
-            cfd_internal_set_error(("cfd_serve: request " + std::to_string(i) + " matches no slot class").c_str());
-            return CFD_E_ARG;
-        }
     }
     std::vector<std::deque<int>> queue(nc);
     std::vector<int> occupant(nslot, -1);

@@ -51,3 +51,27 @@ def test_case_bytes_budget():
             assert b > prev
             prev = b
         assert L.cfd_case_bytes(7, 65, prof) == 0 and L.cfd_case_bytes(65, 5, prof) == 0
+
+
+def test_serve_rejects_bad_requests_before_any_device_work():
+    """cfd_serve checks every request (a grid of one of the slot classes, the slots'
+    precision) and the slot counts before it creates its batch."""
+    from cfd_solver_b200.solver import case_params, serve
+    g = G.cavity(33, 33)
+    cls = [(g, _lib.PROFILE_CAVITY)]
+    ok = (0.0, g, case_params(g), 1e-8, 10)
+    other = G.cavity(65, 65)
+    with pytest.raises(_lib.CfdError, match="request 1 matches no slot class"):
+        serve([ok, (0.1, other, case_params(other), 1e-8, 10)], cls, slots=[2])
+    with pytest.raises(_lib.CfdError, match="request 0 has another precision"):
+        serve([(0.0, g, case_params(g, precision=_lib.PRECISION_MIXED), 1e-8, 10)], cls, slots=[2])
+    with pytest.raises(_lib.CfdError, match="class_slots must be > 0"):
+        serve([ok], cls, slots=[0])
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="a GPU is present")
+def test_serve_without_a_gpu_fails_loudly():
+    from cfd_solver_b200.solver import case_params, serve
+    g = G.cavity(33, 33)
+    with pytest.raises(_lib.CfdError, match="no CUDA device"):
+        serve([(0.0, g, case_params(g), 1e-8, 10)], [(g, _lib.PROFILE_CAVITY)], slots=[2])
