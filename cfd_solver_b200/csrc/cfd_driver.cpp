@@ -195,7 +195,9 @@ int main(int argc, char** argv) {
             return e != v && !*e;
         };
         double d = 0;
-        if (k == "--steps") { if (!num(d)) return usage(); steps = (long long)d; }
+        // a count: a whole number in [0, 2^31 - 1]
+        auto count = [&]() { return num(d) && d >= 0 && d <= 2147483647.0 && d == std::floor(d); };
+        if (k == "--steps") { if (!count()) return usage(); steps = (long long)d; }
         else if (k == "--Re") { if (!num(prm.Re)) return usage(); }
         else if (k == "--Ri") { if (!num(prm.Ri)) return usage(); }
         else if (k == "--Pr") { if (!num(prm.Pr)) return usage(); }
@@ -204,7 +206,7 @@ int main(int argc, char** argv) {
         else if (k == "--dt") { if (!num(prm.dt)) return usage(); }
         else if (k == "--tol-mom") { if (!num(prm.tol_mom)) return usage(); }
         else if (k == "--tol-p") { if (!num(prm.tol_p)) return usage(); }
-        else if (k == "--out-every") { if (!num(d)) return usage(); out_every = (int)d; }
+        else if (k == "--out-every") { if (!count()) return usage(); out_every = (int)d; }
         else if (k == "--solve-to") { if (!num(solve_to)) return usage(); }
         else if (k == "--quiet") quiet = true;
         else if (k == "--time-accurate") prm.time_accurate = 1;

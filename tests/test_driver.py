@@ -28,6 +28,10 @@ def test_bad_input_exits_1(tmp_path):
     assert r.returncode == 1 and ("truncated" in r.stderr or "bad header" in r.stderr)
     r = subprocess.run([str(EXE), "--profile", "sphere"], capture_output=True, text=True)
     assert r.returncode == 1 and "usage" in r.stderr
+    for bad_args in (["--steps", "-5"], ["--steps", "2.5"], ["--steps", "1e12"], ["--out-every", "-1"],
+                     ["--Re"], ["--Re", "abc"], ["--precision", "fp16"], ["--unknown"]):
+        r = subprocess.run([str(EXE), *bad_args], capture_output=True, text=True)
+        assert r.returncode == 1 and "usage" in r.stderr, bad_args
 
 
 @needs_exe
