@@ -28,14 +28,15 @@ class OrcParams(ctypes.Structure):
                 ("maxit_gs", ctypes.c_int), ("maxit_sip", ctypes.c_int),
                 ("profile", ctypes.c_int), ("fix_T_annw", ctypes.c_int),
                 ("fix_circ_de", ctypes.c_int), ("omega_p", ctypes.c_double),
-                ("lid_u", ctypes.c_double), ("time_accurate", ctypes.c_int)]
+                ("lid_u", ctypes.c_double), ("time_accurate", ctypes.c_int),
+                ("atol_gs", ctypes.c_double), ("atol_sip", ctypes.c_double)]
 
 
 # the reference's own values (PSolver.cpp:160-174, 2086-2088, 2290-2291)
 REFERENCE_DEFAULTS = dict(Re=1000.0, Ri=0.0, Pr=0.71, F=0.0, alpha=82.0, dt=1e-4,
                           tol_gs=0.75e-2, tol_sip=0.75e-2, maxit_gs=100000, maxit_sip=100000,
                           profile=OGRID, fix_T_annw=0, fix_circ_de=0, omega_p=1.0, lid_u=1.0,
-                          time_accurate=0)
+                          time_accurate=0, atol_gs=0.0, atol_sip=0.0)
 
 _lib = None
 
@@ -74,7 +75,8 @@ def make_params(**kw) -> OrcParams:
                      maxit_gs=int(d["maxit_gs"]), maxit_sip=int(d["maxit_sip"]),
                      profile=int(d["profile"]), fix_T_annw=int(d["fix_T_annw"]),
                      fix_circ_de=int(d["fix_circ_de"]), omega_p=d["omega_p"], lid_u=d["lid_u"],
-                     time_accurate=int(d["time_accurate"]))
+                     time_accurate=int(d["time_accurate"]), atol_gs=d["atol_gs"],
+                     atol_sip=d["atol_sip"])
 
 
 class OracleCase:
