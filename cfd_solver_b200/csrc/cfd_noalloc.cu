@@ -1,12 +1,13 @@
 // cfd_noalloc.cu -- cfd_gauss_solve_noalloc(): the gauss() seam without any allocation.
 //
-// Some callers cannot call cudaMalloc: code running inside a CUDA graph being captured
-// (allocation is not a capturable operation), hosts whose device memory is owned by
-// another allocator or pool that must not be bypassed, and real-time loops that must not
+// Some callers cannot call cudaMalloc: a host application whose device memory is owned
+// by another allocator or pool that must not be bypassed (a framework's caching allocator,
+// a memory budget enforced by the embedding program), and real-time loops that must not
 // take the allocator's locks or risk an out-of-memory failure in the middle of a step.
 // For them this entry point runs the same solve as cfd_gauss_solve() with its scratch
 // (the second iterate, the reduction partials and a few scalars) in one file-scope
-// device array of fixed size, so the call itself allocates nothing.
+// device array of fixed size, so the call itself allocates nothing. The solve reads its
+// stop flag on the host after every pair of sweeps, so each call waits for its own work.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -77,5 +78,9 @@ extern "C" int cfd_gauss_solve_noalloc(int n0, int n1, int periodic, const doubl
         scratch = g_scratch_ptr[dev];
     }
     // cfd_seam_solve clears the scalars and the counter it relies on before its first sweep
-    return cfd_seam_solve(n0, n1, periodic, coef, phi, q, tol, maxit, sweeps, stream, scratch);
+    const int rc = cfd_seam_solve(n0, n1, periodic, coef, phi, q, tol, maxit, sweeps, stream, scratch);
+    // an error return can leave sweeps of this call queued on the stream; they must finish
+    // before the caller's next call reuses the shared array
+    if (rc == CFD_E_CUDA) cudaStreamSynchronize((cudaStream_t)stream);
+    return rc;
 }

@@ -191,7 +191,9 @@ int cfd_seam_solve(int n0, int n1, int periodic, const double* const* coef, doub
     k_seam_bounds<<<nblk, BS, 0, st>>>(s);
     int done = 0;
     double flag = 0.0;
-    for (int k = 0; k + 1 < maxit + 1 && !done; k += 2) {
+    // sweeps run in pairs (the pair ends in the caller's array), so at most maxit rounded
+    // down to even sweeps are taken
+    for (int k = 0; k + 2 <= maxit && !done; k += 2) {
         k_seam_sweep<<<nblk, BS, 0, st>>>(s, 1, k, tol);
         k_seam_sweep<<<nblk, BS, 0, st>>>(s, 0, k + 1, tol);
         if (cudaMemcpyAsync(&flag, s.sc + SC_DONE, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||

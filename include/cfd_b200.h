@@ -234,14 +234,16 @@ int cfd_batch_work(cfd_batch* b, unsigned long long* out4);
  * periodic with the seam column n0-1 duplicating column 0 (the reference's O-grid);
  * 0: columns 0 and n0-1 are fixed. Chebyshev-accelerated Jacobi sweeps until the
  * relative L1 residual before a sweep is below tol (gauss()'s rule, PSolver.cpp:2438).
+ * Sweeps run in pairs, the stop tested after each pair on the host (the call waits for
+ * its work), so at most maxit rounded down to even sweeps are taken.
  * Scratch (a second iterate and reduction partials) is allocated and freed per call.
  * Returns CFD_OK, CFD_E_MAXITER or CFD_E_DIVERGED; *sweeps receives the sweep count. */
 int cfd_gauss_solve(int n0, int n1, int periodic, const double* const* coef, double* phi,
                     const double* q, double tol, int maxit, int* sweeps, void* stream);
 
-/* Same solve as cfd_gauss_solve() for callers that cannot allocate device memory: code
- * being captured into a CUDA graph, hosts whose device memory belongs to another
- * allocator, loops that must not take the allocator's locks. No counterpart in the
+/* Same solve as cfd_gauss_solve() for callers that cannot allocate device memory: hosts
+ * whose device memory belongs to another allocator or budget, loops that must not take
+ * the allocator's locks or meet an out-of-memory failure mid-step. No counterpart in the
  * reference (its gauss() allocates two full arrays per call, PSolver.cpp:2288-2289).
  * The scratch lives in one static device array sized for n0*n1 <= CFD_NOALLOC_MAX_POINTS
  * (about 8.4 MB, held by every GPU that loads the library until the process exits);

@@ -1,11 +1,12 @@
 """cfd_gauss_solve_noalloc against cfd_gauss_solve.
 
-The no-alloc entry point serves callers that cannot call cudaMalloc (a CUDA graph
-being captured, a host whose device memory belongs to another allocator, a loop that
-must not take the allocator's locks): its scratch is a static device array, and it
-must give the same answer as the allocating entry point -- on two calls in a row,
-since every call reuses (and leaves behind) the same scratch. This file is named to
-be collected last; it also passes on its own in a fresh process.
+The no-alloc entry point serves callers that cannot call cudaMalloc (a host whose
+device memory belongs to another allocator or budget, a loop that must not take the
+allocator's locks or meet an out-of-memory failure mid-step): its scratch is a static
+device array, and it must give the same answer as the allocating entry point -- on two
+calls in a row, since every call reuses (and leaves behind) the same scratch -- and
+leave the device's free memory unchanged. This file is named to be collected last; it
+also passes on its own in a fresh process.
 """
 import ctypes
 
@@ -58,6 +59,51 @@ def test_noalloc_matches_allocating_entry_point_twice():
         sl = (slice(1, -1), slice(None)) if periodic else (slice(1, -1), slice(1, -1))
         err = np.linalg.norm(got[sl] - ref[sl]) / np.linalg.norm(ref[sl])
         assert err < REL, err
+
+
+def test_noalloc_leaves_free_device_memory_unchanged():
+    import torch
+    from cfd_solver_b200 import _lib
+    L = _lib.lib()
+    g = ogrid(33, 25, skew=0.1)
+    coefs, phi0, q = _system(g, 2)
+    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in coefs]
+    ptrs = (ctypes.c_void_p * 25)(*[t.data_ptr() for t in dev])
+    phi = torch.from_numpy(phi0.copy()).cuda()
+    qd = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+    sweeps = ctypes.c_int(0)
+
+    def call():
+        phi.copy_(torch.from_numpy(phi0))
+        torch.cuda.synchronize()
+        rc = L.cfd_gauss_solve_noalloc(g.n0, g.n1, 1, ptrs, ctypes.c_void_p(phi.data_ptr()),
+                                       ctypes.c_void_p(qd.data_ptr()), 1e-12, 600, ctypes.byref(sweeps), None)
+        torch.cuda.synchronize()
+        assert rc == 0, L.cfd_last_error()
+
+    call()  # warm: the first call on a device looks up the array's address
+    free0, _ = torch.cuda.mem_get_info()
+    call()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
+def test_noalloc_sweeps_never_exceed_an_odd_cap():
+    from cfd_solver_b200 import _lib
+    L = _lib.lib()
+    g = ogrid(33, 25, skew=0.1)
+    coefs, phi0, q = _system(g, 3)
+    import torch
+    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in coefs]
+    ptrs = (ctypes.c_void_p * 25)(*[t.data_ptr() for t in dev])
+    phi = torch.from_numpy(phi0.copy()).cuda()
+    qd = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+    sweeps = ctypes.c_int(0)
+    rc = L.cfd_gauss_solve_noalloc(g.n0, g.n1, 1, ptrs, ctypes.c_void_p(phi.data_ptr()),
+                                   ctypes.c_void_p(qd.data_ptr()), 1e-300, 5, ctypes.byref(sweeps), None)
+    torch.cuda.synchronize()
+    assert rc == -5  # CFD_E_MAXITER
+    assert sweeps.value == 4
 
 
 def test_noalloc_rejects_grids_beyond_its_limit():
