@@ -31,7 +31,7 @@ SYMBOLS = ("cfd_params_default", "cfd_last_error", "cfd_device_count", "cfd_set_
            "cfd_gauss_solve", "cfd_gauss_solve_noalloc", "cfd_batch_fetch_stats", "cfd_batch_admit",
            "cfd_batch_set_active", "cfd_serve", "cfd_batch_set_mg", "cfd_batch_get_mg",
            "cfd_batch_autotune", "cfd_batch_save", "cfd_batch_load", "cfd_grid_generate",
-           "cfd_batch_admit_spec")
+           "cfd_batch_admit_spec", "cfd_batch_set_wait_limit")
 
 _D = ctypes.c_double
 _PD = ctypes.POINTER(ctypes.c_double)
@@ -157,6 +157,7 @@ def lib():
     L.cfd_batch_set_mg.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     ip = ctypes.POINTER(ctypes.c_int)
     L.cfd_batch_get_mg.argtypes = [vp, ip, ip, ip, ip]
+    L.cfd_batch_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
     L.cfd_batch_autotune.argtypes = [vp, ctypes.c_int, ip, ctypes.POINTER(ctypes.c_double)]
     L.cfd_batch_save.argtypes = [vp, ctypes.c_char_p]
     L.cfd_batch_load.argtypes = [vp, ctypes.c_char_p]

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/cfd_b200.h"
+#include "cfd_bulk.cuh"
 #include "cfd_common.cuh"
 #include "cfd_kernels.cuh"
 #include "cfd_reduce.cuh"
@@ -1243,6 +1244,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
     bd.jtiles = b->dtiles + pos_jt; bd.njtiles = (int)jtiles.size();
     bd.error = b->flags + 4;
+    bd.wait_polls = kWaitPolls;
     bd.mg_res = mg_res_plane(b->mg_pre, b->mg_post, b->mg_fused);
     bd.sweep_no = b->flags + 7;
     bd.mixed = b->precision == CFD_PRECISION_MIXED;
@@ -1340,6 +1342,14 @@ int cfd_batch_set_mg(cfd_batch* b, int nu_pre, int nu_post, int coarse_sweeps, i
     b->mg_fused = fused;
     b->bd.mg_res = mg_res_plane(nu_pre, nu_post, fused);
     drop_graphs(b);  // the step graphs hold the old schedule
+    return CFD_OK;
+}
+
+int cfd_batch_set_wait_limit(cfd_batch* b, long long polls) {
+    if (!b) return fail(CFD_E_ARG, "null batch");
+    CK(cudaStreamSynchronize(b->st));
+    b->bd.wait_polls = polls < 0 ? kWaitPolls : (unsigned)std::min<long long>(polls, 0xffffffffll);
+    drop_graphs(b);  // the step graphs hold the old limit in their kernel parameters
     return CFD_OK;
 }
 
@@ -1642,6 +1652,8 @@ int cfd_case_step(cfd_case* c, int nsteps, cfd_step_stats* last) {
         if (rc) return rc;
         last->steps = nsteps;
         if (last->status & ST_NAN) return fail(CFD_E_DIVERGED, "NaN in the solution");
+        if (last->status & ST_BREAKDOWN) return fail(CFD_E_BREAKDOWN, "pressure solve: Krylov breakdown");
+        if (last->status & ST_MAXITER) return fail(CFD_E_MAXITER, "an inner solve stopped at its iteration cap");
     }
     return CFD_OK;
 }

@@ -3,15 +3,17 @@
 //
 // Rules kept here: source and destination 16-byte aligned, sizes a multiple of 16 bytes;
 // no multicast (every copy reads this GPU's own memory into this CTA's shared memory);
-// every wait gives up after a fixed number of polls and reports through a flag instead
-// of spinning forever.
+// every wait gives up after a bounded number of polls and reports through a flag instead
+// of spinning forever. A kernel whose wait gave up still waits, at the long default
+// limit, for the copies it issued before its CTA leaves, so no copy lands in shared
+// memory that another CTA owns.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace cfd {
 
-constexpr unsigned kWaitPolls = 1u << 24;  // ~0.1-1 s of polling before a wait gives up
+constexpr unsigned kWaitPolls = 1u << 24;  // ~0.1-1 s of polling before a wait gives up (default)
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -70,9 +72,10 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, 
         : "memory");
 }
 
-// bounded wait for phase `parity` of `bar`; false when it gave up
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
-    for (unsigned n = 0; n < kWaitPolls; n++)
+// bounded wait for phase `parity` of `bar`, at most `polls` polls (0: none, the wait gives
+// up at once); false when it gave up
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned polls = kWaitPolls) {
+    for (unsigned n = 0; n < polls; n++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

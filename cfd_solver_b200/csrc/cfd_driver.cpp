@@ -8,8 +8,8 @@
 //
 //   cfd_b200_solver [INP.DAT] [--steps N] [--Re x] [--Ri x] [--Pr x] [--F x] [--time-accurate] [--alpha deg]
 //                   [--dt x] [--profile ogrid|cavity] [--precision fp64|mixed]
-//                   [--tol-mom x] [--tol-p x] [--out-every N] [--solve-to tol] [--quiet]
-//                   [--dir DIR]
+//                   [--tol-mom x] [--tol-p x] [--atol-mom x] [--atol-p x] [--maxit-mom N]
+//                   [--maxit-p N] [--out-every N] [--solve-to tol] [--quiet] [--dir DIR]
 //
 // --solve-to runs until the steady residual (relative to the first step) is below tol or
 // --steps steps have run, writing the outputs once at the end. Exit status: 0 on success,
@@ -170,6 +170,7 @@ int usage() {
     std::fprintf(stderr,
                  "usage: cfd_b200_solver [INP.DAT] [--steps N] [--Re x] [--Ri x] [--Pr x] [--F x] [--time-accurate] [--alpha deg]\n"
                  "       [--dt x] [--profile ogrid|cavity] [--precision fp64|mixed] [--tol-mom x] [--tol-p x]\n"
+                 "       [--atol-mom x] [--atol-p x] [--maxit-mom N] [--maxit-p N]\n"
                  "       [--out-every N] [--solve-to tol] [--quiet] [--dir DIR]\n");
     return 1;
 }
@@ -206,6 +207,10 @@ int main(int argc, char** argv) {
         else if (k == "--dt") { if (!num(prm.dt)) return usage(); }
         else if (k == "--tol-mom") { if (!num(prm.tol_mom)) return usage(); }
         else if (k == "--tol-p") { if (!num(prm.tol_p)) return usage(); }
+        else if (k == "--atol-mom") { if (!num(prm.atol_mom)) return usage(); }
+        else if (k == "--atol-p") { if (!num(prm.atol_p)) return usage(); }
+        else if (k == "--maxit-mom") { if (!count() || d < 2) return usage(); prm.maxit_mom = (int)d; }
+        else if (k == "--maxit-p") { if (!count() || d < 1) return usage(); prm.maxit_p = (int)d; }
         else if (k == "--out-every") { if (!count()) return usage(); out_every = (int)d; }
         else if (k == "--solve-to") { if (!num(solve_to)) return usage(); }
         else if (k == "--quiet") quiet = true;

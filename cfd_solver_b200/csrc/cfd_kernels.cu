@@ -263,9 +263,12 @@ __global__ void __launch_bounds__(NT, 2) k_rhs(BatchDev b) {
         for (int m = 0; m < RHS_INT; m++) tma_load_3d(SI + m * TX * TYJ, maps + 128, t.i0 + 2, t.j0, ip[m], &bar);
     }
     __syncthreads();
-    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0));
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0, b.wait_polls));
     if (!ok) {
-        if (tid == 0) atomicExch(b.error, 1);
+        if (tid == 0) {
+            atomicExch(b.error, 1);
+            mbar_wait_bounded(&bar, 0);  // the copies land before the CTA leaves
+        }
         return;
     }
     const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
@@ -445,8 +448,14 @@ __global__ void __launch_bounds__(NT, 4) k_face_q(BatchDev b) {
         for (int m = 0; m < FQ_HALO; m++) tma_load_3d(sm + m * JTW * JTH, maps, t.i0, t.j0 - 2, hp[m], &bar);
     }
     __syncthreads();
-    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0));
-    if (!ok && tid == 0) atomicExch(b.error, 1);
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0, b.wait_polls));
+    if (!ok) {
+        if (tid == 0) {
+            atomicExch(b.error, 1);
+            mbar_wait_bounded(&bar, 0);  // the copies land before the CTA leaves
+        }
+        return;
+    }
     const double *P = sm, *U = sm + JTW * JTH, *V = sm + 2 * JTW * JTH, *X = sm + 3 * JTW * JTH,
                  *Y = sm + 4 * JTW * JTH, *E = sm + 5 * JTW * JTH, *G = sm + 6 * JTW * JTH;
     const int ld = c.ld;
@@ -510,7 +519,9 @@ __global__ void __launch_bounds__(NT, 4) k_face_q(BatchDev b) {
         sc[S_NB1] = red[0];
         sc[S_RL1] = red[0];
         is[I_PIT] = 0;
-        is[I_PSTATUS] = 0;
+        // this step's solver status starts with the momentum / energy solves: a field still
+        // iterating when their loop ended stopped at the sweep cap
+        is[I_PSTATUS] = (is[I_MWORD] & ((1 << NFIELD) - 1)) ? ST_MAXITER : 0;
         if (red[0] == 0.0 || !isfinite(red[0])) {
             is[I_PDONE] = 1;
             if (!isfinite(red[0])) is[I_STATUS] |= ST_NAN;

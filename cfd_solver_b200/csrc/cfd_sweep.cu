@@ -238,7 +238,7 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
     for (int fm = mask; fm; fm &= fm - 1, k++) {
         const int f = __ffs(fm) - 1;
         const int bi = k & 1;
-        ok = __syncthreads_and(mbar_wait_bounded(&bar[bi], (k >> 1) & 1)) && ok;
+        ok = __syncthreads_and(mbar_wait_bounded(&bar[bi], (k >> 1) & 1, b.wait_polls)) && ok;
         if (!ok) break;
         const unsigned char* buf = sm + bi * L::BUF;
         if (k == 0) {
@@ -366,7 +366,7 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
     if (!ok) {
         if (tid == 0) {
             atomicExch(b.error, 1);
-            // let the copies still in flight land before the CTA leaves
+            // let the copies still in flight land before the CTA leaves (the long default limit)
             for (int m = k; m < nf && m < k + 2; m++) mbar_wait_bounded(&bar[m & 1], (m >> 1) & 1);
         }
         return;

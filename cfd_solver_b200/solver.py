@@ -98,6 +98,10 @@ class Batch:
     def set_mg(self, nu_pre: int, nu_post: int, coarse_sweeps: int, fused: int = 0):
         _lib.check(_lib.lib().cfd_batch_set_mg(self.h, nu_pre, nu_post, coarse_sweeps, fused), "cfd_batch_set_mg")
 
+    def set_wait_limit(self, polls: int):
+        """Polls of a kernel's bounded copy wait before it gives up (negative: the default)."""
+        _lib.check(_lib.lib().cfd_batch_set_wait_limit(self.h, int(polls)), "cfd_batch_set_wait_limit")
+
     def get_mg(self) -> tuple:
         v = [ctypes.c_int() for _ in range(4)]
         _lib.check(_lib.lib().cfd_batch_get_mg(self.h, *[ctypes.byref(x) for x in v]), "cfd_batch_get_mg")

@@ -116,9 +116,17 @@ int cfd_device_count(int* count);
 /* make `device` current for this thread's later calls (one process per GPU) */
 int cfd_set_device(int device);
 
+/* status bits of cfd_step_stats.status (the reference reports none: its solves loop to
+ * maxiter = 100000 silently, PSolver.cpp:2087, 2291, and it never checks for NaN) */
+#define CFD_STATUS_MAXITER 1   /* this step: a u/v/T/up/vp or pressure solve stopped at its cap */
+#define CFD_STATUS_BREAKDOWN 2 /* this step: the pressure BiCGStab broke down (rho or omega = 0) */
+#define CFD_STATUS_NAN 4       /* sticky: a non-finite residual; the case's fields are invalid */
+
 /* ---- single case (replaces Solver::Solver() + Solver::timeLoop()) ---- */
 int cfd_case_create(const cfd_grid* g, const cfd_params* prm, cfd_case** out);
-/* advance nsteps time steps (the body of timeLoop, PSolver.cpp:1058-1983) */
+/* advance nsteps time steps (the body of timeLoop, PSolver.cpp:1058-1983). With `last`,
+ * the last step's status is also returned: CFD_E_DIVERGED (NaN), CFD_E_BREAKDOWN or
+ * CFD_E_MAXITER; the steps have been taken either way. */
 int cfd_case_step(cfd_case* c, int nsteps, cfd_step_stats* last);
 /* step until steady_res_rel <= tol (or max_steps: CFD_E_NOTCONV). The continuity source q
  * of this projection scheme keeps a compatibility defect in a closed cavity (the pressure
@@ -153,6 +161,13 @@ int cfd_batch_fetch_stats(cfd_batch* b, cfd_step_stats* out, int cap);
  * exactly where it was), keeps the fastest and reports it as {pre, post, coarse, fused}
  * with its time per step. */
 int cfd_batch_set_mg(cfd_batch* b, int nu_pre, int nu_post, int coarse_sweeps, int fused);
+/* Polls a kernel's wait for its bulk copies makes before it gives up (no counterpart in the
+ * reference; default 2^24, about 0.1-1 s; negative restores the default; 0 gives up at
+ * once, which only tests the error path). A wait that gives up sets the batch's error
+ * flag and the kernel returns (after its copies have landed); the step then fails with
+ * CFD_E_CUDA ("a bounded wait inside a kernel timed out") and the batch's fields are
+ * invalid: destroy it. The device stays usable. */
+int cfd_batch_set_wait_limit(cfd_batch* b, long long polls);
 int cfd_batch_get_mg(cfd_batch* b, int* nu_pre, int* nu_post, int* coarse_sweeps, int* fused);
 int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule4, double* out_ms_per_step);
 
