@@ -31,7 +31,7 @@ SYMBOLS = ("cfd_params_default", "cfd_last_error", "cfd_device_count", "cfd_set_
            "cfd_gauss_solve", "cfd_gauss_solve_noalloc", "cfd_batch_fetch_stats", "cfd_batch_admit",
            "cfd_batch_set_active", "cfd_serve", "cfd_batch_set_mg", "cfd_batch_get_mg",
            "cfd_batch_autotune", "cfd_batch_save", "cfd_batch_load", "cfd_grid_generate",
-           "cfd_batch_admit_spec", "cfd_batch_set_wait_limit")
+           "cfd_batch_admit_spec", "cfd_batch_set_wait_limit", "cfd_sip_solve")
 
 _D = ctypes.c_double
 _PD = ctypes.POINTER(ctypes.c_double)
@@ -151,6 +151,7 @@ def lib():
                                   ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p,
                                   _D, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]
     L.cfd_gauss_solve_noalloc.argtypes = L.cfd_gauss_solve.argtypes
+    L.cfd_sip_solve.argtypes = L.cfd_gauss_solve.argtypes
     L.cfd_batch_fetch_stats.argtypes = [vp, ctypes.POINTER(CfdStepStats), ctypes.c_int]
     L.cfd_batch_admit.argtypes = [vp, ctypes.c_int, ctypes.POINTER(CfdGrid), ctypes.POINTER(CfdParams)]
     L.cfd_batch_set_active.argtypes = [vp, ctypes.c_int, ctypes.c_int]

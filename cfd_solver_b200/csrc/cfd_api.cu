@@ -1572,7 +1572,9 @@ static int state_copy(cfd_batch* b, void* host, size_t bytes, bool to_host) {
 //   the state image of cfd_batch_get_state | u64 FNV-1a hash of all preceding bytes
 namespace {
 const char kCkptMagic[8] = {'C', 'F', 'D', 'B', '2', '0', '0', 'C'};
-const uint32_t kCkptVersion = 2;  // 1: padded device planes in the state image; 2: stored columns only
+// 1: padded device planes in the state image; 2: stored columns only; 3: a grid fingerprint per case
+const uint32_t kCkptVersion = 3;
+constexpr size_t kCkptCaseHdr = 24;  // i32 n0, n1, profile, precision; u64 grid fingerprint
 uint64_t fnv1a(const unsigned char* p, size_t n, uint64_t h = 1469598103934665603ull) {
     for (size_t k = 0; k < n; k++) {
         h ^= p[k];
@@ -1580,21 +1582,68 @@ uint64_t fnv1a(const unsigned char* p, size_t n, uint64_t h = 146959810393466560
     }
     return h;
 }
+
+// the splitmix64 output function (Steele, Lea and Flood 2014): a bijective 64-bit mixer
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+
+// A fingerprint of every case's grid (the ten grid planes over the stored columns, one CTA
+// per case): the wrapping sum of a mixed word per value and position, so the result is the
+// same whatever order the threads add in.
+__global__ void k_grid_hash(BatchDev b, unsigned long long* out) {
+    const CaseDev& c = b.cases[blockIdx.x];
+    const int ncols = c.periodic ? c.W : c.n0;
+    const long long per = (long long)c.n1 * ncols;
+    unsigned long long h = 0;
+    for (long long e = threadIdx.x; e < 10 * per; e += blockDim.x) {
+        const int q = (int)(e / per);
+        const long long r = e - q * per;
+        const int j = (int)(r / ncols), i = (int)(r % ncols);
+        const double v = plane(b, c, q)[(long long)j * c.ld + i];
+        h += mix64((unsigned long long)__double_as_longlong(v) ^ mix64((unsigned long long)e));
+    }
+    atomicAdd(out + blockIdx.x, h);
+}
+
+int grid_fingerprints(cfd_batch* b, std::vector<uint64_t>& out) {
+    unsigned long long* d = nullptr;
+    CK(cudaMalloc((void**)&d, sizeof(unsigned long long) * b->n));
+    out.assign(b->n, 0);
+    cudaError_t e = cudaMemsetAsync(d, 0, sizeof(unsigned long long) * b->n, b->st);
+    if (e == cudaSuccess) {
+        k_grid_hash<<<b->n, 256, 0, b->st>>>(b->bd, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), d, sizeof(uint64_t) * b->n, cudaMemcpyDeviceToHost, b->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(CFD_E_CUDA, std::string("grid fingerprint: ") + cudaGetErrorString(e));
+    return CFD_OK;
+}
 }  // namespace
 
 int cfd_batch_save(cfd_batch* b, const char* path) {
     if (!b || !path) return fail(CFD_E_ARG, "bad arguments");
     const size_t sb = cfd_batch_state_bytes(b);
-    std::vector<unsigned char> buf(8 + 8 + (size_t)16 * b->n + sb + 8);
+    std::vector<uint64_t> fp;
+    if (int rc = grid_fingerprints(b, fp)) return rc;
+    std::vector<unsigned char> buf(8 + 8 + kCkptCaseHdr * b->n + sb + 8);
     unsigned char* p = buf.data();
     memcpy(p, kCkptMagic, 8);
     const uint32_t hdr[2] = {kCkptVersion, (uint32_t)b->n};
     memcpy(p + 8, hdr, 8);
     for (int c = 0; c < b->n; c++) {
         const int32_t g[4] = {b->hc[c].n0, b->hc[c].n1, b->hc[c].profile, b->prm[c].precision};
-        memcpy(p + 16 + 16 * (size_t)c, g, 16);
+        memcpy(p + 16 + kCkptCaseHdr * c, g, 16);
+        memcpy(p + 16 + kCkptCaseHdr * c + 16, &fp[c], 8);
     }
-    unsigned char* st = p + 16 + 16 * (size_t)b->n;
+    unsigned char* st = p + 16 + kCkptCaseHdr * b->n;
     if (int rc = cfd_batch_get_state(b, st, sb)) return rc;
     const uint64_t h = fnv1a(p, buf.size() - 8);
     memcpy(p + buf.size() - 8, &h, 8);
@@ -1615,7 +1664,7 @@ int cfd_batch_load(cfd_batch* b, const char* path) {
     while ((n = fread(tmp, 1, sizeof(tmp), f)) > 0) buf.insert(buf.end(), tmp, tmp + n);
     fclose(f);
     const size_t sb = cfd_batch_state_bytes(b);
-    const size_t need = 8 + 8 + (size_t)16 * b->n + sb + 8;
+    const size_t need = 8 + 8 + kCkptCaseHdr * b->n + sb + 8;
     if (buf.size() < 16 || memcmp(buf.data(), kCkptMagic, 8) != 0) return fail(CFD_E_ARG, "not a checkpoint file");
     uint32_t hdr[2];
     memcpy(hdr, buf.data() + 8, 8);
@@ -1625,18 +1674,113 @@ int cfd_batch_load(cfd_batch* b, const char* path) {
     uint64_t h;
     memcpy(&h, buf.data() + need - 8, 8);
     if (h != fnv1a(buf.data(), need - 8)) return fail(CFD_E_ARG, "checkpoint is corrupt (hash mismatch)");
+    std::vector<uint64_t> fp;
+    if (int rc = grid_fingerprints(b, fp)) return rc;
     for (int c = 0; c < b->n; c++) {
         int32_t g[4];
-        memcpy(g, buf.data() + 16 + 16 * (size_t)c, 16);
+        uint64_t gh;
+        memcpy(g, buf.data() + 16 + kCkptCaseHdr * c, 16);
+        memcpy(&gh, buf.data() + 16 + kCkptCaseHdr * c + 16, 8);
         if (g[0] != b->hc[c].n0 || g[1] != b->hc[c].n1 || g[2] != b->hc[c].profile || g[3] != b->prm[c].precision)
             return fail(CFD_E_ARG, "checkpoint case " + std::to_string(c) + " has another geometry or precision");
+        if (gh != fp[c])
+            return fail(CFD_E_ARG, "checkpoint case " + std::to_string(c) + " was saved on another grid");
     }
-    return cfd_batch_set_state(b, buf.data() + 16 + 16 * (size_t)b->n, sb);
+    return cfd_batch_set_state(b, buf.data() + 16 + kCkptCaseHdr * b->n, sb);
 }
 
 int cfd_batch_get_state(cfd_batch* b, void* host, size_t bytes) { return state_copy(b, host, bytes, true); }
 int cfd_batch_set_state(cfd_batch* b, const void* host, size_t bytes) {
     return state_copy(b, const_cast<void*>(host), bytes, false);
+}
+
+// ---- the sip9p() seam (replaces PSolver.cpp:2067-2278, called at :1466)
+// A one-case batch of the caller's size carries the solve: its pressure stencil and
+// multigrid hierarchy come from the caller's nine planes (the grid the batch is created
+// with only sizes it), and the step's own BiCGStab + V-cycle kernels run host-driven on the
+// correction of phi0, with the reference's relative L1 stop rule.
+int cfd_sip_solve(int n0, int n1, int periodic, const double* const* coef9, double* phi, const double* q,
+                  double tol, int maxit, int* iters, void* stream) {
+    if (iters) *iters = 0;
+    if (n0 < 8 || n1 < (periodic ? 6 : 7) || !coef9 || !phi || !q || maxit < 1 || !(tol >= 0.0))
+        return fail(CFD_E_ARG, "cfd_sip_solve: bad arguments");
+    for (int m = 0; m < 9; m++)
+        if (!coef9[m]) return fail(CFD_E_ARG, "cfd_sip_solve: null coefficient plane");
+    // the caller's arrays are complete once its stream has drained
+    CK(cudaStreamSynchronize((cudaStream_t)stream));
+    cfd_grid_spec spec{};
+    spec.profile = periodic ? CFD_PROFILE_OGRID : CFD_PROFILE_CAVITY;
+    spec.n0 = n0;
+    spec.n1 = n1;
+    spec.ar = 2.0;
+    spec.r_outer = 20.0;
+    const size_t np = (size_t)n0 * n1;
+    std::vector<double> planes(10 * np), normals(4 * (size_t)n0);
+    int rc = cfd_grid_generate(&spec, planes.data(), normals.data());
+    if (rc) return rc;
+    cfd_grid g{};
+    g.n0 = n0;
+    g.n1 = n1;
+    g.dxi0 = 1.0 / (n0 - 1);
+    g.dxi1 = 1.0 / (n1 - 1);
+    g.ar = spec.ar;
+    const double** gp[10] = {&g.x, &g.y, &g.xix, &g.xiy, &g.etx, &g.ety, &g.alph, &g.beta, &g.gam, &g.jac};
+    for (int m = 0; m < 10; m++) *gp[m] = planes.data() + m * np;
+    g.xnix = normals.data();
+    g.xniy = normals.data() + n0;
+    g.xnox = normals.data() + 2 * n0;
+    g.xnoy = normals.data() + 3 * n0;
+    cfd_params p;
+    cfd_params_default(&p);
+    p.profile = spec.profile;
+    p.tol_p = tol;
+    p.atol_p = 0.0;
+    p.maxit_p = maxit;
+    cfd_batch* b = nullptr;
+    rc = cfd_batch_create(1, &g, &p, &b);
+    if (rc) return rc;
+    auto finish = [&](int code) {
+        cudaStreamSynchronize(b->st);
+        cfd_batch_destroy(b);
+        return code;
+    };
+    BatchDev& bd = b->bd;
+    const CaseDev& d = b->hc[0];
+    // sip9p's argument order (ap, ae, as, an, aw, ase, asw, ane, anw) -> P_AP .. P_ASW
+    SipIn in;
+    const int order[9] = {0, 1, 4, 3, 2, 7, 8, 5, 6};
+    for (int m = 0; m < 9; m++) in.a[m] = coef9[order[m]];
+    in.phi = phi;
+    in.q = q;
+    in.n0 = n0;
+    const long long npad = (long long)n1 * (d.W + 2 * H);
+    k_sip_pack<<<(unsigned)((npad + 255) / 256), 256, 0, b->st>>>(bd, in);
+    for (int l = 0; l + 1 < b->nlev_max; l++)
+        if (bd.natiles[l + 1] > 0) k_mg_galerkin<<<bd.natiles[l + 1], NT, 0, b->st>>>(bd, l, 0);
+    if (cudaMemsetAsync(b->flags, 0, 4 * sizeof(int), b->st) != cudaSuccess)
+        return finish(fail(CFD_E_CUDA, "cfd_sip_solve: flag reset failed"));
+    k_sip_init<<<bd.njtiles, NT, 0, b->st>>>(bd);
+    for (int it = 0; it < maxit; it++) {
+        if (it > 0) {
+            int a = 0;
+            rc = read_flag(b, 0, &a);
+            if (rc) return finish(rc);
+            if (a <= 0) break;
+        }
+        enq_p_iter(b, bd);
+    }
+    k_sip_out<<<(unsigned)(((long long)np + 255) / 256), 256, 0, b->st>>>(bd, phi, n0);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(b->st) != cudaSuccess)
+        return finish(fail(CFD_E_CUDA, "cfd_sip_solve: kernel failure"));
+    int is[NISCAL];
+    if (cudaMemcpy(is, b->iscal, sizeof(is), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return finish(fail(CFD_E_CUDA, "cfd_sip_solve: status read failed"));
+    if (iters) *iters = is[I_PIT];
+    const int st = is[I_STATUS] | is[I_PSTATUS];
+    if (st & ST_NAN) return finish(fail(CFD_E_DIVERGED, "cfd_sip_solve: residual not finite"));
+    if (st & ST_BREAKDOWN) return finish(fail(CFD_E_BREAKDOWN, "cfd_sip_solve: Krylov breakdown"));
+    if (st & ST_MAXITER) return finish(fail(CFD_E_MAXITER, "cfd_sip_solve: maxit reached"));
+    return finish(CFD_OK);
 }
 
 // ---- single case

@@ -855,13 +855,18 @@ static_assert(MG_PRR_THREADS >= MPR_BX * MPR_BY && MG_PRR_THREADS >= TX * TY && 
 __device__ __forceinline__ int mpr_at(int xx, int ry) {  // point (xx, ry) of the ringed region
     return (xx & 1) * MPR_XP + ry * MPR_XS + (xx >> 1);
 }
+// the fine residual region (65 x 17 points), split by column parity like x: the blocks write
+// it and the restriction reads it at column stride 2, which a plain row-major tile serves
+// with two-way bank conflicts; split, consecutive threads touch consecutive words
+constexpr int MPR_RS = 33, MPR_RP = MPR_RH * MPR_RS + 16;
+__device__ __forceinline__ int mpr_rat(int x, int y) { return (x & 1) * MPR_RP + y * MPR_RS + (x >> 1); }
 
 // Each thread owns one 2 x 2 block of E, which holds one point of each colour (E starts at
 // an even column and row, and a level with a coarser one has an even width when periodic,
 // so the colours are the four parity classes); its four stencils stay in registers.
 __global__ void __launch_bounds__(MG_PRR_THREADS, 3) k_mg_prr(BatchDev b, int l, int dst, int inner) {
     __shared__ float xs[2 * MPR_XP];
-    __shared__ float rs[MPR_RW * MPR_RH];
+    __shared__ float rs[2 * MPR_RP];
     const Tile t = b.atiles[l + 1][blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
@@ -949,7 +954,7 @@ __global__ void __launch_bounds__(MG_PRR_THREADS, 3) k_mg_prr(BatchDev b, int l,
                                  f[7] * xs[mpr_at(xx + 1, ry - 1)] + f[8] * xs[mpr_at(xx - 1, ry - 1)];
                 r = f[9] - ax;
             }
-            rs[(y - 1) * MPR_RW + (x - 1)] = r;
+            rs[mpr_rat(x - 1, y - 1)] = r;
             // owned: columns 2 i0 .. 2 i0 + 63 (E columns 2 .. 65), rows 2 j0 - 1 .. jhi
             const int gi = ei0 + x, gj = ej0 + y;
             if (x >= 2 && gi >= F.ilo && gi <= F.ihi && gj <= jhi)
@@ -960,9 +965,12 @@ __global__ void __launch_bounds__(MG_PRR_THREADS, 3) k_mg_prr(BatchDev b, int l,
     const int li = tid % TX, lj = tid / TX;
     const int I = t.i0 + li, J = t.j0 + lj;
     if (I < C.ilo || I > C.ihi || J > C.n1 - 2) return;
-    const int f = (2 * lj + 1) * MPR_RW + (2 * li + 1);  // fine (2I, 2J) in the residual region
-    const float r4 = 0.0625f * (rs[f - MPR_RW - 1] + rs[f - MPR_RW + 1] + rs[f + MPR_RW - 1] + rs[f + MPR_RW + 1]) +
-                     0.125f * (rs[f - MPR_RW] + rs[f + MPR_RW] + rs[f - 1] + rs[f + 1]) + 0.25f * rs[f];
+    const int fx = 2 * li + 1, fy = 2 * lj + 1;  // fine (2I, 2J) in the residual region
+    const float r4 = 0.0625f * (rs[mpr_rat(fx - 1, fy - 1)] + rs[mpr_rat(fx + 1, fy - 1)] + rs[mpr_rat(fx - 1, fy + 1)] +
+                                rs[mpr_rat(fx + 1, fy + 1)]) +
+                     0.125f * (rs[mpr_rat(fx, fy - 1)] + rs[mpr_rat(fx, fy + 1)] + rs[mpr_rat(fx - 1, fy)] +
+                               rs[mpr_rat(fx + 1, fy)]) +
+                     0.25f * rs[mpr_rat(fx, fy)];
     mplane(b, C, M_B)[(long long)J * C.ld + I] = r4;
     store_mirrored(mplane(b, C, M_X), C.ld, I, J, C.W, per, 0.0f);
 }
@@ -1721,6 +1729,110 @@ __global__ void __launch_bounds__(256) k_state_pack(BatchDev b, double* stage, c
             for (int i = lane; i < nc; i += 32) store_mirrored(row, 0, i, 0, d.W, d.periodic, srow[i]);
         }
     }
+}
+
+}  // namespace cfd
+
+// ---------------------------------------------------------------------------
+// The sip9p() seam (cfd_sip_solve, PSolver.cpp:2067-2278): a one-case batch whose pressure
+// stencil is the caller's nine stored planes instead of the grid's. The solve is the step's
+// own BiCGStab + multigrid, run on the correction e of A (phi0 + e) = q with e = 0 on the
+// boundary rows (and, without periodic xi, the boundary columns), as sip9p holds them.
+namespace cfd {
+
+// caller's [j][i] arrays -> case 0's padded planes: the stencil on the unknown cells (zero
+// elsewhere, as k_assemble_p leaves it) in FP64 and as multigrid level 0, phi0 into P_SI and
+// q into P_VORT at every stored point; a periodic case's halo columns take the wrap
+__global__ void k_sip_pack(BatchDev b, SipIn in) {
+    const CaseDev& c = b.cases[0];
+    const int W = c.W, per = c.periodic;
+    const int ncols = W + 2 * H;  // padded columns -H .. W + H - 1
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)c.n1 * ncols) return;
+    const int j = (int)(e / ncols), col = (int)(e % ncols) - H;
+    int i = col;  // the caller's column
+    if (per) i = col < 0 ? col + W : (col >= W ? col - W : col);
+    else if (col < 0 || col >= c.n0) return;
+    const long long src = (long long)j * in.n0 + i;
+    const long long k = (long long)j * c.ld + col;
+    const bool unknown = j >= 1 && j <= c.n1 - 2 && i >= c.ilo && i <= c.ihi;
+    const LevelDev& L0 = c.lev[0];
+    const long long k0 = (long long)j * L0.ld + col;
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+        const double v = unknown ? in.a[q][src] : 0.0;
+        plane(b, c, P_AP + q)[k] = v;
+        mplane(b, L0, M_AP + q)[k0] = (float)v;
+    }
+    plane(b, c, P_SI)[k] = in.phi[src];
+    plane(b, c, P_VORT)[k] = in.q[src];
+}
+
+// r0 = q - A phi0 on the unknown cells (phi0's boundary values enter through the stencil),
+// then the pressure solve's start as k_face_q leaves it for a step: r0 is the right-hand
+// side, the shadow residual and the first preconditioner input; the iterate starts at zero
+__global__ void __launch_bounds__(NT) k_sip_init(BatchDev b) {
+    const Tile t = b.jtiles[blockIdx.x];
+    const CaseDev& c = b.cases[t.c];
+    const int tid = threadIdx.x, li = tid % TX, lj = tid / TX, i = t.i0 + li;
+    const int ld = c.ld;
+    const double* X = plane(b, c, P_SI);
+    const double* Q = plane(b, c, P_VORT);
+    const LevelDev& L0 = c.lev[0];
+    double red[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int j = t.j0 + lj + h * TY;
+        if (i < c.ilo || i > c.ihi || j > c.n1 - 2) continue;
+        const long long k = (long long)j * ld + i;
+        const double ax = plane(b, c, P_AP)[k] * X[k] + plane(b, c, P_AE)[k] * X[k + 1] +
+                          plane(b, c, P_AW)[k] * X[k - 1] + plane(b, c, P_AN)[k] * X[k + ld] +
+                          plane(b, c, P_AS)[k] * X[k - ld] + plane(b, c, P_ANE)[k] * X[k + ld + 1] +
+                          plane(b, c, P_ANW)[k] * X[k + ld - 1] + plane(b, c, P_ASE)[k] * X[k - ld + 1] +
+                          plane(b, c, P_ASW)[k] * X[k - ld - 1];
+        const double r = Q[k] - ax;
+        plane(b, c, P_Q)[k] = r;
+        plane(b, c, P_KR)[k] = r;
+        mplane(b, L0, M_B)[(long long)j * L0.ld + i] = (float)r;
+        red[0] += fabs(r);
+        red[1] += r * r;
+        red[2] = fmax(red[2], fabs(r));
+    }
+    if (case_reduce<3, 0x4u>(b, t.c, blockIdx.x, c.jt_begin, c.jt_count, red) && tid == 0) {
+        double* sc = b.scal + (long long)t.c * NSCAL;
+        int* is = b.iscal + (long long)t.c * NISCAL;
+        sc[S_QL1] = red[0];
+        sc[S_QL2] = sqrt(red[1]);
+        sc[S_QMAX] = red[2];
+        sc[S_RHO] = red[1];
+        sc[S_ALPHA] = 1.0;
+        sc[S_OMEGA] = 1.0;
+        sc[S_BETA] = 0.0;
+        sc[S_NB1] = red[0];
+        sc[S_RL1] = red[0];
+        is[I_PIT] = 0;
+        is[I_PSTATUS] = 0;
+        if (red[0] == 0.0 || !isfinite(red[0])) {
+            is[I_PDONE] = 1;
+            if (!isfinite(red[0])) is[I_STATUS] |= ST_NAN;
+        } else {
+            is[I_PDONE] = 0;
+            atomicAdd(b.active, 1);
+        }
+    }
+}
+
+// phi = phi0 + e on the unknown cells of the caller's [j][i] array (a periodic case's seam
+// column n0 - 1 repeats column 0); boundary values are left as the caller gave them
+__global__ void k_sip_out(BatchDev b, double* phi, int n0) {
+    const CaseDev& c = b.cases[0];
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)c.n1 * n0) return;
+    const int j = (int)(e / n0), i = (int)(e % n0);
+    const int col = (c.periodic && i == n0 - 1) ? 0 : i;
+    if (j < 1 || j > c.n1 - 2 || col < c.ilo || col > c.ihi) return;
+    const long long k = (long long)j * c.ld + col;
+    phi[e] = plane(b, c, P_SI)[k] + plane(b, c, P_PCOR)[k];
 }
 
 }  // namespace cfd

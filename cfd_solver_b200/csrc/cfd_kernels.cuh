@@ -27,4 +27,14 @@ __global__ void k_si(BatchDev b);
 __global__ void k_state_pack(BatchDev b, double* stage, const long long* off, int to_stage);
 __global__ void k_loop_cond(cudaGraphConditionalHandle h, const int* flag, int* counter, int maxc, int* total);
 __global__ void k_if_cond(cudaGraphConditionalHandle h, const int* flag, int* total);
+// the sip9p() seam: the caller's stencil (in the plane order P_AP .. P_ASW), phi0 and q
+struct SipIn {
+    const double* a[9];
+    const double* phi;
+    const double* q;
+    int n0;
+};
+__global__ void k_sip_pack(BatchDev b, SipIn in);
+__global__ void k_sip_init(BatchDev b);
+__global__ void k_sip_out(BatchDev b, double* phi, int n0);
 }  // namespace cfd

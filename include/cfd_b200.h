@@ -256,6 +256,22 @@ int cfd_batch_work(cfd_batch* b, unsigned long long* out4);
 int cfd_gauss_solve(int n0, int n1, int periodic, const double* const* coef, double* phi,
                     const double* q, double tol, int maxit, int* sweeps, void* stream);
 
+/* ---- the sip9p() seam on device arrays (replaces PSolver.cpp:2067-2278, called at :1466)
+ * Solves the pressure-correction system given its 9 stored coefficient planes in sip9p()'s
+ * argument order (ap, ae, as, an, aw, ase, asw, ane, anw), each a device array of n1*n0
+ * float64 in [j][i] order; phi (device, in/out) carries the initial guess and the boundary
+ * values, which stay fixed as sip9p holds them (rows j = 0 and n1-1, and with periodic = 0
+ * columns 0 and n0-1); q is the right-hand side. periodic = 1: xi is periodic with the seam
+ * column n0-1 duplicating column 0. BiCGStab preconditioned by a Galerkin multigrid V-cycle
+ * built from the given planes (replacing the SIP iteration, which has no parallel form)
+ * until the L1 residual is below tol times the initial one (sip9p's rule,
+ * PSolver.cpp:2259). The call allocates a one-case batch for the solve (device memory of
+ * about cfd_case_bytes(n0, n1, profile)), waits for `stream` before it starts, and returns
+ * once phi is written. Returns CFD_OK, CFD_E_MAXITER, CFD_E_BREAKDOWN or CFD_E_DIVERGED;
+ * *iters receives the BiCGStab iterations. */
+int cfd_sip_solve(int n0, int n1, int periodic, const double* const* coef9, double* phi,
+                  const double* q, double tol, int maxit, int* iters, void* stream);
+
 /* Same solve as cfd_gauss_solve() for callers that cannot allocate device memory: hosts
  * whose device memory belongs to another allocator or budget, loops that must not take
  * the allocator's locks or meet an out-of-memory failure mid-step. No counterpart in the
@@ -293,11 +309,12 @@ size_t cfd_batch_state_bytes(cfd_batch* b);
 int cfd_batch_get_state(cfd_batch* b, void* host, size_t bytes);
 int cfd_batch_set_state(cfd_batch* b, const void* host, size_t bytes);
 /* Checkpoint files, in place of the reference's restart file spa100.dat (PSolver.cpp:2006-2016,
- * whose C++ writer dumps pointers): "CFDB200C", u32 version (2), u32 number of cases, per
- * case i32 n0, n1, profile, precision, the state image above, u64 FNV-1a hash of all
- * preceding bytes (little-endian). cfd_batch_load() checks magic, version, every case's
- * geometry and precision against the batch, and the hash, and fails with CFD_E_ARG
- * (the batch untouched) on any mismatch. */
+ * whose C++ writer dumps pointers): "CFDB200C", u32 version (3), u32 number of cases, per
+ * case i32 n0, n1, profile, precision and a u64 fingerprint of its grid (x, y, the metrics
+ * and J), the state image above, u64 FNV-1a hash of all preceding bytes (little-endian).
+ * cfd_batch_load() checks magic, version, every case's geometry, precision and grid
+ * fingerprint against the batch, and the hash, and fails with CFD_E_ARG (the batch
+ * untouched) on any mismatch. */
 int cfd_batch_save(cfd_batch* b, const char* path);
 int cfd_batch_load(cfd_batch* b, const char* path);
 

@@ -15,16 +15,22 @@
 #
 # Outputs go only to oracle/_ref/ (git-ignored): cfd_ref (350x570 capacity, the
 # reference's own) and cfd_ref_big (1040x1040 capacity, for 513^2 / 1025^2 grids).
+#
+#   oracle/build_ref.sh [--if-present]   # --if-present: exit 0 when the sources are absent
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REF_DIR="${CFD_REFERENCE_DIR:-/root/reference}"
 SRC="$REF_DIR/s.cpp"
 OUT="$HERE/_ref"
-mkdir -p "$OUT"
 if [ ! -f "$SRC" ]; then
-    echo "build_ref.sh: reference source $SRC not found" >&2
+    if [ "${1:-}" = "--if-present" ]; then
+        echo "build_ref.sh: reference source not present; oracle/_ref/cfd_ref not rebuilt" >&2
+        exit 0
+    fi
+    echo "build_ref.sh: reference source $SRC not found (set CFD_REFERENCE_DIR)" >&2
     exit 1
 fi
+mkdir -p "$OUT"
 
 transform() {
     awk '

@@ -6,7 +6,7 @@ per-step diagnostics and (for one case) its assembled coefficient planes.
 Entries the reference never assigns (us/vs on the boundary rows, q on the seam
 column, 4th-order coefficients on the 9-point rows) are stored as NaN.
 
-    python tests/golden/make_golden.py        # needs /root/reference (this container only)
+    python tests/golden/make_golden.py        # needs the compiled reference (oracle/build_ref.sh)
 """
 from __future__ import annotations
 

@@ -13,7 +13,8 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 FIX = Path(__file__).with_name("golden") / "c2_twin513_2steps.npz"
-TIGHT_GPU = dict(tol_mom=1e-13, atol_mom=1e-13, maxit_mom=2000, tol_p=1e-12, atol_p=1e-12, maxit_p=600)
+# absolute floors are L1 sums over the 262,656 unknown cells: 1e-9 is ~4e-15 per cell
+TIGHT_GPU = dict(tol_mom=1e-13, atol_mom=1e-9, maxit_mom=2000, tol_p=1e-12, atol_p=1e-9, maxit_p=600)
 
 
 @pytest.mark.skipif(not FIX.exists(), reason="golden 513 x 513 state not generated")

@@ -86,6 +86,11 @@ def test_checkpoint_file_restart_is_exact(tmp_path):
     with Batch(gs[:2], ps[:2]) as other:
         with pytest.raises(_lib.CfdError, match="does not match"):
             other.load(ck)
+    # the same sizes, profiles and precision on another grid (another skew) are rejected too
+    moved = [ogrid(g.n0, g.n1, skew=0.17) if g.kind == "ogrid" else cavity(g.n0, g.n1, skew=0.17) for g in gs]
+    with Batch(moved, ps) as other:
+        with pytest.raises(_lib.CfdError, match="another grid"):
+            other.load(ck)
 
 
 def test_state_image_layout():

@@ -1,23 +1,16 @@
 """The output writers reproduce the reference's files byte for byte when given the
 reference's own fields (the oracle restatement is bit-exact with the reference)."""
-import os
-from pathlib import Path
-
 import numpy as np
 import pytest
 
 from cfd_solver_b200.grid import ogrid
 from cfd_solver_b200.outputs import parse_spt, write_coeff_his, write_spt, write_surf_dist
+from oracle import refrun
 
-REF = Path(os.environ.get("CFD_REFERENCE_DIR", "/root/reference"))
 
-
-@pytest.mark.skipif(not (REF / "s.cpp").exists(), reason="reference sources not present")
+@pytest.mark.skipif(not (refrun.REF_DIR / "cfd_ref").exists(),
+                    reason="compiled reference not built (oracle/build_ref.sh)")
 def test_writers_match_reference_files(tmp_path, oracle_lib):
-    from oracle import refrun
-    if not refrun.REF_DIR.joinpath("cfd_ref").exists():
-        import subprocess
-        subprocess.run([str(refrun.HERE / "build_ref.sh")], check=True)
     g = ogrid(24, 18, skew=0.1)
     prm = dict(Re=100.0, Ri=1.0, dt=1e-3)
     r = refrun.run(g, 1, prm)  # loop 0 writes the files
