@@ -31,7 +31,8 @@ SYMBOLS = ("cfd_params_default", "cfd_last_error", "cfd_device_count", "cfd_set_
            "cfd_gauss_solve", "cfd_gauss_solve_noalloc", "cfd_batch_fetch_stats", "cfd_batch_admit",
            "cfd_batch_set_active", "cfd_serve", "cfd_batch_set_mg", "cfd_batch_get_mg",
            "cfd_batch_autotune", "cfd_batch_save", "cfd_batch_load", "cfd_grid_generate",
-           "cfd_batch_admit_spec", "cfd_batch_set_wait_limit", "cfd_sip_solve")
+           "cfd_batch_admit_spec", "cfd_batch_set_wait_limit", "cfd_sip_solve", "cfd_pool_create",
+           "cfd_pool_admit", "cfd_pool_release", "cfd_pool_free", "cfd_pool_case_bytes")
 
 _D = ctypes.c_double
 _PD = ctypes.POINTER(ctypes.c_double)
@@ -159,6 +160,12 @@ def lib():
     ip = ctypes.POINTER(ctypes.c_int)
     L.cfd_batch_get_mg.argtypes = [vp, ip, ip, ip, ip]
     L.cfd_batch_set_wait_limit.argtypes = [vp, ctypes.c_longlong]
+    L.cfd_pool_create.argtypes = [ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.cfd_pool_admit.argtypes = [vp, ctypes.POINTER(CfdGrid), ctypes.POINTER(CfdParams), ip]
+    L.cfd_pool_release.argtypes = [vp, ctypes.c_int]
+    L.cfd_pool_free.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+    L.cfd_pool_case_bytes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.cfd_pool_case_bytes.restype = ctypes.c_size_t
     L.cfd_batch_autotune.argtypes = [vp, ctypes.c_int, ip, ctypes.POINTER(ctypes.c_double)]
     L.cfd_batch_save.argtypes = [vp, ctypes.c_char_p]
     L.cfd_batch_load.argtypes = [vp, ctypes.c_char_p]
@@ -167,7 +174,7 @@ def lib():
     L.cfd_serve.argtypes = [ctypes.POINTER(CfdServeConfig), ctypes.POINTER(CfdRequest), ctypes.c_int,
                             ctypes.POINTER(CfdResult), ctypes.POINTER(CfdServeStats)]
     special = {"cfd_params_default", "cfd_last_error", "cfd_case_bytes", "cfd_batch_stream",
-               "cfd_batch_launches", "cfd_batch_state_bytes"}
+               "cfd_batch_launches", "cfd_batch_state_bytes", "cfd_pool_case_bytes"}
     for name in SYMBOLS:
         if name not in special:
             getattr(L, name).restype = ctypes.c_int

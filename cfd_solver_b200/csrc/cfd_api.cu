@@ -182,7 +182,15 @@ struct cfd_batch {
     long long* stage_off = nullptr; // per-case offsets into it (doubles)
     Tile* dtiles = nullptr;
     int* dcc = nullptr;
+    size_t cap_tiles = 0, cap_cc = 0, cap_partial = 0, cap_tword = 0;  // table allocations (entries)
+    int ntable_cases = 0;    // cases in the tile tables (one coarsest level each)
     char* dtmaps = nullptr;  // two CUtensorMaps per case
+    // slot pool (cfd_pool_create): cases are placed in one byte arena at admission
+    bool is_pool = false;
+    size_t pool_bytes = 0;
+    std::vector<std::pair<size_t, size_t>> pool_free;  // free regions (offset, bytes), sorted
+    std::vector<std::pair<size_t, size_t>> pool_region; // per case: its region, or (0, 0)
+    size_t stage_bytes = 0;
     BatchDev bd{};
     int nlev_max = 0;
     int ncol[MAXLEV] = {};
@@ -576,7 +584,7 @@ int run_vcycle(cfd_batch* b) {
     }
     {
         Prof pr(b, K_MG_COARSE);
-        k_mg_coarse<<<b->n, 1024, 0, b->st>>>(bd, -1, b->coarse_sweeps);
+        k_mg_coarse<<<b->ntable_cases, 1024, 0, b->st>>>(bd, -1, b->coarse_sweeps);
     }
     for (int l = b->nlev_max - 2; l >= 0; l--) {
         if (bd.nmtiles[l] == 0) continue;
@@ -798,6 +806,7 @@ int build_step_graph(cfd_batch* b, int cur) {
 
 int one_step(cfd_batch* b) {
     int rc;
+    if (b->ntable_cases == 0) return CFD_OK;  // an empty slot pool: nothing to step
     if (b->use_graph && !b->prof) {
         if (!b->gexec[b->cur]) {
             rc = build_step_graph(b, b->cur);
@@ -949,6 +958,167 @@ int upload_case(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, boo
     return upload_state(b, c, g, p, setup);
 }
 
+namespace {
+// ---- a case's place in the arenas, and the tile tables over a set of cases
+
+// the multigrid levels and the precision-form planes of case d in the FP32 arena from
+// offset off32 (words, 32-aligned): G.words32() words
+void place_levels(CaseDev& d, const CaseGeom& G, long long off32) {
+    d.nlev = (int)G.lev.size();
+    for (int l = 0; l < d.nlev; l++) {
+        const LevelGeom& lg = G.lev[l];
+        LevelDev& L = d.lev[l];
+        L.W = lg.W; L.n1 = lg.n1; L.ld = lg.ld; L.ilo = lg.ilo; L.ihi = lg.ihi; L.nlo = lg.ilo;
+        L.base = off32 + 32 - H;
+        L.ps = lg.ps;
+        off32 += (long long)NMG * lg.ps + 32;
+        off32 = rup(off32, 32);
+    }
+    d.xld = G.xld;
+    d.xps = G.xps;
+    d.xbase = off32 + 32 - H32;
+}
+
+int set_kernel_attributes(cfd_batch* b) {
+    b->sw_smem = b->precision == CFD_PRECISION_MIXED ? sweep_smem_mx() : sweep_smem_f64();
+    const void* swk = b->precision == CFD_PRECISION_MIXED ? (const void*)k_sweep_mx : (const void*)k_sweep_f64;
+    CK(cudaFuncSetAttribute(swk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->sw_smem));
+    CK(cudaFuncSetAttribute(swk, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    CK(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem));
+    CK(cudaFuncSetAttribute(k_face_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFaceQSmem));
+    return CFD_OK;
+}
+
+// grows a device table to at least `need` entries of `sz` bytes (contents not kept)
+template <typename T>
+int grow(T*& ptr, size_t& cap, size_t need) {
+    need = std::max<size_t>(need, 1);
+    if (need <= cap) return CFD_OK;
+    cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    const cudaError_t e = cudaMalloc((void**)&ptr, sizeof(T) * need);
+    if (e != cudaSuccess) return fail(CFD_E_OOM, std::string("tile tables: ") + cudaGetErrorString(e));
+    cap = need;
+    return CFD_OK;
+}
+
+// The tile tables of the cases `ids` (in that order; a case's tiles in row-major tile order,
+// so every per-case reduction sums in the same order whatever else is in the tables), each
+// case's offsets into them, the batch-wide maxima the launches use, and the device copies.
+// The step graphs hold the old tables and are dropped.
+int build_tables(cfd_batch* b, const std::vector<int>& ids) {
+    CK(cudaStreamSynchronize(b->st));
+    std::vector<Tile> ftiles, jtiles;
+    std::vector<std::vector<Tile>> at(MAXLEV), mt(MAXLEV);
+    std::vector<std::vector<int>> cc(MAXLEV);
+    b->nlev_max = 0;
+    b->max_W = 0;
+    b->maxit_mom = 0;
+    b->maxit_p = 0;
+    for (int l = 0; l < MAXLEV; l++) b->ncol[l] = 0;
+    int jt_max = 0;
+    for (int c : ids) {
+        CaseDev& d = b->hc[c];
+        d.tile_begin = (int)ftiles.size();
+        make_tiles(d.ilo, d.ihi, d.n1, c, ftiles);
+        d.tile_count = (int)ftiles.size() - d.tile_begin;
+        d.jt_begin = (int)jtiles.size();
+        make_tiles(d.ilo, d.ihi, d.n1, c, jtiles, TYJ);
+        d.jt_count = (int)jtiles.size() - d.jt_begin;
+        for (int l = 0; l < d.nlev; l++) {
+            LevelDev& L = d.lev[l];
+            L.tile_begin = (int)at[l].size();
+            make_tiles(L.ilo, L.ihi, L.n1, c, at[l]);
+            L.tile_count = (int)at[l].size() - L.tile_begin;
+            if (l < d.nlev - 1) make_tiles(L.ilo, L.ihi, L.n1, c, mt[l], TYJ);
+            else cc[l].push_back(c);
+            b->ncol[l] = std::max(b->ncol[l], (d.periodic && (L.W & 1)) ? 6 : 4);
+        }
+        b->nlev_max = std::max(b->nlev_max, d.nlev);
+        b->max_W = std::max(b->max_W, d.W);
+        b->maxit_mom = std::max(b->maxit_mom, b->prm[c].maxit_mom);
+        b->maxit_p = std::max(b->maxit_p, b->prm[c].maxit_p);
+        jt_max = std::max(jt_max, d.jt_count);
+    }
+    std::vector<Tile> all(ftiles);
+    const size_t pos_jt = all.size();
+    all.insert(all.end(), jtiles.begin(), jtiles.end());
+    std::vector<int> allcc;
+    size_t pos_at[MAXLEV], pos_mt[MAXLEV], pos_cc[MAXLEV];
+    for (int l = 0; l < MAXLEV; l++) {
+        pos_at[l] = all.size();
+        all.insert(all.end(), at[l].begin(), at[l].end());
+        pos_mt[l] = all.size();
+        all.insert(all.end(), mt[l].begin(), mt[l].end());
+        pos_cc[l] = allcc.size();
+        allcc.insert(allcc.end(), cc[l].begin(), cc[l].end());
+    }
+    if (int rc = grow(b->dtiles, b->cap_tiles, all.size())) return rc;
+    if (int rc = grow(b->dcc, b->cap_cc, allcc.size())) return rc;
+    if (int rc = grow(b->partial, b->cap_partial, PSTRIDE * std::max(ftiles.size(), jtiles.size() * SW_WARPS)))
+        return rc;
+    if (int rc = grow(b->tword, b->cap_tword, jtiles.size())) return rc;
+    if (!all.empty())
+        CK(cudaMemcpyAsync(b->dtiles, all.data(), sizeof(Tile) * all.size(), cudaMemcpyHostToDevice, b->st));
+    if (!allcc.empty())
+        CK(cudaMemcpyAsync(b->dcc, allcc.data(), sizeof(int) * allcc.size(), cudaMemcpyHostToDevice, b->st));
+    CK(cudaMemcpyAsync(b->dc, b->hc.data(), sizeof(CaseDev) * b->n, cudaMemcpyHostToDevice, b->st));
+    BatchDev& bd = b->bd;
+    bd.partial = b->partial;
+    bd.tword = b->tword;
+    bd.ftiles = b->dtiles;
+    bd.nftiles = (int)ftiles.size();
+    bd.jtiles = b->dtiles + pos_jt;
+    bd.njtiles = (int)jtiles.size();
+    for (int l = 0; l < MAXLEV; l++) {
+        bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
+        bd.mtiles[l] = b->dtiles + pos_mt[l]; bd.nmtiles[l] = (int)mt[l].size();
+        bd.ccases[l] = b->dcc + pos_cc[l]; bd.nccases[l] = (int)cc[l].size();
+    }
+    b->ntable_cases = (int)ids.size();
+    b->sw_grid = (int)jtiles.size();  // one CTA per 32 x 16 tile
+    b->swf_threads = jt_max >= 1024 ? SWF_THREADS : 128;
+    const size_t bc_smem = 2 * (size_t)(b->max_W + 1) * sizeof(double);
+    if (bc_smem > 48 * 1024)
+        CK(cudaFuncSetAttribute(k_bc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bc_smem));
+    drop_graphs(b);
+    CK(cudaStreamSynchronize(b->st));
+    return CFD_OK;
+}
+
+// the case's five 3-D tensor maps (x, y = row, z = plane): over the FP64 planes from the halo
+// column -2 (x = column + 2), boxes 36 x 20 (tile + halo), 32 x 16 (tile) and 32 x 16 x 3
+// (three consecutive planes); over the FP32 correction planes from column -4 (x = column + 4,
+// so both boxes start on 16-byte boundaries), 40 x 20 and 32 x 16
+int encode_tmaps(cfd_batch* b, const CaseDev& d, unsigned char* mc) {
+    EncodeTiledFn enc = tensor_map_encoder();
+    if (!enc) return fail(CFD_E_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint32_t es[3] = {1, 1, 1};
+    auto make = [&](int off, CUtensorMapDataType ty, void* gaddr, const cuuint64_t* dims, const cuuint64_t* strides,
+                    const cuuint32_t* box) {
+        return enc(reinterpret_cast<CUtensorMap*>(mc + off), ty, 3, gaddr, dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    };
+    const cuuint64_t d64[3] = {(cuuint64_t)d.ld, (cuuint64_t)d.n1, (cuuint64_t)NPLANES};
+    const cuuint64_t s64[2] = {(cuuint64_t)d.ld * 8, (cuuint64_t)d.ps * 8};
+    const cuuint32_t bh[3] = {TX + 4, TYJ + 4, 1}, bt[3] = {TX, TYJ, 1}, bt3[3] = {TX, TYJ, 3};
+    const cuuint64_t d32[3] = {(cuuint64_t)d.xld, (cuuint64_t)d.n1, (cuuint64_t)NXPLANES};
+    const cuuint64_t s32[2] = {(cuuint64_t)d.xld * 4, (cuuint64_t)d.xps * 4};
+    const cuuint32_t xh[3] = {TX + 8, TYJ + 4, 1};
+    void* g64 = b->f64 + d.base + H - 2;
+    void* g32 = b->f32 + d.xbase;
+    CUresult r = make(TMAP_F64_HALO, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, g64, d64, s64, bh);
+    if (r == CUDA_SUCCESS) r = make(TMAP_F64_TILE, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, g64, d64, s64, bt);
+    if (r == CUDA_SUCCESS) r = make(TMAP_F64_TILE3, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, g64, d64, s64, bt3);
+    if (r == CUDA_SUCCESS) r = make(TMAP_X32_HALO, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g32, d32, s32, xh);
+    if (r == CUDA_SUCCESS) r = make(TMAP_X32_TILE, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g32, d32, s32, bt);
+    if (r != CUDA_SUCCESS) return fail(CFD_E_CUDA, "cuTensorMapEncodeTiled failed");
+    return CFD_OK;
+}
+}  // namespace
+
 int cfd_internal_grid_gen(const cfd_grid_spec* spec, double* d_planes, double* d_normals, cudaStream_t stream);
 
 // Case `c` from a grid generated on the device into `gen` (10 planes, 4 normal rows, 5
@@ -1064,17 +1234,12 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess)
         return cleanup(fail(CFD_E_CUDA, "stream creation failed"));
 
-    // ---- geometry, offsets, tiles
+    // ---- geometry, offsets
     long long off64 = 0, off32 = 0;
-    std::vector<Tile> ftiles, jtiles;
-    std::vector<std::vector<Tile>> at(MAXLEV), mt(MAXLEV);
-    std::vector<std::vector<int>> cc(MAXLEV);
     b->hc.resize(ncases);
     b->prm.assign(params, params + ncases);
     b->q_l2_first.assign(ncases, -1.0);
     b->sr_first.assign(ncases, -1.0);
-    b->maxit_mom = 0;
-    b->maxit_p = 0;
     for (int c = 0; c < ncases; c++) {
         const cfd_grid& g = grids[c];
         const cfd_params& p = params[c];
@@ -1089,37 +1254,10 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         off64 += G.bytes64() - 16 + 16;
         off64 = rup(off64, 16);
         case_params_to_dev(d, g, p);
-        d.tile_begin = (int)ftiles.size();
-        make_tiles(G.ilo, G.ihi, g.n1, c, ftiles);
-        d.tile_count = (int)ftiles.size() - d.tile_begin;
-        d.jt_begin = (int)jtiles.size();
-        make_tiles(G.ilo, G.ihi, g.n1, c, jtiles, TYJ);
-        d.jt_count = (int)jtiles.size() - d.jt_begin;
-        d.nlev = (int)G.lev.size();
-        for (int l = 0; l < d.nlev; l++) {
-            const LevelGeom& lg = G.lev[l];
-            LevelDev& L = d.lev[l];
-            L.W = lg.W; L.n1 = lg.n1; L.ld = lg.ld; L.ilo = lg.ilo; L.ihi = lg.ihi; L.nlo = lg.ilo;
-            L.base = off32 + 32 - H;
-            L.ps = lg.ps;
-            off32 += (long long)NMG * lg.ps + 32;
-            off32 = rup(off32, 32);
-            L.tile_begin = (int)at[l].size();
-            make_tiles(lg.ilo, lg.ihi, lg.n1, c, at[l]);
-            L.tile_count = (int)at[l].size() - L.tile_begin;
-            if (l < d.nlev - 1) make_tiles(lg.ilo, lg.ihi, lg.n1, c, mt[l], TYJ);
-            else cc[l].push_back(c);
-            b->ncol[l] = std::max(b->ncol[l], (G.periodic && (lg.W & 1)) ? 6 : 4);
-        }
-        d.xld = G.xld;
-        d.xps = G.xps;
-        d.xbase = off32 + 32 - H32;
-        off32 += (long long)NXPLANES * G.xps + 32;
+        place_levels(d, G, off32);
+        off32 += G.words32();
         off32 = rup(off32, 32);
-        b->nlev_max = std::max(b->nlev_max, d.nlev);
         b->max_W = std::max(b->max_W, d.W);
-        b->maxit_mom = std::max(b->maxit_mom, p.maxit_mom);
-        b->maxit_p = std::max(b->maxit_p, p.maxit_p);
         if (c == 0) b->precision = p.precision;
         if (p.precision != b->precision)
             return cleanup(fail(CFD_E_ARG, "all cases of a batch must use the same precision"));
@@ -1128,11 +1266,7 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     b->n64 = off64 + 16;
     b->n32 = off32 + 32;
 
-    // ---- device allocations
-    size_t ntl = ftiles.size() + jtiles.size();
-    for (int l = 0; l < MAXLEV; l++) ntl += at[l].size() + mt[l].size();
-    size_t ncc = 0;
-    for (int l = 0; l < MAXLEV; l++) ncc += cc[l].size();
+    // ---- device allocations (the tile tables: build_tables)
 #define ALLOC(ptr, bytes)                                                         \
     do {                                                                          \
         cudaError_t e_ = cudaMalloc((void**)&(ptr), (bytes));                     \
@@ -1144,15 +1278,10 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     ALLOC(b->dc, sizeof(CaseDev) * ncases);
     ALLOC(b->scal, sizeof(double) * NSCAL * ncases);
     ALLOC(b->iscal, sizeof(int) * NISCAL * ncases);
-    ALLOC(b->partial, sizeof(double) * PSTRIDE *
-                          std::max<size_t>(std::max(ftiles.size(), jtiles.size() * SW_WARPS), 1));
     ALLOC(b->counter, sizeof(unsigned) * ncases);
     ALLOC(b->flags, sizeof(int) * NFLAGS);
     ALLOC(b->work, sizeof(unsigned long long) * 4);
-    ALLOC(b->tword, sizeof(int) * std::max<size_t>(jtiles.size(), 1));
     ALLOC(b->dtmaps, (size_t)TMAP_STRIDE * ncases);
-    ALLOC(b->dtiles, sizeof(Tile) * std::max<size_t>(ntl, 1));
-    ALLOC(b->dcc, sizeof(int) * std::max<size_t>(ncc, 1));
 #undef ALLOC
     if (cudaHostAlloc((void**)&b->h_flags, sizeof(int) * NFLAGS, cudaHostAllocDefault) != cudaSuccess)
         return cleanup(fail(CFD_E_CUDA, "pinned allocation failed"));
@@ -1168,92 +1297,33 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
         const size_t smem = 2 * (size_t)(b->max_W + 1) * sizeof(double);
         if (smem > 48 * 1024)
             CK(cudaFuncSetAttribute(k_bc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        b->sw_smem = b->precision == CFD_PRECISION_MIXED ? sweep_smem_mx() : sweep_smem_f64();
-        const void* swk = b->precision == CFD_PRECISION_MIXED ? (const void*)k_sweep_mx : (const void*)k_sweep_f64;
-        CK(cudaFuncSetAttribute(swk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->sw_smem));
-        CK(cudaFuncSetAttribute(swk, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-        b->sw_grid = (int)jtiles.size();  // one CTA per 32 x 16 tile
-        int jt_max = 0;
-        for (const auto& d : b->hc) jt_max = std::max(jt_max, d.jt_count);
-        b->swf_threads = jt_max >= 1024 ? SWF_THREADS : 128;
-        CK(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem));
-        CK(cudaFuncSetAttribute(k_face_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFaceQSmem));
+        if (int rc = set_kernel_attributes(b)) return cleanup(rc);
     }
-
-    // ---- tile tables
-    std::vector<Tile> all(ftiles);
-    const size_t pos_jt = all.size();
-    all.insert(all.end(), jtiles.begin(), jtiles.end());
-    std::vector<int> allcc;
-    size_t pos_at[MAXLEV], pos_mt[MAXLEV], pos_cc[MAXLEV];
-    for (int l = 0; l < MAXLEV; l++) {
-        pos_at[l] = all.size();
-        all.insert(all.end(), at[l].begin(), at[l].end());
-        pos_mt[l] = all.size();
-        all.insert(all.end(), mt[l].begin(), mt[l].end());
-        pos_cc[l] = allcc.size();
-        allcc.insert(allcc.end(), cc[l].begin(), cc[l].end());
-    }
-    CK(cudaMemcpyAsync(b->dtiles, all.data(), sizeof(Tile) * all.size(), cudaMemcpyHostToDevice, b->st));
-    if (!allcc.empty())
-        CK(cudaMemcpyAsync(b->dcc, allcc.data(), sizeof(int) * allcc.size(), cudaMemcpyHostToDevice, b->st));
-    CK(cudaMemcpyAsync(b->dc, b->hc.data(), sizeof(CaseDev) * ncases, cudaMemcpyHostToDevice, b->st));
 
     BatchDev& bd = b->bd;
     bd.cases = b->dc; bd.ncases = ncases; bd.f64 = b->f64; bd.f32 = b->f32;
-    bd.scal = b->scal; bd.iscal = b->iscal; bd.partial = b->partial; bd.counter = b->counter;
+    bd.scal = b->scal; bd.iscal = b->iscal; bd.counter = b->counter;
     bd.active = b->flags; bd.mactive = b->flags + 1;
     bd.work = b->work;
     bd.tmaps = b->dtmaps;
+    // ---- tile tables over every case
     {
-        // 3-D tensor maps per case (x, y = row, z = plane): over the FP64 planes from the halo
-        // column -2 (x = column + 2), boxes 36 x 20 (tile + halo), 32 x 16 (tile) and
-        // 32 x 16 x 3 (three consecutive planes); over the FP32 correction planes from column
-        // -4 (x = column + 4, so both boxes start on 16-byte boundaries), 40 x 20 and 32 x 16
-        EncodeTiledFn enc = tensor_map_encoder();
-        if (!enc) return cleanup(fail(CFD_E_CUDA, "cuTensorMapEncodeTiled unavailable"));
+        std::vector<int> ids(ncases);
+        for (int c = 0; c < ncases; c++) ids[c] = c;
+        if (int rc = build_tables(b, ids)) return cleanup(rc);
+    }
+    {
         std::vector<unsigned char> maps((size_t)TMAP_STRIDE * ncases);
-        for (int c = 0; c < ncases; c++) {
-            const CaseDev& d = b->hc[c];
-            unsigned char* mc = maps.data() + (size_t)TMAP_STRIDE * c;
-            const cuuint32_t es[3] = {1, 1, 1};
-            auto make = [&](int off, CUtensorMapDataType ty, void* gaddr, const cuuint64_t* dims,
-                            const cuuint64_t* strides, const cuuint32_t* box) {
-                return enc(reinterpret_cast<CUtensorMap*>(mc + off), ty, 3, gaddr, dims, strides, box, es,
-                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-            };
-            const cuuint64_t d64[3] = {(cuuint64_t)d.ld, (cuuint64_t)d.n1, (cuuint64_t)NPLANES};
-            const cuuint64_t s64[2] = {(cuuint64_t)d.ld * 8, (cuuint64_t)d.ps * 8};
-            const cuuint32_t bh[3] = {TX + 4, TYJ + 4, 1}, bt[3] = {TX, TYJ, 1}, bt3[3] = {TX, TYJ, 3};
-            const cuuint64_t d32[3] = {(cuuint64_t)d.xld, (cuuint64_t)d.n1, (cuuint64_t)NXPLANES};
-            const cuuint64_t s32[2] = {(cuuint64_t)d.xld * 4, (cuuint64_t)d.xps * 4};
-            const cuuint32_t xh[3] = {TX + 8, TYJ + 4, 1};
-            void* g64 = b->f64 + d.base + H - 2;
-            void* g32 = b->f32 + d.xbase;
-            CUresult r = make(TMAP_F64_HALO, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, g64, d64, s64, bh);
-            if (r == CUDA_SUCCESS) r = make(TMAP_F64_TILE, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, g64, d64, s64, bt);
-            if (r == CUDA_SUCCESS) r = make(TMAP_F64_TILE3, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, g64, d64, s64, bt3);
-            if (r == CUDA_SUCCESS) r = make(TMAP_X32_HALO, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g32, d32, s32, xh);
-            if (r == CUDA_SUCCESS) r = make(TMAP_X32_TILE, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g32, d32, s32, bt);
-            if (r != CUDA_SUCCESS)
-                return cleanup(fail(CFD_E_CUDA, "cuTensorMapEncodeTiled failed for case " + std::to_string(c)));
-        }
+        for (int c = 0; c < ncases; c++)
+            if (int rc = encode_tmaps(b, b->hc[c], maps.data() + (size_t)TMAP_STRIDE * c))
+                return cleanup(rc);
         CK(cudaMemcpyAsync(b->dtmaps, maps.data(), maps.size(), cudaMemcpyHostToDevice, b->st));
     }
-    bd.ftiles = b->dtiles; bd.nftiles = (int)ftiles.size();
-    bd.jtiles = b->dtiles + pos_jt; bd.njtiles = (int)jtiles.size();
     bd.error = b->flags + 4;
     bd.wait_polls = kWaitPolls;
     bd.mg_res = mg_res_plane(b->mg_pre, b->mg_post, b->mg_fused);
     bd.sweep_no = b->flags + 7;
     bd.mixed = b->precision == CFD_PRECISION_MIXED;
-    bd.tword = b->tword;
-    for (int l = 0; l < MAXLEV; l++) {
-        bd.atiles[l] = b->dtiles + pos_at[l]; bd.natiles[l] = (int)at[l].size();
-        bd.mtiles[l] = b->dtiles + pos_mt[l]; bd.nmtiles[l] = (int)mt[l].size();
-        bd.ccases[l] = b->dcc + pos_cc[l]; bd.nccases[l] = (int)cc[l].size();
-    }
 
     // ---- upload grid + initial state (padded planes with halos)
     b->cur = 0;
@@ -1277,6 +1347,209 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     flush_profile(b);
     *out = b;
     return CFD_OK;
+}
+
+// ---- slot pool: cases placed in one byte arena at admission (no counterpart in the reference)
+namespace {
+constexpr size_t kPoolAlign = 256;
+
+// the bytes a case takes in a pool: its FP64 planes, then its FP32 levels and planes
+size_t pool_case_bytes(const CaseGeom& G) {
+    return rup((long long)G.bytes64() * 8, kPoolAlign) + rup((long long)G.words32() * 4, kPoolAlign);
+}
+
+// first fit in the sorted free list; returns false when no region is large enough
+bool pool_take(cfd_batch* b, size_t bytes, size_t* off) {
+    for (size_t k = 0; k < b->pool_free.size(); k++) {
+        auto& f = b->pool_free[k];
+        if (f.second < bytes) continue;
+        *off = f.first;
+        f.first += bytes;
+        f.second -= bytes;
+        if (f.second == 0) b->pool_free.erase(b->pool_free.begin() + (long)k);
+        return true;
+    }
+    return false;
+}
+
+// returns a region to the free list, merging it with its neighbours
+void pool_give(cfd_batch* b, size_t off, size_t bytes) {
+    auto& v = b->pool_free;
+    auto it = std::lower_bound(v.begin(), v.end(), std::make_pair(off, (size_t)0));
+    it = v.insert(it, {off, bytes});
+    if (it + 1 != v.end() && it->first + it->second == (it + 1)->first) {
+        it->second += (it + 1)->second;
+        v.erase(it + 1);
+    }
+    if (it != v.begin() && (it - 1)->first + (it - 1)->second == it->first) {
+        (it - 1)->second += it->second;
+        v.erase(it);
+    }
+}
+
+std::vector<int> pool_ids(const cfd_batch* b) {
+    std::vector<int> ids;
+    for (int c = 0; c < b->n; c++)
+        if (b->pool_region[c].second) ids.push_back(c);
+    return ids;
+}
+}  // namespace
+
+int cfd_pool_create(size_t hbm_budget, int max_cases, int precision, cfd_batch** out) {
+    if (!out || max_cases <= 0 || max_cases > (1 << 16) || hbm_budget < (1u << 20) ||
+        (precision != CFD_PRECISION_FP64 && precision != CFD_PRECISION_MIXED))
+        return fail(CFD_E_ARG, "cfd_pool_create: bad arguments");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(CFD_E_CUDA, "no CUDA device available (this library has no CPU path)");
+    cfd_batch* b = new cfd_batch();
+    b->n = max_cases;
+    b->is_pool = true;
+    b->precision = precision;
+    cudaGetDevice(&b->dev);
+    auto cleanup = [&](int rc) { cfd_batch_destroy(b); return rc; };
+    if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(CFD_E_CUDA, "stream creation failed"));
+    b->hc.assign(max_cases, CaseDev{});
+    cfd_params dp;
+    cfd_params_default(&dp);
+    dp.precision = precision;
+    b->prm.assign(max_cases, dp);
+    b->geom.assign(max_cases, CaseGeom{});
+    b->pool_region.assign(max_cases, {0, 0});
+    b->pool_bytes = hbm_budget / kPoolAlign * kPoolAlign;
+    b->pool_free.push_back({0, b->pool_bytes});
+#define ALLOC(ptr, bytes)                                                         \
+    do {                                                                          \
+        cudaError_t e_ = cudaMalloc((void**)&(ptr), (bytes));                     \
+        if (e_ != cudaSuccess)                                                    \
+            return cleanup(fail(CFD_E_OOM, std::string("cudaMalloc ") + #ptr + ": " + cudaGetErrorString(e_))); \
+    } while (0)
+    ALLOC(b->f64, b->pool_bytes);
+    b->f32 = reinterpret_cast<float*>(b->f64);  // one arena: a case's FP32 part follows its FP64 part
+    b->n64 = (long long)(b->pool_bytes / 8);
+    b->n32 = (long long)(b->pool_bytes / 4);
+    ALLOC(b->dc, sizeof(CaseDev) * max_cases);
+    ALLOC(b->scal, sizeof(double) * NSCAL * max_cases);
+    ALLOC(b->iscal, sizeof(int) * NISCAL * max_cases);
+    ALLOC(b->counter, sizeof(unsigned) * max_cases);
+    ALLOC(b->flags, sizeof(int) * NFLAGS);
+    ALLOC(b->work, sizeof(unsigned long long) * 4);
+    ALLOC(b->dtmaps, (size_t)TMAP_STRIDE * max_cases);
+#undef ALLOC
+    if (cudaHostAlloc((void**)&b->h_flags, sizeof(int) * NFLAGS, cudaHostAllocDefault) != cudaSuccess)
+        return cleanup(fail(CFD_E_CUDA, "pinned allocation failed"));
+    // every slot starts empty: inactive, its pressure solve done, no momentum word
+    std::vector<int> is((size_t)NISCAL * max_cases, 0);
+    for (int c = 0; c < max_cases; c++) is[(size_t)c * NISCAL + I_PDONE] = 1;
+    if (cudaMemsetAsync(b->scal, 0, sizeof(double) * NSCAL * max_cases, b->st) != cudaSuccess ||
+        cudaMemcpyAsync(b->iscal, is.data(), sizeof(int) * is.size(), cudaMemcpyHostToDevice, b->st) != cudaSuccess ||
+        cudaMemsetAsync(b->counter, 0, sizeof(unsigned) * max_cases, b->st) != cudaSuccess ||
+        cudaMemsetAsync(b->work, 0, sizeof(unsigned long long) * 4, b->st) != cudaSuccess ||
+        cudaMemsetAsync(b->flags, 0, sizeof(int) * NFLAGS, b->st) != cudaSuccess ||
+        cudaStreamSynchronize(b->st) != cudaSuccess)
+        return cleanup(fail(CFD_E_CUDA, "pool initialisation failed"));
+    if (int rc = set_kernel_attributes(b)) return cleanup(rc);
+    BatchDev& bd = b->bd;
+    bd.cases = b->dc; bd.ncases = max_cases; bd.f64 = b->f64; bd.f32 = b->f32;
+    bd.scal = b->scal; bd.iscal = b->iscal; bd.counter = b->counter;
+    bd.active = b->flags; bd.mactive = b->flags + 1;
+    bd.work = b->work;
+    bd.tmaps = b->dtmaps;
+    bd.error = b->flags + 4;
+    bd.wait_polls = kWaitPolls;
+    bd.mg_res = mg_res_plane(b->mg_pre, b->mg_post, b->mg_fused);
+    bd.sweep_no = b->flags + 7;
+    bd.mixed = precision == CFD_PRECISION_MIXED;
+    if (int rc = build_tables(b, {})) return cleanup(rc);
+    *out = b;
+    return CFD_OK;
+}
+
+int cfd_pool_admit(cfd_batch* b, const cfd_grid* g, const cfd_params* p, int* slot) {
+    if (!b || !b->is_pool || !slot) return fail(CFD_E_ARG, "cfd_pool_admit: not a slot pool");
+    *slot = -1;
+    int rc = check_params(g, p);
+    if (rc) return rc;
+    if (p->precision != b->precision) return fail(CFD_E_ARG, "case precision differs from the pool's");
+    int c = 0;
+    while (c < b->n && b->pool_region[c].second) c++;
+    if (c == b->n) return fail(CFD_E_OOM, "every case slot of the pool is taken");
+    const CaseGeom G = case_geom(g->n0, g->n1, p->profile);
+    if (G.W > 4096) return fail(CFD_E_ARG, "grid width above 4096 columns");
+    const size_t bytes = pool_case_bytes(G);
+    size_t off = 0;
+    if (!pool_take(b, bytes, &off)) return fail(CFD_E_OOM, "no free region of the pool's budget fits this case");
+    CK(cudaStreamSynchronize(b->st));
+    CaseDev& d = b->hc[c];
+    memset(&d, 0, sizeof(d));
+    d.W = G.W; d.n0 = g->n0; d.n1 = g->n1; d.ld = G.ld;
+    d.periodic = G.periodic; d.ilo = G.ilo; d.ihi = G.ihi; d.profile = p->profile;
+    d.base = (long long)(off / 8) + 16 - H;
+    d.ps = G.ps;
+    case_params_to_dev(d, *g, *p);
+    place_levels(d, G, (long long)((off + rup((long long)G.bytes64() * 8, kPoolAlign)) / 4));
+    b->geom[c] = G;
+    b->prm[c] = *p;
+    b->pool_region[c] = {off, bytes};
+    std::vector<unsigned char> maps(TMAP_STRIDE);
+    auto undo = [&](int code) {
+        pool_give(b, off, bytes);
+        b->pool_region[c] = {0, 0};
+        memset(&b->hc[c], 0, sizeof(CaseDev));
+        build_tables(b, pool_ids(b));
+        return code;
+    };
+    rc = encode_tmaps(b, d, maps.data());
+    if (rc) return undo(rc);
+    // the region may hold a retired case's planes: every plane starts from zero
+    if (cudaMemsetAsync(reinterpret_cast<char*>(b->f64) + off, 0, bytes, b->st) != cudaSuccess ||
+        cudaMemcpyAsync(b->dtmaps + (size_t)TMAP_STRIDE * c, maps.data(), TMAP_STRIDE, cudaMemcpyHostToDevice,
+                        b->st) != cudaSuccess ||
+        cudaMemsetAsync(b->scal + (size_t)c * NSCAL, 0, sizeof(double) * NSCAL, b->st) != cudaSuccess)
+        return undo(fail(CFD_E_CUDA, "cfd_pool_admit: slot initialisation failed"));
+    rc = build_tables(b, pool_ids(b));
+    if (rc) return undo(rc);
+    rc = upload_case(b, c, *g, *p, true);
+    if (rc) return undo(rc);
+    *slot = c;
+    return CFD_OK;
+}
+
+int cfd_pool_release(cfd_batch* b, int slot) {
+    if (!b || !b->is_pool || slot < 0 || slot >= b->n || !b->pool_region[slot].second)
+        return fail(CFD_E_ARG, "cfd_pool_release: not an occupied slot of a pool");
+    CK(cudaStreamSynchronize(b->st));
+    // the entry leaves every launch: inactive, its pressure solve done, no momentum word
+    int w[NISCAL];
+    CK(cudaMemcpy(w, b->iscal + (size_t)slot * NISCAL, sizeof(w), cudaMemcpyDeviceToHost));
+    w[I_ACTIVE] = 0;
+    w[I_PDONE] = 1;
+    w[I_MWORD] = 0;
+    CK(cudaMemcpy(b->iscal + (size_t)slot * NISCAL, w, sizeof(w), cudaMemcpyHostToDevice));
+    pool_give(b, b->pool_region[slot].first, b->pool_region[slot].second);
+    b->pool_region[slot] = {0, 0};
+    memset(&b->hc[slot], 0, sizeof(CaseDev));
+    b->geom[slot] = CaseGeom{};
+    return build_tables(b, pool_ids(b));
+}
+
+int cfd_pool_free(cfd_batch* b, size_t* free_bytes, size_t* largest) {
+    if (!b || !b->is_pool) return fail(CFD_E_ARG, "cfd_pool_free: not a slot pool");
+    size_t tot = 0, big = 0;
+    for (auto& f : b->pool_free) {
+        tot += f.second;
+        big = std::max(big, f.second);
+    }
+    if (free_bytes) *free_bytes = tot;
+    if (largest) *largest = big;
+    return CFD_OK;
+}
+
+size_t cfd_pool_case_bytes(int n0, int n1, int profile) {
+    if (n0 < 8 || n1 < 6) return 0;
+    return pool_case_bytes(case_geom(n0, n1, profile));
 }
 
 int cfd_batch_step(cfd_batch* b, int nsteps) {
@@ -1321,7 +1594,8 @@ int cfd_batch_destroy(cfd_batch* b) {
     drop_graphs(b);
     for (auto& l : b->pending) { cudaEventDestroy(l.e0); cudaEventDestroy(l.e1); }
     for (auto e : b->pool) cudaEventDestroy(e);
-    cudaFree(b->f64); cudaFree(b->f32); cudaFree(b->dc); cudaFree(b->scal); cudaFree(b->iscal);
+    if ((void*)b->f32 != (void*)b->f64) cudaFree(b->f32);
+    cudaFree(b->f64); cudaFree(b->dc); cudaFree(b->scal); cudaFree(b->iscal);
     cudaFree(b->stage); cudaFree(b->stage_off);
     cudaFree(b->partial); cudaFree(b->counter); cudaFree(b->flags); cudaFree(b->work); cudaFree(b->tword); cudaFree(b->dtiles); cudaFree(b->dcc); cudaFree(b->dtmaps);
     if (b->h_flags) cudaFreeHost(b->h_flags);
@@ -1542,17 +1816,23 @@ static int state_copy(cfd_batch* b, void* host, size_t bytes, bool to_host) {
     if (!b || !host) return fail(CFD_E_ARG, "bad arguments");
     const size_t need = cfd_batch_state_bytes(b);
     if (bytes < need) return fail(CFD_E_ARG, "state buffer too small");
-    if (!b->stage) {
-        std::vector<long long> off(b->n);
-        long long o = 0;
-        for (int c = 0; c < b->n; c++) {
-            off[c] = o;
-            o += state_doubles(b->hc[c]);
-        }
-        CK(cudaMalloc((void**)&b->stage, need));
-        CK(cudaMalloc((void**)&b->stage_off, sizeof(long long) * b->n));
-        CK(cudaMemcpyAsync(b->stage_off, off.data(), sizeof(long long) * b->n, cudaMemcpyHostToDevice, b->st));
+    // per-case offsets into the image (a slot pool's cases change with admissions)
+    std::vector<long long> off(b->n);
+    long long o = 0;
+    for (int c = 0; c < b->n; c++) {
+        off[c] = o;
+        o += state_doubles(b->hc[c]);
     }
+    if (need > b->stage_bytes) {
+        CK(cudaStreamSynchronize(b->st));
+        cudaFree(b->stage);
+        b->stage = nullptr;
+        b->stage_bytes = 0;
+        CK(cudaMalloc((void**)&b->stage, need));
+        b->stage_bytes = need;
+    }
+    if (!b->stage_off) CK(cudaMalloc((void**)&b->stage_off, sizeof(long long) * b->n));
+    CK(cudaMemcpyAsync(b->stage_off, off.data(), sizeof(long long) * b->n, cudaMemcpyHostToDevice, b->st));
     b->bd.cur = b->cur;
     if (to_host) {
         k_state_pack<<<b->n * 7, 256, 0, b->st>>>(b->bd, b->stage, b->stage_off, 1);
@@ -1568,8 +1848,9 @@ static int state_copy(cfd_batch* b, void* host, size_t bytes, bool to_host) {
 }
 
 // Checkpoint file (replaces the reference's spa100.dat restart writer, PSolver.cpp:2006-2016):
-//   "CFDB200C" | u32 version 2 | u32 cases | per case i32 n0, n1, profile, precision |
-//   the state image of cfd_batch_get_state | u64 FNV-1a hash of all preceding bytes
+//   "CFDB200C" | u32 version 3 | u32 cases | per case i32 n0, n1, profile, precision and a
+//   u64 grid fingerprint | the state image of cfd_batch_get_state | u64 FNV-1a hash of all
+//   preceding bytes
 namespace {
 const char kCkptMagic[8] = {'C', 'F', 'D', 'B', '2', '0', '0', 'C'};
 // 1: padded device planes in the state image; 2: stored columns only; 3: a grid fingerprint per case

@@ -170,14 +170,58 @@ class Batch:
             pass
 
 
+class Pool(Batch):
+    """A slot pool (cfd_pool_*): cases of any size placed in one device arena of
+    `hbm_budget` bytes as they are admitted and given back when released. Every Batch
+    method works on it; its case indices are slots."""
+
+    def __init__(self, hbm_budget: int, max_cases: int = 256, precision: int = _lib.PRECISION_FP64):
+        L = _lib.lib()
+        self.grids = [None] * int(max_cases)
+        self._keep = []
+        self.h = ctypes.c_void_p()
+        _lib.check(L.cfd_pool_create(int(hbm_budget), int(max_cases), int(precision), ctypes.byref(self.h)),
+                   "cfd_pool_create")
+        self.steps = 0
+
+    def place(self, grid, params):
+        """Admit a case; returns its slot, or None when no free region of the budget (or no
+        slot) is left for it (CFD_E_OOM: nothing changed)."""
+        s, keep = _lib.make_grid(grid)
+        slot = ctypes.c_int(-1)
+        rc = _lib.lib().cfd_pool_admit(self.h, ctypes.byref(s), ctypes.byref(params), ctypes.byref(slot))
+        if rc == -3:
+            return None
+        _lib.check(rc, "cfd_pool_admit")
+        self._keep.extend(keep)
+        self.grids[slot.value] = grid
+        return slot.value
+
+    def release(self, slot: int):
+        _lib.check(_lib.lib().cfd_pool_release(self.h, int(slot)), "cfd_pool_release")
+        self.grids[slot] = None
+
+    def free(self) -> tuple:
+        """(free bytes, largest free region) of the budget."""
+        a, b = ctypes.c_size_t(), ctypes.c_size_t()
+        _lib.check(_lib.lib().cfd_pool_free(self.h, ctypes.byref(a), ctypes.byref(b)), "cfd_pool_free")
+        return a.value, b.value
+
+    @staticmethod
+    def case_bytes(grid) -> int:
+        prof = _lib.PROFILE_CAVITY if grid.kind == "cavity" else _lib.PROFILE_OGRID
+        return int(_lib.lib().cfd_pool_case_bytes(grid.n0, grid.n1, prof))
+
+
 def serve(requests, classes, steps_per_tick: int = 50, slots=None, hbm_budget: int = 0,
           precision: int = _lib.PRECISION_FP64):
     """Run a real-time serving session (cfd_serve).
 
     requests: list of (arrival_s, grid, params, tol, max_steps); classes: list of
-    (template grid, profile); slots: slots per class (or None with hbm_budget); precision:
-    CFD_PRECISION_* of the slots (every request's params must match).
-    Returns (list of result dicts, stats dict).
+    (template grid, profile) with slots: fixed slots per class; or slots=None: admission by
+    free device memory into a slot pool of hbm_budget bytes (requests of any size; classes
+    may be empty); precision: CFD_PRECISION_* of the session (every request's params must
+    match). Returns (list of result dicts, stats dict).
     """
     keep = []
     grids = []
@@ -185,8 +229,8 @@ def serve(requests, classes, steps_per_tick: int = 50, slots=None, hbm_budget: i
         s, k = _lib.make_grid(g)
         keep.extend(k)
         grids.append(s)
-    garr = (_lib.CfdGrid * len(grids))(*grids)
-    profs = (ctypes.c_int * len(classes))(*[p for _, p in classes])
+    garr = (_lib.CfdGrid * max(1, len(grids)))(*grids)
+    profs = (ctypes.c_int * max(1, len(classes)))(*[p for _, p in classes])
     sl = (ctypes.c_int * len(classes))(*slots) if slots is not None else None
     cfg = _lib.CfdServeConfig(nclasses=len(classes), class_grids=garr, class_profile=profs,
                               class_slots=sl, hbm_budget=int(hbm_budget), steps_per_tick=steps_per_tick,

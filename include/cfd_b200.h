@@ -187,6 +187,24 @@ int cfd_batch_admit(cfd_batch* b, int slot, const cfd_grid* g, const cfd_params*
 int cfd_batch_admit_spec(cfd_batch* b, int slot, const cfd_grid_spec* spec, const cfd_params* p);
 int cfd_batch_set_active(cfd_batch* b, int slot, int active);
 
+/* ---- slot pool: admission by free device memory (no counterpart in the reference, which
+ * runs one case per process) ----
+ * A pool is a batch whose cases are placed in one device arena of hbm_budget bytes as they
+ * are admitted, whatever their size, and give their memory back when released; every
+ * cfd_batch_* call works on it. Its case indices are slots 0 .. max_cases-1; an empty slot
+ * takes part in no launch. cfd_pool_admit() places a new case in the first free region
+ * that fits it and writes its slot; CFD_E_OOM (nothing changed) when no free region of the
+ * budget fits or every slot is taken -- retry after a release. The other cases keep their
+ * resident state and step on bit for bit as they would alone (each case's tiles keep their
+ * order in the launches). cfd_pool_release() frees a slot and its memory at once.
+ * cfd_pool_case_bytes() is the arena bytes a case takes; cfd_pool_free() reports the free
+ * bytes and the largest free region. */
+int cfd_pool_create(size_t hbm_budget, int max_cases, int precision, cfd_batch** out);
+int cfd_pool_admit(cfd_batch* b, const cfd_grid* g, const cfd_params* p, int* slot);
+int cfd_pool_release(cfd_batch* b, int slot);
+int cfd_pool_free(cfd_batch* b, size_t* free_bytes, size_t* largest);
+size_t cfd_pool_case_bytes(int n0, int n1, int profile);
+
 /* ---- serving session: requests with arrival times over slot classes ---- */
 typedef struct cfd_request {
     double arrival_s;     /* seconds after the session starts */
@@ -204,11 +222,13 @@ typedef struct cfd_result {
 } cfd_result;
 
 typedef struct cfd_serve_config {
-    int nclasses;
+    int nclasses;                /* fixed slots only: the slot classes */
     const cfd_grid* class_grids; /* one template grid per slot class (sets n0, n1) */
     const int* class_profile;    /* CFD_PROFILE_* of each class */
-    const int* class_slots;      /* slots per class; NULL: an equal share of hbm_budget each */
-    size_t hbm_budget;           /* device bytes for all slots when class_slots is NULL */
+    const int* class_slots;      /* slots per class; NULL: admission by free device memory --
+                                    a slot pool (cfd_pool_create) of hbm_budget bytes takes
+                                    requests of any size, the classes are not used */
+    size_t hbm_budget;           /* device bytes of the pool when class_slots is NULL */
     int steps_per_tick;          /* steps between convergence checks / admissions */
     int precision;               /* CFD_PRECISION_* of every slot (requests must match) */
 } cfd_serve_config;
@@ -219,9 +239,12 @@ typedef struct cfd_serve_stats {
     int converged, failed, slots;
 } cfd_serve_stats;
 
-/* Runs a serving session in real time: requests are admitted into free slots of their
- * class as they arrive, all active slots advance together, converged cases are retired
- * and their slots back-filled. results[i] belongs to reqs[i]. */
+/* Runs a serving session in real time: requests are admitted as they arrive -- by free
+ * device memory (class_slots NULL: oldest first into the first free region of the budget
+ * that fits; a smaller request may pass a larger one that does not fit yet, until the
+ * oldest has waited 20 ticks) or into free slots of their class -- all admitted cases
+ * advance together, converged cases are retired and their memory or slots reused.
+ * results[i] belongs to reqs[i]. */
 int cfd_serve(const cfd_serve_config* cfg, const cfd_request* reqs, int nreq, cfd_result* results,
               cfd_serve_stats* stats);
 
