@@ -60,9 +60,12 @@ def parse():
     ap.add_argument("--conv-cap", type=int, default=20000, help="step cap per case of the converged block")
     ap.add_argument("--cap", type=int, default=30000, help="step cap per case (converged)")
     ap.add_argument("--chunk", type=int, default=100, help="steps between retirement checks")
-    ap.add_argument("--requests", type=int, default=512, help="requests of the serve workload")
+    ap.add_argument("--requests", type=int, default=64, help="requests of the serve workload")
     ap.add_argument("--rate", type=float, default=4.0, help="Poisson arrival rate (requests/s)")
-    ap.add_argument("--max-steps", type=int, default=1000, help="step cap per request (serve)")
+    ap.add_argument("--max-steps", type=int, default=12000, help="step cap per request (serve)")
+    ap.add_argument("--serve-gb", type=float, default=24.0, help="device memory budget of the served pool (GB)")
+    ap.add_argument("--plain-sample", type=int, default=8, help="requests the plain server runs for real")
+    ap.add_argument("--no-serve", action="store_true", help="leave the serve block out of the default line")
     ap.add_argument("--mg", default=None,
                     help="multigrid schedule pre,post,coarse,fused (default: the library's)")
     return ap.parse_args()
@@ -463,50 +466,71 @@ def run_converged(args):
     print(json.dumps(line))
 
 
-def run_serve(args):
-    """A Poisson request stream (sizes N in {129,257,513,1025} w.p. {.4,.3,.2,.1}, physics as
-    the sweep) through the native serving loop, against a plain single-case FP64 server
-    (FIFO, one case at a time) whose service times are measured per size."""
-    import math as _m
-    from cfd_solver_b200.grid import cavity
+def serve_block(nreq: int, rate: float, tol: float, cap: int, tick: int, budget_gb: float, plain_sample: int):
+    """The served form: a Poisson stream of the benchmark's request mix through cfd_serve's
+    admission by free device memory, against a plain FP64 single-case server run for real on
+    the stream's first `plain_sample` requests.
+
+    Stream: `nreq` requests at `rate`/s, N in {129, 257, 513, 1025} w.p. {.4, .3, .2, .1},
+    physics as the sweep, cavity form, precision form; each is retired at steady_res_rel <=
+    `tol` or after `cap` steps. Plain server: the sampled requests, FIFO, each run alone on the
+    FP64 path to the same rule (service times measured, host wall clock); their latencies
+    follow from those service times and the arrival times."""
     from cfd_solver_b200.solver import case_params, serve
     from cfd_solver_b200.workloads import SERVE_PROBS, SERVE_SIZES, make_case, serve_stream
-    sizes, probs = list(SERVE_SIZES), list(SERVE_PROBS)
-    prec = 1 if args.precision == "mixed" else 0
     reqs, cases = [], []
-    for t, d in serve_stream(args.requests, args.rate):
+    for t, d in serve_stream(nreq, rate):
         g, prm = make_case(d, "cavity")
         cases.append((g, prm))
-        reqs.append((t, g, case_params(g, precision=prec, **prm), args.tol, args.max_steps))
-    classes = [(cavity(N, N), 1) for N in sizes]
-    slots = [64, 32, 16, 8]
-    results, st = serve(reqs, classes, steps_per_tick=args.chunk, slots=slots, precision=prec)
-    # plain server: FIFO, one case at a time, service = steps x plain step time of its size
-    pt = plain_times_by_size([cases[i] for i in range(len(cases))], warm=300, timed=200)
-    free, lat = 0.0, []
-    for (ta, g, *_), r in zip(reqs, results):
-        start = max(free, ta)
-        free = start + r["steps"] * pt[g.n0] / 1e3
-        lat.append(free - ta)
-    lat_s = sorted(lat)
-    pct = lambda q: lat_s[min(len(lat_s) - 1, max(0, _m.ceil(q * len(lat_s)) - 1))]
-    finished = len(results)
-    line = {"metric": "served cases/s", "value": finished / max(st["makespan_s"], 1e-9), "unit": "cases/s",
-            "n_gpus": 1, "value_counts": "finished requests (converged or at their step cap) per second",
-            "higher_is_better": True, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
-            "data": "synthetic (seeded Poisson stream)",
-            "config": {"workload": f"{args.requests} requests, Poisson rate {args.rate}/s, N in {sizes} "
-                                   f"w.p. {probs}, cavity form", "tol": args.tol,
-                       "max_steps": args.max_steps, "slots": dict(zip(sizes, slots)),
-                       "steps_per_tick": args.chunk, "precision": args.precision},
-            "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
-            "mean_latency_s": st["mean_latency_s"], "makespan_s": st["makespan_s"],
-            "converged": st["converged"], "finished_at_cap": args.requests - st["converged"],
+        reqs.append((t, g, case_params(g, precision=1, **prm), tol, cap))
+    budget = int(budget_gb * (1 << 30))
+    results, st = serve(reqs, [], steps_per_tick=tick, slots=None, hbm_budget=budget, precision=1)
+    lat = sorted(r["latency_s"] for r in results)
+    conv = sorted(r["latency_s"] for r in results if r["status"] == 0)
+
+    def pct(v, q):
+        return v[min(len(v) - 1, max(0, math.ceil(q * len(v)) - 1))] if v else None
+
+    # plain FP64 server, run for real on the first requests of the stream (FIFO)
+    free, plain_lat, plain_conv, served_lat = 0.0, [], 0, []
+    for i in range(min(plain_sample, len(reqs))):
+        g, prm = cases[i]
+        wall, steps, s1, _ = plain_solve(g, prm, tol, cap, tick)
+        start = max(free, reqs[i][0])
+        free = start + wall
+        plain_lat.append(free - reqs[i][0])
+        plain_conv += (s1["steady_res_rel"] <= tol) and not (s1["status"] & 4)
+        served_lat.append(results[i]["latency_s"])
+    return {"metric": "served cases/s", "value": len(results) / max(st["makespan_s"], 1e-9), "unit": "cases/s",
+            "value_counts": "finished requests (converged or at the step cap) per second",
+            "workload": f"{nreq} requests, Poisson {rate}/s, N in {list(SERVE_SIZES)} w.p. {list(SERVE_PROBS)}, "
+                        f"cavity form, precision form, admission by free device memory ({budget_gb} GB)",
+            "tol": tol, "step_cap": cap, "steps_per_tick": tick,
+            "p50_latency_s": pct(lat, 0.5), "p99_latency_s": pct(lat, 0.99),
+            "converged": len(conv), "p50_latency_converged_s": pct(conv, 0.5),
+            "p99_latency_converged_s": pct(conv, 0.99), "makespan_s": st["makespan_s"],
+            "peak_cases_resident": max_resident(results),
             "cell_updates_per_s": st["cell_updates"] / max(st["makespan_s"], 1e-9),
-            "plain": {"cases_per_s": len(lat) / max(free - reqs[0][0], 1e-9), "p50_latency_s": pct(0.5),
-                      "p99_latency_s": pct(0.99), "ms_per_step_by_N": pt,
-                      "path": "single case, FP64, FIFO (service times measured per size)"}}
-    print(json.dumps(line))
+            "plain_sample": {"requests": len(plain_lat), "path": "single case alone, FP64, FIFO, run for real",
+                             "p50_latency_s": pct(sorted(plain_lat), 0.5), "max_latency_s": max(plain_lat, default=None),
+                             "converged": plain_conv, "served_p50_latency_same_requests_s":
+                                 pct(sorted(served_lat), 0.5),
+                             "served_max_latency_same_requests_s": max(served_lat, default=None)}}
+
+
+def max_resident(results):
+    ev = sorted([(r["admit_s"], 1) for r in results] + [(r["done_s"], -1) for r in results])
+    cur = peak = 0
+    for _, d in ev:
+        cur += d
+        peak = max(peak, cur)
+    return peak
+
+
+def run_serve(args):
+    """The serve block alone, printed as its own line (--workload serve)."""
+    blk = serve_block(args.requests, args.rate, args.tol, args.max_steps, args.chunk, args.serve_gb, args.plain_sample)
+    print(json.dumps(dict(blk, n_gpus=1, higher_is_better=True, dtype="f64+f32", data="synthetic (seeded Poisson stream)")))
 
 
 def run_precision(args):
@@ -739,10 +763,13 @@ def main():
             cpu = {"value": None, "unavailable": sample}
     st0 = b.stats(0)
     b.close()
-    conv = None
+    conv = srv = None
     if rank == 0 and world == 1 and not args.no_converged:
         # the headline metric (converged cases/s, batched vs plain), both arms run on this GPU
         conv = converged_block(args, args.ncases, args.conv_cap, args.tol, args.chunk)
+    if rank == 0 and world == 1 and not args.no_serve:
+        srv = serve_block(args.requests, args.rate, args.tol, args.max_steps, args.chunk, args.serve_gb,
+                          args.plain_sample)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -758,6 +785,7 @@ def main():
                 "clocks": clk, "gpu_launches": launches, "kernels": kernels,
                 "dominant_kernel": dom[0],
                 "converged": conv,
+                "serve": srv,
                 "baseline_metric_note": ("the headline metric is converged cases/s (the `converged` "
                                          "block: batched precision form vs the plain FP64 single-case "
                                          "path, both run); a case needs 1e3-1e5 steps to its steady "
