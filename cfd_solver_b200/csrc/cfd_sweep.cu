@@ -13,8 +13,11 @@
 //
 // A warp owns four consecutive rows of the tile, a lane one column: the thread reads its
 // eight-row x five-column window once into registers, so its four cells cost ten
-// shared-memory loads each instead of twenty-five. The per-tile L1 residuals go to
-// per-warp partials that k_sweep_fin sums per case in a fixed order after the launch.
+// shared-memory loads each instead of twenty-five. Each cell's off-centre sum (25-point, or
+// 9-point on the near-wall cells) is formed just before its update, and the per-CTA
+// constants and each field's warp residual sums sit in shared memory, so the kernel holds
+// its 128 registers with little spilling. The per-tile L1 residuals go to one partial row
+// per tile that k_sweep_fin sums per case in a fixed order after the launch.
 //
 // Three modes share the code:
 //   SW_F64    FP64 iterates x_k (the plain path);
@@ -208,10 +211,19 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
     const double* sc = b.scal + (long long)t.c * NSCAL;
     const bool weighted = MODE == SW_MX ? true : sweep > 0;
     const bool has_prev = MODE == SW_MX ? sweep > 1 : (MODE == SW_F64 && sweep > 0);
-    const ST gU = (ST)(2.0 / (c.cheb_a[0] + c.cheb_b[0])), gT = (ST)(2.0 / (c.cheb_a[1] + c.cheb_b[1]));
-    const ST wU = weighted ? (ST)sc[S_CW0] : ST(1), wT = weighted ? (ST)sc[S_CW1] : ST(1);
+    // per-CTA constants of the sweeps (Chebyshev step g and weight w of the u-type and T
+    // systems, 1/Pr) and the tile's per-warp residual sums, in shared memory
+    __shared__ ST sconst[5];
+    __shared__ double sred[SW_WARPS * NFIELD];
     const double rPr64 = 1.0 / c.Pr;
-    const ST rPr = (ST)rPr64;
+    if (tid < SW_WARPS * NFIELD) sred[tid] = 0.0;
+    if (tid == 0) {
+        sconst[0] = (ST)(2.0 / (c.cheb_a[0] + c.cheb_b[0]));
+        sconst[1] = (ST)(2.0 / (c.cheb_a[1] + c.cheb_b[1]));
+        sconst[2] = weighted ? (ST)sc[S_CW0] : ST(1);
+        sconst[3] = weighted ? (ST)sc[S_CW1] : ST(1);
+        sconst[4] = (ST)rPr64;
+    }
     const int ld = c.ld, xld = c.xld, W = c.W, per = c.periodic;
     const int i = t.i0 + lane;
     bool inq[SW_ROWS], nearw[SW_ROWS], drop_s[SW_ROWS], drop_n[SW_ROWS];
@@ -227,18 +239,19 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
 
     ST* OPS = reinterpret_cast<ST*>(sm + L::OPS);
     float* RAP = reinterpret_cast<float*>(sm + L::RAP);
-    bool any_nearw = false;
-#pragma unroll
-    for (int q = 0; q < SW_ROWS; q++) any_nearw |= nearw[q];
     // the thread's periodic mirror column (written alongside column i), or none
     const int mcol = mirror_col(i, W, per);
-    double r[NFIELD] = {0.0, 0.0, 0.0, 0.0, 0.0};
     bool ok = true;
     int k = 0;
     for (int fm = mask; fm; fm &= fm - 1, k++) {
         const int f = __ffs(fm) - 1;
         const int bi = k & 1;
-        ok = __syncthreads_and(mbar_wait_bounded(&bar[bi], (k >> 1) & 1, b.wait_polls)) && ok;
+        // one thread polls the buffer's mbarrier; the barrier after it orders the other
+        // threads' reads of the landed copies after its observation (the others wait in the
+        // barrier instead of spending issue slots on polls)
+        bool got = true;
+        if (tid == 0) got = mbar_wait_bounded(&bar[bi], (k >> 1) & 1, b.wait_polls);
+        ok = __syncthreads_and(got) && ok;
         if (!ok) break;
         const unsigned char* buf = sm + bi * L::BUF;
         if (k == 0) {
@@ -285,23 +298,8 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
             }
         }
 
-        // off-centre sums: the 25-point form for every cell, then the few near-wall cells
-        ST sum[SW_ROWS];
-#pragma unroll
-        for (int q = 0; q < SW_ROWS; q++) {
-            const int o = (wrp * SW_ROWS + q) * TX + lane;
-            sum[q] = sw_sum25<ST>(w, q, OPS[o], OPS[SW_CELLS + o], OPS[2 * SW_CELLS + o]);
-        }
-        if (any_nearw) {
-#pragma unroll
-            for (int q = 0; q < SW_ROWS; q++) {
-                if (!nearw[q]) continue;
-                const int o = (wrp * SW_ROWS + q) * TX + lane;
-                sum[q] = sw_sum9<ST>(w, q, OPS[o], OPS[SW_CELLS + o], OPS[2 * SW_CELLS + o], drop_s[q], drop_n[q]);
-            }
-        }
-        const ST g = isT ? gT : gU, wgt = isT ? wT : wU;
-        const ST scale = isT ? rPr : ST(1);
+        const ST g = sconst[isT ? 1 : 0], wgt = sconst[isT ? 3 : 2];
+        const ST scale = isT ? sconst[4] : ST(1);
         // the reference's T solve passes atnw in the annw slot (PSolver.cpp:1290): the
         // (i-1, j+2) coefficient of the 25-point T rows becomes anw = -8/9 B instead of B/9
         const bool tbug = isT && !c.fix_T_annw;
@@ -325,7 +323,8 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
         for (int q = 0; q < SW_ROWS; q++) {
             const int o = (wrp * SW_ROWS + q) * TX + lane;
             const ST E = OPS[o], G = OPS[SW_CELLS + o], B = OPS[2 * SW_CELLS + o];
-            ST sm_ = sum[q];
+            // off-centre sum: the 25-point form, or the 9-point form on the near-wall cells
+            ST sm_ = nearw[q] ? sw_sum9<ST>(w, q, E, G, B, drop_s[q], drop_n[q]) : sw_sum25<ST>(w, q, E, G, B);
             if (tbug && !nearw[q]) sm_ -= B * w[q + 4][1];
             sm_ *= scale;
             const ST D = (nearw[q] ? ST(2) : ST(2.5)) * (E + G);
@@ -359,9 +358,10 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
                 }
             }
         }
+        // the field's warp residual (lane 0), summed as the tile's partial after the last field
 #pragma unroll
-        for (int ff = 0; ff < NFIELD; ff++)
-            if (ff == f) r[ff] += racc;
+        for (int o = 16; o > 0; o >>= 1) racc += __shfl_down_sync(0xffffffffu, racc, o);
+        if (lane == 0) sred[wrp * NFIELD + f] = racc;
     }
     if (!ok) {
         if (tid == 0) {
@@ -372,26 +372,12 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
         return;
     }
     // the tile's partial L1 residuals, one row per tile (summed per case by k_sweep_fin):
-    // warps, then the tile's four warps in a fixed order through the first field buffer,
-    // free once every field has been read and no copy is in flight
-#pragma unroll
-    for (int ff = 0; ff < NFIELD; ff++) {
-        double x = r[ff];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        r[ff] = x;
-    }
-    double* red = reinterpret_cast<double*>(sm);
-    __syncthreads();
-    if (lane == 0) {
-#pragma unroll
-        for (int ff = 0; ff < NFIELD; ff++) red[wrp * NFIELD + ff] = r[ff];
-    }
+    // the tile's four warp sums in a fixed order
     __syncthreads();
     if (tid < NFIELD) {
         double x = 0.0;
 #pragma unroll
-        for (int w = 0; w < SW_WARPS; w++) x += red[w * NFIELD + tid];
+        for (int w = 0; w < SW_WARPS; w++) x += sred[w * NFIELD + tid];
         b.partial[(long long)blockIdx.x * PSTRIDE + tid] = x;
     }
 }

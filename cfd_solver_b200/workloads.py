@@ -37,15 +37,19 @@ SERVE_SIZES = (129, 257, 513, 1025)
 SERVE_PROBS = (0.4, 0.3, 0.2, 0.1)
 
 
-def serve_stream(nrequests: int, rate: float, seed: int = SWEEP_SEED + 7):
+def serve_stream(nrequests: int, rate: float, seed: int = SWEEP_SEED + 7, sizes=SERVE_SIZES,
+                 probs=SERVE_PROBS):
     """The served request stream: Poisson arrivals at `rate` requests/s, N in
     {129, 257, 513, 1025} with probability {.4, .3, .2, .1}, the other physics of the
-    sweep draws of the same seed. Returns [(arrival_s, draw)] in arrival order."""
+    sweep draws of the same seed. `sizes` restricts N to a subset of the classes (their
+    probabilities renormalised). Returns [(arrival_s, draw)] in arrival order."""
     rng = np.random.default_rng(seed)
+    p = np.array([probs[list(SERVE_SIZES).index(n)] for n in sizes], dtype=float)
+    p /= p.sum()
     out = []
     t = 0.0
     for d in sweep_draws(nrequests, seed=seed):
-        d = dict(d, N=int(rng.choice(list(SERVE_SIZES), p=list(SERVE_PROBS))))
+        d = dict(d, N=int(rng.choice(list(sizes), p=list(p))))
         t += float(rng.exponential(1.0 / rate))
         out.append((t, d))
     return out
