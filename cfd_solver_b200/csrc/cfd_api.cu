@@ -506,6 +506,49 @@ __global__ void k_grid_to_slot(const double* gen, int n0, int n1, int W, int per
     region[(long long)pid * ps + 16 + (long long)j * ld + col] = v;
 }
 
+// The initial state (initial_state() on the host, PSolver.cpp:614-748) of a case whose grid
+// was generated on the device, written straight into its six state planes in the padded
+// layout pad_plane() gives (the planes are zeroed by the caller; a periodic case's halo
+// columns take the wrap). `x0`, `y0` are row 0 of x and y. Cavity: zero fields,
+// lid u = up = lid_u on row n1-1 (columns 1 .. n0-2), T = 1 on row 0. O-grid: the uniform
+// stream (uinf, vinf) with T = p = 0, and on the wall row the rotating-wall velocity
+// (-w y, w x) with T = 1; the far-field row keeps the stream (either branch of the inflow
+// test there copies the stream from the row below).
+__global__ void k_init_state(double* region, long long ps, int ld, int n0, int n1, int W, int periodic,
+                             int cavity, const double* x0, const double* y0, double uinf, double vinf,
+                             double speed_amp,
+                             double lid_u, int pu, int pv, int pT, int pup, int pvp) {
+    const int ncols = periodic ? W + 2 * H : n0;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)n1 * ncols) return;
+    const int j = (int)(e / ncols), cpad = (int)(e % ncols);
+    const int col = periodic ? cpad - H : cpad;
+    const int i = col < 0 ? col + W : (col >= W && periodic ? col - W : col);
+    double u, v, T, up, vp;
+    if (cavity) {
+        u = (j == n1 - 1 && i >= 1 && i <= n0 - 2) ? lid_u : 0.0;
+        up = u;
+        v = vp = 0.0;
+        T = j == 0 ? 1.0 : 0.0;
+    } else if (j == 0) {
+        u = -speed_amp * y0[i];
+        v = speed_amp * x0[i];
+        up = u;
+        vp = v;
+        T = 1.0;
+    } else {
+        u = up = uinf;
+        v = vp = vinf;
+        T = 0.0;
+    }
+    const long long k = 16 + (long long)j * ld + col;
+    region[(long long)pu * ps + k] = u;
+    region[(long long)pv * ps + k] = v;
+    region[(long long)pT * ps + k] = T;
+    region[(long long)pup * ps + k] = up;
+    region[(long long)pvp * ps + k] = vp;
+}
+
 static_assert(P_X == 0 && P_Y == 1 && P_XIX == 2 && P_XIY == 3 && P_ETX == 4 && P_ETY == 5 && P_ALPH == 6 &&
                   P_BETA == 7 && P_GAM == 8 && P_JAC == 9,
               "grid planes 0..9 in the order of cfd_grid_generate's planes");
@@ -913,15 +956,19 @@ int put_plane(cfd_batch* b, const CaseDev& d, int plane_id, const double* src, s
 
 // Initial state, descriptor and per-case scalars of case `c` once its grid planes are in
 // place, and with `setup` its pressure stencil and multigrid hierarchy. The initial state
-// reads only n0, n1, row 0 of x and y and the outer normals xnox, xnoy of `g`.
-int upload_state(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, bool setup) {
+// reads only n0, n1, row 0 of x and y and the outer normals xnox, xnoy of `g`; with
+// `state_on_device` the caller has written the state planes already (k_init_state).
+int upload_state(cfd_batch* b, int c, const cfd_grid& g, const cfd_params& p, bool setup,
+                 bool state_on_device = false) {
     CaseDev& d = b->hc[c];
-    std::vector<double> pad;
-    std::vector<double> st[6];
-    initial_state(&g, &p, d, st);
-    const int sid[6] = {P_U, P_V, P_T0 + b->cur, P_UP0 + b->cur, P_VP0 + b->cur, P_P};
-    for (int m = 0; m < 6; m++)
-        if (int rc = put_plane(b, d, sid[m], st[m].data(), pad)) return rc;
+    if (!state_on_device) {
+        std::vector<double> pad;
+        std::vector<double> st[6];
+        initial_state(&g, &p, d, st);
+        const int sid[6] = {P_U, P_V, P_T0 + b->cur, P_UP0 + b->cur, P_VP0 + b->cur, P_P};
+        for (int m = 0; m < 6; m++)
+            if (int rc = put_plane(b, d, sid[m], st[m].data(), pad)) return rc;
+    }
     CK(cudaMemcpyAsync(b->dc + c, &d, sizeof(CaseDev), cudaMemcpyHostToDevice, b->st));
     std::vector<double> sc(NSCAL, 0.0);
     std::vector<int> is(NISCAL, 0);
@@ -1138,11 +1185,7 @@ int upload_case_generated(cfd_batch* b, int c, const cfd_grid_spec& spec, const 
     const int sblocks = (int)std::min<long long>((np + SCAN_THREADS - 1) / SCAN_THREADS, 148LL * 8);
     k_grid_scan<<<sblocks, SCAN_THREADS, 0, b->st>>>(gen, n0, n1, cs, scan);
     CK(cudaGetLastError());
-    std::vector<double> x0(n0), y0(n0), nv(4 * (size_t)n0);
     unsigned long long hs[5];
-    CK(cudaMemcpyAsync(x0.data(), gen + (long long)P_X * np, sizeof(double) * n0, cudaMemcpyDeviceToHost, b->st));
-    CK(cudaMemcpyAsync(y0.data(), gen + (long long)P_Y * np, sizeof(double) * n0, cudaMemcpyDeviceToHost, b->st));
-    CK(cudaMemcpyAsync(nv.data(), nrm, sizeof(double) * 4 * n0, cudaMemcpyDeviceToHost, b->st));
     CK(cudaMemcpyAsync(hs, scan, sizeof(hs), cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
     if (hs[4] != 0) return fail(CFD_E_ARG, "grid metrics invalid (alpha, gamma must be > 0)");
@@ -1163,19 +1206,21 @@ int upload_case_generated(cfd_batch* b, int c, const cfd_grid_spec& spec, const 
     case_scalars_to_dev(d, dxi0, dxi1, ar, p);
     cheb_finish(emax, rmax, d);
     b->prm[c] = p;
+    // the initial state on the device as well: nothing of the case crosses PCIe
+    const int sid[6] = {P_U, P_V, P_T0 + b->cur, P_UP0 + b->cur, P_VP0 + b->cur, P_P};
+    for (int m = 0; m < 6; m++) CK(cudaMemsetAsync(region + (long long)sid[m] * d.ps, 0, sizeof(double) * d.ps, b->st));
+    const long long nst = (long long)n1 * (d.periodic ? d.W + 2 * H : n0);
+    k_init_state<<<(unsigned)((nst + 255) / 256), 256, 0, b->st>>>(
+        region, d.ps, d.ld, n0, n1, d.W, d.periodic, spec.profile == CFD_PROFILE_CAVITY, gen + (long long)P_X * np,
+        gen + (long long)P_Y * np, d.uinf, d.vinf, d.speed_amp, d.lid_u, sid[0], sid[1], sid[2], sid[3], sid[4]);
+    CK(cudaGetLastError());
     cfd_grid g{};
     g.n0 = n0;
     g.n1 = n1;
     g.dxi0 = dxi0;
     g.dxi1 = dxi1;
     g.ar = ar;
-    g.x = x0.data();
-    g.y = y0.data();
-    g.xnix = nv.data();
-    g.xniy = nv.data() + n0;
-    g.xnox = nv.data() + 2 * n0;
-    g.xnoy = nv.data() + 3 * n0;
-    return upload_state(b, c, g, p, true);
+    return upload_state(b, c, g, p, true, true);
 }
 
 // ==========================================================================

@@ -179,10 +179,10 @@ int cfd_batch_autotune(cfd_batch* b, int steps, int* out_schedule4, double* out_
  * slot (its kernels skip it), 1 re-activates it. */
 int cfd_batch_admit(cfd_batch* b, int slot, const cfd_grid* g, const cfd_params* p);
 /* cfd_batch_admit() of the grid cfd_grid_generate() makes for `spec`, generated straight
- * into the slot's device planes: no grid crosses PCIe (only row 0 of x and y and the
- * normals come back, for the initial state). The slot's Chebyshev bounds and metric check
- * are computed on the device with the same per-point arithmetic as the host path, so the
- * case steps bit for bit like cfd_batch_admit() of that grid. spec->n0, n1, profile must
+ * into the slot's device planes together with the case's initial state: nothing of the
+ * case crosses PCIe (five words of the metric scan come back). The slot's Chebyshev bounds
+ * and metric check are computed on the device with the same per-point arithmetic as the
+ * host path, so the case steps bit for bit like cfd_batch_admit() of that grid. spec->n0, n1, profile must
  * match the slot; CFD_E_ARG (the slot untouched) for a mismatch or an invalid spec. */
 int cfd_batch_admit_spec(cfd_batch* b, int slot, const cfd_grid_spec* spec, const cfd_params* p);
 int cfd_batch_set_active(cfd_batch* b, int slot, int active);

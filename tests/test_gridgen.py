@@ -69,17 +69,19 @@ def test_admit_spec_steps_like_admit_of_the_generated_grid(kind, kw):
     """A case generated straight into a slot (cfd_batch_admit_spec) steps bit for bit like
     cfd_batch_admit() of the grid cfd_grid_generate() returns: the same padded grid planes,
     the same Chebyshev bounds (the device scan rounds every operation as the host loop
-    does) and the same initial state."""
+    does) and the same initial state, which admit_spec writes on the device (the O-grid
+    case has a rotating wall, F != 0, so its wall row carries the wall velocity; the batch
+    has taken an odd number of steps, so the state goes to the second T/up/vp buffers)."""
     from cfd_solver_b200.solver import Batch, case_params
     spec_kw = {k: v for k, v in kw.items() if k not in ("n0", "n1")}
     gdev = G.generate_on_device(kind, **kw)
     first = G.generate_on_device(kind, **dict(kw, skew=0.05))  # the slots' first occupant
-    prm = case_params(gdev, Re=200.0, Ri=1.0, dt=1e-3)
+    prm = case_params(gdev, Re=200.0, Ri=1.0, dt=1e-3, F=0.3 if kind == "ogrid" else 0.0)
     with Batch([first, first], [prm, prm]) as b:
-        b.step(2)
+        b.step(3)
         b.admit_spec(0, kind, prm, **spec_kw)
         b.admit(1, gdev, prm)
-        for name in ("x", "y", "xix", "ety", "alph", "beta", "gam", "jac", "u", "v", "T", "p"):
+        for name in ("x", "y", "xix", "ety", "alph", "beta", "gam", "jac", "u", "v", "T", "p", "up", "vp"):
             assert np.array_equal(b.plane(0, name), b.plane(1, name)), name
         b.step(4)
         for name in ("u", "v", "T", "p", "up", "vp"):
