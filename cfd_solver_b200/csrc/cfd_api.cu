@@ -569,6 +569,11 @@ void case_scalars_to_dev(CaseDev& d, double dxi0, double dxi1, double ar, const 
     d.ca = cos(p.alpha_deg * d.Pi / 180.0);
     d.ar = g.ar; d.omega_p = p.omega_p; d.lid_u = p.lid_u;
     d.tol_mom = p.tol_mom; d.atol_mom = p.atol_mom; d.tol_p = p.tol_p; d.atol_p = p.atol_p;
+    // the sweeps' per-case factors, formed once here rather than by every thread of every CTA
+    d.swk[0] = d.dt / (d.Re * d.d0 * d.d0);
+    d.swk[1] = d.dt / (d.Re * d.d1 * d.d1);
+    d.swk[2] = d.dt / (d.Re * d.d0 * d.d1);
+    d.rPr = 1.0 / d.Pr;
     d.pc1 = 1.0 / (2.0 * g.dxi0 * g.dxi0);
     d.pc2 = 1.0 / (8.0 * g.dxi0 * g.dxi1);
     d.pc3 = 1.0 / (2.0 * g.dxi1 * g.dxi1);

@@ -116,6 +116,8 @@ struct CaseDev {
     double uinf, vinf, speed_amp, accn_amp, Pi, ar, omega_p, lid_u, sa, ca;
     double tol_mom, atol_mom, tol_p, atol_p;
     double cheb_a[2], cheb_b[2];  // eigenvalue bounds of D^-1 A (u-type, T) for the Chebyshev sweeps
+    double swk[3];                // dt / (Re dxi0^2), dt / (Re dxi1^2), dt / (Re dxi0 dxi1): E, G, B per metric
+    double rPr;                   // 1 / Pr
     double pc1, pc2, pc3;         // 1 / (2 dxi0^2), 1 / (8 dxi0 dxi1), 1 / (2 dxi1^2): pressure stencil
     LevelDev lev[MAXLEV];
 };

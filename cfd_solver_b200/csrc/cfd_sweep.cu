@@ -215,7 +215,7 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
     // systems, 1/Pr) and the tile's per-warp residual sums, in shared memory
     __shared__ ST sconst[5];
     __shared__ double sred[SW_WARPS * NFIELD];
-    const double rPr64 = 1.0 / c.Pr;
+    const double rPr64 = c.rPr;
     if (tid < SW_WARPS * NFIELD) sred[tid] = 0.0;
     if (tid == 0) {
         sconst[0] = (ST)(2.0 / (c.cheb_a[0] + c.cheb_b[0]));
@@ -257,8 +257,7 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
         if (k == 0) {
             // alpha, beta, gamma of the thread's own cells -> E, G, B, 1/ap_u, 1/ap_T
             const double* MET = reinterpret_cast<const double*>(sm + L::MET);
-            const double kE = c.dt / (c.Re * c.d0 * c.d0), kG = c.dt / (c.Re * c.d1 * c.d1),
-                         kB = c.dt / (c.Re * c.d0 * c.d1);
+            const double kE = c.swk[0], kG = c.swk[1], kB = c.swk[2];
 #pragma unroll
             for (int q = 0; q < SW_ROWS; q++) {
                 const int o = (wrp * SW_ROWS + q) * TX + lane;
@@ -267,8 +266,9 @@ __device__ __forceinline__ void sweep_tile(const BatchDev& b, unsigned char* sm,
                 OPS[o] = (ST)E;
                 OPS[SW_CELLS + o] = (ST)G;
                 OPS[2 * SW_CELLS + o] = (ST)B;
-                RAP[o] = (float)(1.0 / (1.0 + D));
-                RAP[SW_CELLS + o] = (float)(1.0 / (1.0 + D * rPr64));
+                // the correctly rounded reciprocal (the value 1.0 / x gives, in fewer instructions)
+                RAP[o] = (float)__drcp_rn(1.0 + D);
+                RAP[SW_CELLS + o] = (float)__drcp_rn(1.0 + D * rPr64);
             }
         }
         const bool isT = f == F_T;
