@@ -75,3 +75,55 @@ def test_serve_without_a_gpu_fails_loudly():
     g = G.cavity(33, 33)
     with pytest.raises(_lib.CfdError, match="no CUDA device"):
         serve([(0.0, g, case_params(g), 1e-8, 10)], [(g, _lib.PROFILE_CAVITY)], slots=[2])
+
+
+def test_pool_case_bytes_cover_both_arenas():
+    """cfd_pool_case_bytes: a case's FP64 planes and its FP32 levels and planes, each part
+    256-byte aligned -- at least the FP64 planes, and growing with the grid."""
+    L = _lib.lib()
+    for prof in (_lib.PROFILE_OGRID, _lib.PROFILE_CAVITY):
+        prev = 0
+        for n in (33, 65, 129, 257, 513, 1025):
+            b = L.cfd_pool_case_bytes(n, n, prof)
+            assert b % 256 == 0 and b >= NPLANES_FP64 * n * n * 8 and b > prev, (prof, n, b)
+            prev = b
+        assert L.cfd_pool_case_bytes(7, 65, prof) == 0
+
+
+def test_serve_by_free_memory_rejects_bad_requests_before_any_device_work():
+    """With no fixed slots cfd_serve admits by free device memory: any grid size is taken,
+    but a request larger than the whole budget, of another precision or without a grid is
+    rejected before the session's pool exists (so also on a host without a GPU)."""
+    from cfd_solver_b200.solver import Pool, case_params, serve
+    g = G.cavity(65, 65)
+    ok = (0.0, g, case_params(g), 1e-8, 10)
+    with pytest.raises(_lib.CfdError, match="CFD_E_OOM: cfd_serve: request 0 needs more device memory"):
+        serve([ok], [], slots=None, hbm_budget=Pool.case_bytes(g) - 256)
+    with pytest.raises(_lib.CfdError, match="request 1 has another precision"):
+        serve([ok, (0.1, g, case_params(g, precision=_lib.PRECISION_MIXED), 1e-8, 10)], [], slots=None,
+              hbm_budget=1 << 30)
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="a GPU is present")
+def test_pool_without_a_gpu_fails_loudly():
+    from cfd_solver_b200.solver import Pool
+    with pytest.raises(_lib.CfdError, match="no CUDA device"):
+        Pool(1 << 30, max_cases=4)
+
+
+def test_seams_reject_bad_arguments_before_any_device_work():
+    import ctypes
+    L = _lib.lib()
+    nulls9 = (ctypes.c_void_p * 9)()
+    nulls25 = (ctypes.c_void_p * 25)()
+    one = ctypes.c_void_p(8)
+    # sip9p seam: grid too small, null planes, a cap below one iteration
+    assert L.cfd_sip_solve(7, 25, 1, nulls9, one, one, 1e-8, 10, None, None) == -1
+    assert L.cfd_sip_solve(33, 25, 1, nulls9, one, one, 1e-8, 10, None, None) == -1
+    assert b"null coefficient plane" in L.cfd_last_error()
+    assert L.cfd_sip_solve(33, 25, 1, None, one, one, 1e-8, 0, None, None) == -1
+    # gauss seams
+    for fn in (L.cfd_gauss_solve, L.cfd_gauss_solve_noalloc):
+        assert fn(33, 25, 1, nulls25, one, one, 1e-8, 10, None, None) == -1
+        assert fn(33, 25, 1, None, one, one, 1e-8, 1, None, None) == -1
+    assert L.cfd_batch_set_wait_limit(None, 0) == -1
