@@ -384,8 +384,8 @@ void initial_state(const cfd_grid* g, const cfd_params* p, const CaseDev& c, std
 // Eigenvalue bounds of D^-1 A for the Chebyshev sweeps. With E = dt/Re (alpha/dxi0^2 +
 // gamma/dxi1^2) the smooth modes of the 25-point operator sit at 1/(1 + 2.5 E) and Gershgorin
 // bounds the top: 1 + ((17/6) E + 4.5 |beta| dt/(Re dxi0 dxi1)) / (1 + 2.5 E); the 9-point
-// rows lie inside both. Margins: 0.9 below, 1.05 above. T uses Re*Pr; the reference's T
-// slot bug (atnw for annw) adds 7/9 |beta| c to the off-diagonal sum.
+// rows lie inside both (margins: cheb_finish). T uses Re*Pr; the reference's T slot bug
+// (atnw for annw) adds 7/9 |beta| c to the off-diagonal sum.
 // Per-system constants of the bound scan: dt/scale, the cross-term factor, dt/(scale dxi0
 // dxi1), dxi0^2, dxi1^2 (index 0: u, v, up, vp with scale Re; 1: T with scale Re Pr).
 struct ChebScan {
@@ -405,10 +405,18 @@ ChebScan cheb_consts(const cfd_params& p, double dxi0, double dxi1) {
     return cs;
 }
 
+// The interval [a0, b0] = [1/(1 + 2.5 E), 1 + rmax] widened on each side by 2 % of its
+// width, but by at most 10 % of a0 below and 5 % of b0 above. The mass-dominated systems of
+// small time steps have narrow intervals (w << a0): width margins keep them narrow, and their
+// solves meet the stop rule after two sweeps instead of three. Large time steps give wide
+// intervals whose smallest eigenvalue lies within a few per cent of a0 (a0 = 0.053, w = 2.45
+// for a 257 x 257 cavity at E = 7): there the lower margin must stay a fraction of a0, since
+// a0 - 0.02 w would put the lower end near zero and triple the sweep count.
 void cheb_finish(const double* emax, const double* rmax, CaseDev& d) {
     for (int ty = 0; ty < 2; ty++) {
-        d.cheb_a[ty] = 0.9 / (1.0 + 2.5 * emax[ty]);
-        d.cheb_b[ty] = 1.05 * (1.0 + rmax[ty]);
+        const double a0 = 1.0 / (1.0 + 2.5 * emax[ty]), b0 = 1.0 + rmax[ty], w = b0 - a0;
+        d.cheb_a[ty] = a0 - std::min(0.1 * a0, 0.02 * w);
+        d.cheb_b[ty] = b0 + std::min(0.05 * b0, 0.02 * w);
     }
 }
 
