@@ -107,7 +107,8 @@ def reference_sample(draws, budget_s: float, cores: int, offset: int = 0):
     binary = str(ROOT / "oracle" / "_ref" / "cfd_ref")
     if not Path(binary).exists():
         return None, "oracle/_ref/cfd_ref not built"
-    # ~0.84 s per 257^2 step on one core (survey probe); size the sample to the budget
+    # the reference's step time per size on one core (0.84 s at 257^2, measured on this
+    # image's host); the sample is sized to the budget from these
     per_step = {65: 0.02, 129: 0.1, 193: 0.35, 257: 0.84}
     tasks, est = [], 0.0
     k = offset
