@@ -221,16 +221,27 @@ class NvmlClockSampler:
     def stop(self):
         self.run = False
         self.th.join(timeout=5)
-        sm, reasons = [], set()
         names = {self.HW: "hw_slowdown", self.HW_THERMAL: "hw_thermal_slowdown",
                  self.SW_THERMAL: "sw_thermal_slowdown", self.SW_POWER: "sw_power_cap"}
-        for ts, mhz, rs in self.samples:
-            if self.t0 is not None and not (self.t0 <= ts <= (self.t1 or ts)):
-                continue
-            sm.append(float(mhz))
-            for bit, n in names.items():
-                if rs & bit:
-                    reasons.add(n)
+
+        def collect(lo, hi):
+            sm, reasons = [], set()
+            for ts, mhz, rs in self.samples:
+                if lo is not None and not (lo <= ts <= (hi if hi is not None else ts)):
+                    continue
+                sm.append(float(mhz))
+                for bit, n in names.items():
+                    if rs & bit:
+                        reasons.add(n)
+            return sm, reasons
+
+        sm, reasons = collect(self.t0, self.t1)
+        window = "timed region"
+        if not sm and self.t0 is not None:
+            # a timed region of a few tens of ms can fall between two polls: take the samples
+            # within 50 ms of it, and say so
+            sm, reasons = collect(self.t0 - 0.05, (self.t1 or self.t0) + 0.05)
+            window = "timed region +- 50 ms"
         try:
             self.nv.nvmlShutdown()
         except Exception:
@@ -238,7 +249,7 @@ class NvmlClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(self.max_mhz), "reasons": sorted(reasons),
-                "samples": len(sm), "source": "nvml, 10 ms"}
+                "samples": len(sm), "source": "nvml, 10 ms", "window": window}
 
 
 def clock_sampler(index: int):

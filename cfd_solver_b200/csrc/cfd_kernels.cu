@@ -868,12 +868,15 @@ __global__ void __launch_bounds__(MG_PRR_THREADS, 3) k_mg_prr(BatchDev b, int l,
     __shared__ float xs[2 * MPR_XP];
     __shared__ float rs[2 * MPR_RP];
     const Tile t = b.atiles[l + 1][blockIdx.x];
-    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    // the case's done flag and the level's geometry in one round trip (the geometry is part
+    // of the exit test, so its loads are issued before the branch)
+    const int pdone = b.iscal[(long long)t.c * NISCAL + I_PDONE];
     const CaseDev& c = b.cases[t.c];
     const LevelDev& F = c.lev[l];
     const LevelDev& C = c.lev[l + 1];
     const int tid = threadIdx.x;
     const int fl = F.ld, W = F.W, per = c.periodic, n1 = F.n1;
+    if (pdone || W <= 0) return;
     if (per && (W & 1)) {
         if (tid == 0) atomicExch(b.error, 1);
         return;
@@ -912,6 +915,32 @@ __global__ void __launch_bounds__(MG_PRR_THREADS, 3) k_mg_prr(BatchDev b, int l,
     // point of colour cc in the block: (dx, dy) = (cc & 1, cc >> 1); its ringed position is
     // (2 bx + dx + 1, 2 by + dy + 1)
     float xr[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
+    // the first sweep from zero: a colour's neighbours of the colours not yet relaxed are
+    // still zero, so colour 0 reads none, colour 1 its E/W neighbours (colour 0), colour 2
+    // its N/S (colour 0) and diagonal (colour 1) neighbours, colour 3 all eight
+    auto relax0 = [&](auto cc_) {
+        constexpr int cc = decltype(cc_)::value;
+        constexpr int dx = cc & 1, dy = cc >> 1;
+        if (ok[dy][dx]) {
+            const float(&f)[10] = a[dy][dx];
+            const int xx = 2 * bx + dx + 1, ry = 2 * by + dy + 1;
+            float sm = 0.0f;
+            if (cc == 1) sm = f[1] * xs[mpr_at(xx + 1, ry)] + f[2] * xs[mpr_at(xx - 1, ry)];
+            if (cc == 2)
+                sm = f[3] * xs[mpr_at(xx, ry + 1)] + f[4] * xs[mpr_at(xx, ry - 1)] +
+                     f[5] * xs[mpr_at(xx + 1, ry + 1)] + f[6] * xs[mpr_at(xx - 1, ry + 1)] +
+                     f[7] * xs[mpr_at(xx + 1, ry - 1)] + f[8] * xs[mpr_at(xx - 1, ry - 1)];
+            if (cc == 3)
+                sm = f[1] * xs[mpr_at(xx + 1, ry)] + f[2] * xs[mpr_at(xx - 1, ry)] +
+                     f[3] * xs[mpr_at(xx, ry + 1)] + f[4] * xs[mpr_at(xx, ry - 1)] +
+                     f[5] * xs[mpr_at(xx + 1, ry + 1)] + f[6] * xs[mpr_at(xx - 1, ry + 1)] +
+                     f[7] * xs[mpr_at(xx + 1, ry - 1)] + f[8] * xs[mpr_at(xx - 1, ry - 1)];
+            const float v = (f[9] - sm) / f[0];
+            xs[mpr_at(xx, ry)] = v;
+            xr[dy][dx] = v;
+        }
+        __syncthreads();
+    };
     auto relax = [&](auto cc_) {
         constexpr int cc = decltype(cc_)::value;
         constexpr int dx = cc & 1, dy = cc >> 1;
@@ -932,7 +961,10 @@ __global__ void __launch_bounds__(MG_PRR_THREADS, 3) k_mg_prr(BatchDev b, int l,
     using C1 = std::integral_constant<int, 1>;
     using C2 = std::integral_constant<int, 2>;
     using C3 = std::integral_constant<int, 3>;
-    for (int n = 0; n < inner; n++) {
+    if (inner > 0) {
+        relax0(C0{}); relax0(C1{}); relax0(C2{}); relax0(C3{});
+    }
+    for (int n = 1; n < inner; n++) {
         relax(C0{}); relax(C1{}); relax(C2{}); relax(C3{});
     }
     // residual on the restriction's fine points (E without its ring), x of the owned points
@@ -1018,11 +1050,14 @@ __device__ __forceinline__ int mg_gs_at(int xx, int ry) {  // halo point (xx, ry
 __global__ void __launch_bounds__(MG_GS_THREADS, 8) k_mg_gs(BatchDev b, int l, int mode, int src, int dst, int inner) {
     __shared__ float xs[2 * MG_GS_XP];
     const Tile t = b.mtiles[l][blockIdx.x];
-    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
+    // the case's done flag and the level's geometry in one round trip (the geometry is part
+    // of the exit test, so its loads are issued before the branch)
+    const int pdone = b.iscal[(long long)t.c * NISCAL + I_PDONE];
     const CaseDev& c = b.cases[t.c];
     const LevelDev& L = c.lev[l];
     const int tid = threadIdx.x;
     const int ld = L.ld, W = L.W, per = c.periodic, n1 = L.n1;
+    if (pdone || W <= 0) return;
     if (per && (W & 1)) {
         if (tid == 0) atomicExch(b.error, 1);
         return;
