@@ -266,6 +266,17 @@ __global__ void __launch_bounds__(NT, 3) k_rhs(BatchDev b) {
         for (int m = 0; m < RHS_HALO; m++) tma_load_3d(sm + m * JTW * JTH, maps, t.i0, t.j0 - 2, hp[m], &bar);
         for (int m = 0; m < RHS_INT; m++) tma_load_3d(SI + m * TX * TYJ, maps + 128, t.i0 + 2, t.j0, ip[m], &bar);
     }
+    // the case's constants and planes, loaded while the copies are in flight
+    const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0, ilo = c.ilo, ihi = c.ihi;
+    const bool cav = c.profile == CAVITY;
+    const double d0 = c.d0, d1 = c.d1, dt = c.dt, Re = c.Re, Pr = c.Pr, Ri = c.Ri;
+    const double rd0 = 1.0 / d0, rd1 = 1.0 / d1;
+    double* const fb = b.f64 + c.base + H;  // plane 0 of the case; plane k at fb + k * ps
+    const long long ps = c.ps;
+    const bool warm = c.warm_up != 0;
+    int nextm = 0;  // fields whose first iterate goes into the scratch plane (FP64 form)
+    if (!b.mixed)
+        for (int f = 0; f < NFIELD; f++) nextm |= (b.iscal[(long long)t.c * NISCAL + I_MNEXT0 + f] != 0) << f;
     __syncthreads();
     const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0, b.wait_polls));
     if (!ok) {
@@ -275,30 +286,22 @@ __global__ void __launch_bounds__(NT, 3) k_rhs(BatchDev b) {
         }
         return;
     }
-    const int ld = c.ld, W = c.W, per = c.periodic, n1 = c.n1, n0 = c.n0;
-    const bool cav = c.profile == CAVITY;
-    const double d0 = c.d0, d1 = c.d1, dt = c.dt, Re = c.Re, Pr = c.Pr, Ri = c.Ri;
-    const double rd0 = 1.0 / d0, rd1 = 1.0 / d1;
     const double *Us = sm, *Vs = sm + JTW * JTH, *Ts = sm + 2 * JTW * JTH, *Ps = sm + 3 * JTW * JTH,
                  *UPs = sm + 4 * JTW * JTH, *VPs = sm + 5 * JTW * JTH;
-    const double* U = plane(b, c, P_U);
-    const double* V = plane(b, c, P_V);
-    const double* T = plane(b, c, P_T0 + cur);
-    const double* UP = plane(b, c, P_UP0 + cur);
-    const double* VP = plane(b, c, P_VP0 + cur);
+    const double* U = fb + P_U * ps;
+    const double* V = fb + P_V * ps;
+    const double* T = fb + (P_T0 + cur) * ps;
+    const double* UP = fb + (P_UP0 + cur) * ps;
+    const double* VP = fb + (P_VP0 + cur) * ps;
     // iterate buffers of field f: A (the solution) and B (the Jacobi scratch)
-    auto Ap = [&](int f) { return plane(b, c, f < 2 ? P_US + f : P_T0 + 2 * (f - 2) + nxt); };
-    auto Bp = [&](int f) { return plane(b, c, P_BU + f); };
-    const bool warm = c.warm_up != 0;
-    int nextm = 0;  // fields whose first iterate goes into the scratch plane (FP64 form)
-    if (!b.mixed)
-        for (int f = 0; f < NFIELD; f++) nextm |= (b.iscal[(long long)t.c * NISCAL + I_MNEXT0 + f] != 0) << f;
+    auto Ap = [&](int f) { return fb + (f < 2 ? P_US + f : P_T0 + 2 * (f - 2) + nxt) * ps; };
+    auto Bp = [&](int f) { return fb + (P_BU + f) * ps; };
     const int li = tid % TX, lj = tid / TX;
     const int i = t.i0 + li;
 #pragma unroll 1
     for (int h = 0; h < 2; h++) {
         const int j = t.j0 + lj + h * TY;
-        if (i < c.ilo || i > c.ihi || j > n1 - 2) continue;
+        if (i < ilo || i > ihi || j > n1 - 2) continue;
         const int o = (lj + h * TY + 2) * JTW + (li + 2);
         const int oi = (lj + h * TY) * TX + li;
         const long long k = (long long)j * ld + i;
@@ -355,11 +358,11 @@ __global__ void __launch_bounds__(NT, 3) k_rhs(BatchDev b) {
             sumv = bs * VPs[s0] + c1 * VPs[s1] + c2 * VPs[s2];
             qvp = qvp - sumv;
         }
-        plane(b, c, P_RU)[k] = qu;
-        plane(b, c, P_RV)[k] = qv;
-        plane(b, c, P_RT)[k] = qt;
-        plane(b, c, P_RUP)[k] = qup;
-        plane(b, c, P_RVP)[k] = qvp;
+        fb[P_RU * ps + k] = qu;
+        fb[P_RV * ps + k] = qv;
+        fb[P_RT * ps + k] = qt;
+        fb[P_RUP * ps + k] = qup;
+        fb[P_RVP * ps + k] = qvp;
         // seed the iterates (PSolver.cpp:1241-1337): u*, v*, T from the current fields;
         // up/vp from the previous solution (warm start) or zero. A solve predicted to stop
         // after an odd number of sweeps starts in the scratch plane, so that its result
@@ -451,6 +454,15 @@ __global__ void __launch_bounds__(NT, 4) k_face_q(BatchDev b) {
         const int hp[FQ_HALO] = {P_P, P_UP0 + nxt, P_VP0 + nxt, P_XIX, P_XIY, P_ETX, P_ETY};
         for (int m = 0; m < FQ_HALO; m++) tma_load_3d(sm + m * JTW * JTH, maps, t.i0, t.j0 - 2, hp[m], &bar);
     }
+    // the case's constants and output planes, loaded while the copies are in flight
+    const int ld = c.ld, ilo = c.ilo, ihi = c.ihi, n1 = c.n1, ld0 = c.lev[0].ld;
+    double* QP = plane(b, c, P_Q);
+    double* KRP = plane(b, c, P_KR);
+    float* B0 = mplane(b, c.lev[0], M_B);
+    // reciprocals once per thread: the per-cell quotients become products (each within an
+    // ulp of the quotient; 1 / (4 d) is 0.25 / d exactly)
+    const double dt = c.dt, rd0 = 1.0 / c.d0, rd1 = 1.0 / c.d1, q0 = 0.25 * rd0, q1 = 0.25 * rd1;
+    const double hdt = 0.5 * dt, rdt = 1.0 / dt;
     __syncthreads();
     const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, 0, b.wait_polls));
     if (!ok) {
@@ -462,17 +474,12 @@ __global__ void __launch_bounds__(NT, 4) k_face_q(BatchDev b) {
     }
     const double *P = sm, *U = sm + JTW * JTH, *V = sm + 2 * JTW * JTH, *X = sm + 3 * JTW * JTH,
                  *Y = sm + 4 * JTW * JTH, *E = sm + 5 * JTW * JTH, *G = sm + 6 * JTW * JTH;
-    const int ld = c.ld;
-    // reciprocals once per thread: the per-cell quotients become products (each within an
-    // ulp of the quotient; 1 / (4 d) is 0.25 / d exactly)
-    const double dt = c.dt, rd0 = 1.0 / c.d0, rd1 = 1.0 / c.d1, q0 = 0.25 * rd0, q1 = 0.25 * rd1;
-    const double hdt = 0.5 * dt, rdt = 1.0 / dt;
     const int li = tid % TX, lj = tid / TX;
     const int i = t.i0 + li;
     double red[3] = {0.0, 0.0, 0.0};
     for (int h = 0; h < 2; h++) {
         const int j = t.j0 + lj + h * TY;
-        if (!ok || i < c.ilo || i > c.ihi || j > c.n1 - 2) continue;
+        if (!ok || i < ilo || i > ihi || j > n1 - 2) continue;
         const int k = (lj + h * TY + 2) * JTW + (li + 2);
         const int kE = k + 1, kW = k - 1, kN = k + JTW, kS = k - JTW;
         double dpdxi_ip = (P[kE] - P[k]) * rd0;
@@ -500,11 +507,11 @@ __global__ void __launch_bounds__(NT, 4) k_face_q(BatchDev b) {
         // q doubles as BiCGStab's shadow residual r_hat; p, v and the iterate pcor are
         // initialised by the first iteration's kernels (beta = 0, x = 0)
         const long long kg = (long long)j * ld + i;
-        plane(b, c, P_Q)[kg] = q;
-        plane(b, c, P_KR)[kg] = q;
+        QP[kg] = q;
+        KRP[kg] = q;
         // the first iteration's p = r_0 = q, as the preconditioner's right-hand side (k_bicg_p
         // has nothing to do in the first iteration; the second reads p_1 from the q plane)
-        mplane(b, c.lev[0], M_B)[(long long)j * c.lev[0].ld + i] = (float)q;
+        B0[(long long)j * ld0 + i] = (float)q;
         red[0] += fabs(q);
         red[1] += q * q;
         red[2] = fmax(red[2], fabs(q));
