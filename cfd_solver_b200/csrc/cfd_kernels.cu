@@ -879,15 +879,12 @@ __global__ void __launch_bounds__(MG_PRR_THREADS, 3) k_mg_prr(BatchDev b, int l,
     __shared__ float xs[2 * MPR_XP];
     __shared__ float rs[2 * MPR_RP];
     const Tile t = b.atiles[l + 1][blockIdx.x];
-    // the case's done flag and the level's geometry in one round trip (the geometry is part
-    // of the exit test, so its loads are issued before the branch)
-    const int pdone = b.iscal[(long long)t.c * NISCAL + I_PDONE];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
     const LevelDev& F = c.lev[l];
     const LevelDev& C = c.lev[l + 1];
     const int tid = threadIdx.x;
     const int fl = F.ld, W = F.W, per = c.periodic, n1 = F.n1;
-    if (pdone || W <= 0) return;
     if (per && (W & 1)) {
         if (tid == 0) atomicExch(b.error, 1);
         return;
@@ -1061,14 +1058,11 @@ __device__ __forceinline__ int mg_gs_at(int xx, int ry) {  // halo point (xx, ry
 __global__ void __launch_bounds__(MG_GS_THREADS, 8) k_mg_gs(BatchDev b, int l, int mode, int src, int dst, int inner) {
     __shared__ float xs[2 * MG_GS_XP];
     const Tile t = b.mtiles[l][blockIdx.x];
-    // the case's done flag and the level's geometry in one round trip (the geometry is part
-    // of the exit test, so its loads are issued before the branch)
-    const int pdone = b.iscal[(long long)t.c * NISCAL + I_PDONE];
+    if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
     const CaseDev& c = b.cases[t.c];
     const LevelDev& L = c.lev[l];
     const int tid = threadIdx.x;
     const int ld = L.ld, W = L.W, per = c.periodic, n1 = L.n1;
-    if (pdone || W <= 0) return;
     if (per && (W & 1)) {
         if (tid == 0) atomicExch(b.error, 1);
         return;
