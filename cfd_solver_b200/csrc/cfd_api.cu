@@ -689,11 +689,12 @@ void enq_mid(cfd_batch* b, BatchDev& bd) {
     k_face_q<<<bd.njtiles, NT, kFaceQSmem, b->st>>>(bd);
 }
 // one BiCGStab iteration in two halves: up to the half-step exit (k_bicg_s), and the rest,
-// which the step graph skips when every case stopped at the half step. k_bicg_p forms the
-// iteration's direction (the first one, p_1 = r_0, is written by k_face_q).
+// which the step graph skips when every case stopped at the half step. The next iteration's
+// direction p_{k+1} is formed at the end of the second half (k_bicg_p, from the beta and
+// omega k_bicg_x has just computed), so the first iteration, whose p_1 = r_0 k_face_q writes,
+// and every step whose cases all stop at the first half step launch no k_bicg_p.
 void enq_p_first(cfd_batch* b, BatchDev& bd) {
     const int nf = bd.njtiles;  // the BiCGStab kernels run on the 32 x 16 tiles
-    { Prof pr(b, K_BICG_P); k_bicg_p<<<nf, NT, 0, b->st>>>(bd); }
     run_vcycle(b);
     { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 0); }
     { Prof pr(b, K_BICG_S); k_bicg_s<<<nf, NT, 0, b->st>>>(bd); }
@@ -703,6 +704,7 @@ void enq_p_second(cfd_batch* b, BatchDev& bd) {
     run_vcycle(b);
     { Prof pr(b, K_SPMV); k_spmv<<<nf, NT, 0, b->st>>>(bd, 1); }
     { Prof pr(b, K_BICG_X); k_bicg_x<<<nf, NT, 0, b->st>>>(bd, b->maxit_p); }
+    { Prof pr(b, K_BICG_P); k_bicg_p<<<nf, NT, 0, b->st>>>(bd); }
 }
 void enq_p_iter(cfd_batch* b, BatchDev& bd) {
     enq_p_first(b, bd);

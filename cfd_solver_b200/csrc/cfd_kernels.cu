@@ -550,9 +550,10 @@ __global__ void __launch_bounds__(NT, 4) k_face_q(BatchDev b) {
 __global__ void __launch_bounds__(NT, 3) k_bicg_p(BatchDev b) {
     const Tile t = b.jtiles[blockIdx.x];
     if (b.iscal[(long long)t.c * NISCAL + I_PDONE]) return;
-    // p_{k+1} = r_k + beta (p_k - omega v_k). In the first iteration there is nothing to do:
-    // p_1 = r_0 = q, which k_face_q has written as the preconditioner's right-hand side; the
-    // second iteration reads p_1 from the q plane.
+    // p_{k+1} = r_k + beta (p_k - omega v_k), launched at the end of iteration k (after
+    // k_bicg_x has counted it and formed beta). p_1 = r_0 = q is k_face_q's, written as the
+    // preconditioner's right-hand side, so after the first iteration p_1 is read from the q
+    // plane. Before any iteration (it == 0) there is nothing to do.
     const int it = b.iscal[(long long)t.c * NISCAL + I_PIT];
     if (it == 0) return;
     const CaseDev& c = b.cases[t.c];
