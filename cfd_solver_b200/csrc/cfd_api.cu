@@ -197,7 +197,8 @@ struct cfd_batch {
     int maxit_mom = 100, maxit_p = 200;
     int precision = CFD_PRECISION_FP64;
     int sw_grid = 0;      // CTAs of the sweep kernel (one per 32 x 16 tile)
-    size_t sw_smem = 0;
+    size_t sw_smem = 0;   // its dynamic shared memory (the precision form: the first sweep's)
+    size_t sw_smem1 = 0;  // the precision form's later sweeps (k_sweep_mx1)
     int coarse_sweeps = 12;
     int mg_pre = 1, mg_post = 3;  // multigrid sweeps before / after the coarse correction
     int mg_fused = 2;             // 1: a smoothing phase's sweeps in one launch; 2: and the
@@ -658,20 +659,41 @@ int run_vcycle(cfd_batch* b) {
 // ---- the pieces of one step (also captured into the step graph)
 void enq_begin(cfd_batch* b, BatchDev& bd) {
     cudaMemsetAsync(b->flags, 0, 4 * sizeof(int), b->st);
-    cudaMemsetAsync(b->flags + 7, 0, sizeof(int), b->st);
     Prof pr(b, K_RHS);
     k_rhs<<<bd.njtiles, NT, kRhsSmem, b->st>>>(bd);
 }
+// FP64 form: sweeps in pairs (the iterates ping-pong between two planes)
 void enq_mom_pair(cfd_batch* b, BatchDev& bd) {
     for (int s = 0; s < 2; s++) {
         {
             Prof pr(b, K_SWEEP);
-            if (b->precision == CFD_PRECISION_MIXED) k_sweep_mx<<<b->sw_grid, SW_THREADS, b->sw_smem, b->st>>>(bd);
-            else k_sweep_f64<<<b->sw_grid, SW_THREADS, b->sw_smem, b->st>>>(bd);
+            k_sweep_f64<<<b->sw_grid, SW_THREADS, b->sw_smem, b->st>>>(bd);
         }
         Prof pr(b, K_SWEEP_FIN);
         k_sweep_fin<<<b->n, b->swf_threads, 0, b->st>>>(bd);
     }
+}
+// precision form: the step's first sweep (FP64 residual, k_sweep_mx0), then one FP32
+// sweep (k_sweep_mx1) per loop iteration
+void enq_mom_mx_first(cfd_batch* b, BatchDev& bd) {
+    {
+        Prof pr(b, K_SWEEP);
+        k_sweep_mx0<<<b->sw_grid, SW_THREADS, b->sw_smem, b->st>>>(bd);
+    }
+    Prof pr(b, K_SWEEP_FIN);
+    k_sweep_fin<<<b->n, b->swf_threads, 0, b->st>>>(bd);
+}
+void enq_mom_mx_next(cfd_batch* b, BatchDev& bd) {
+    {
+        Prof pr(b, K_SWEEP);
+        k_sweep_mx1<<<b->sw_grid, SW_THREADS, b->sw_smem1, b->st>>>(bd);
+    }
+    Prof pr(b, K_SWEEP_FIN);
+    k_sweep_fin<<<b->n, b->swf_threads, 0, b->st>>>(bd);
+}
+// loop iterations that bound the momentum / energy solves at maxit_mom sweeps
+int mom_loop_cap(const cfd_batch* b) {
+    return b->precision == CFD_PRECISION_MIXED ? std::max(1, b->maxit_mom - 1) : std::max(1, b->maxit_mom / 2);
 }
 void enq_mid(cfd_batch* b, BatchDev& bd) {
     if (b->precision == CFD_PRECISION_MIXED) {
@@ -721,11 +743,15 @@ int one_step_direct(cfd_batch* b) {
     BatchDev& bd = b->bd;
     bd.cur = b->cur;
     enq_begin(b, bd);
-    // momentum / energy solves: sweeps in pairs until every (case, field) stopped; the
-    // counter is read every second pair (a finished case's CTAs leave at once)
-    const int npairs = std::max(1, b->maxit_mom / 2);
+    // momentum / energy solves: sweeps (in pairs in the FP64 form) until every (case, field)
+    // stopped; the counter is read every second loop iteration (a finished case's CTAs
+    // leave at once)
+    const bool mixed = b->precision == CFD_PRECISION_MIXED;
+    if (mixed) enq_mom_mx_first(b, bd);
+    const int npairs = mom_loop_cap(b);
     for (int pair = 0; pair < npairs; pair++) {
-        enq_mom_pair(b, bd);
+        if (mixed) enq_mom_mx_next(b, bd);
+        else enq_mom_pair(b, bd);
         if (pair % 2 == 1 || pair == npairs - 1) {
             int m = 0;
             int rc = read_flag(b, 1, &m);
@@ -837,10 +863,16 @@ int build_step_graph(cfd_batch* b, int cur) {
         prev = n;
         return CFD_OK;
     };
-    int rc = child([&] { enq_begin(b, bd); });
+    const bool mixed = b->precision == CFD_PRECISION_MIXED;
+    int rc = child([&] {
+        enq_begin(b, bd);
+        if (mixed) enq_mom_mx_first(b, bd);
+    });
     const long long la = b->launches;
-    if (!rc) rc = loop([&] { enq_mom_pair(b, bd); }, b->flags + 1, b->flags + 2,
-                       std::max(1, b->maxit_mom / 2), b->flags + 5);
+    if (!rc) rc = loop([&] {
+        if (mixed) enq_mom_mx_next(b, bd);
+        else enq_mom_pair(b, bd);
+    }, b->flags + 1, b->flags + 2, mom_loop_cap(b), b->flags + 5);
     const long long lm = b->launches;
     if (!rc) rc = child([&] { enq_mid(b, bd); });
     const long long lp0 = b->launches;
@@ -1042,9 +1074,15 @@ void place_levels(CaseDev& d, const CaseGeom& G, long long off32) {
 }
 
 int set_kernel_attributes(cfd_batch* b) {
-    b->sw_smem = b->precision == CFD_PRECISION_MIXED ? sweep_smem_mx() : sweep_smem_f64();
-    const void* swk = b->precision == CFD_PRECISION_MIXED ? (const void*)k_sweep_mx : (const void*)k_sweep_f64;
+    b->sw_smem = b->precision == CFD_PRECISION_MIXED ? sweep_smem_mx0() : sweep_smem_f64();
+    const void* swk = b->precision == CFD_PRECISION_MIXED ? (const void*)k_sweep_mx0 : (const void*)k_sweep_f64;
     CK(cudaFuncSetAttribute(swk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->sw_smem));
+    if (b->precision == CFD_PRECISION_MIXED) {
+        // six CTAs of the FP32 sweep per SM need the largest shared-memory carve-out
+        b->sw_smem1 = sweep_smem_mx1();
+        CK(cudaFuncSetAttribute(k_sweep_mx1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->sw_smem1));
+        CK(cudaFuncSetAttribute(k_sweep_mx1, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    }
     CK(cudaFuncSetAttribute(swk, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     CK(cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem));
     CK(cudaFuncSetAttribute(k_face_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFaceQSmem));
@@ -1382,7 +1420,6 @@ int cfd_batch_create(int ncases, const cfd_grid* grids, const cfd_params* params
     bd.error = b->flags + 4;
     bd.wait_polls = kWaitPolls;
     bd.mg_res = mg_res_plane(b->mg_pre, b->mg_post, b->mg_fused);
-    bd.sweep_no = b->flags + 7;
     bd.mixed = b->precision == CFD_PRECISION_MIXED;
 
     // ---- upload grid + initial state (padded planes with halos)
@@ -1520,7 +1557,6 @@ int cfd_pool_create(size_t hbm_budget, int max_cases, int precision, cfd_batch**
     bd.error = b->flags + 4;
     bd.wait_polls = kWaitPolls;
     bd.mg_res = mg_res_plane(b->mg_pre, b->mg_post, b->mg_fused);
-    bd.sweep_no = b->flags + 7;
     bd.mixed = precision == CFD_PRECISION_MIXED;
     if (int rc = build_tables(b, {})) return cleanup(rc);
     *out = b;

@@ -140,7 +140,6 @@ struct BatchDev {
     int* mactive;          // global count of (case, field) pairs still iterating (momentum)
     int* error;            // set when a bounded wait in a kernel gives up
     unsigned wait_polls;   // polls of a kernel's bounded mbarrier waits before they give up
-    int* sweep_no;         // momentum sweep launches of the current step (k_sweep_fin counts)
     int mixed;             // 1: the precision form (momentum iterates are FP32 corrections)
     int* tword;            // per 32 x 16 tile: its case's I_MWORD, so the sweep kernel reads it
                            // in the same round trip as the tile itself

@@ -391,15 +391,23 @@ __global__ void __launch_bounds__(SW_THREADS, 4) k_sweep_f64(BatchDev b) {
     sweep_tile<SW_F64>(b, sm, bar);
 }
 
-// precision form: every still-iterating field of every case is at the same sweep index
-// within one launch (all start at 0 together, one sweep per launch), so the launch runs
-// either the FP64 residual sweep (the step's first launch) or the FP32 correction sweeps
-__global__ void __launch_bounds__(SW_THREADS, 4) k_sweep_mx(BatchDev b) {
+// precision form, the step's first sweep (every still-iterating field of every case starts
+// at sweep 0 together): the FP64 residual r = rhs - A x0 and the first FP32 correction
+__global__ void __launch_bounds__(SW_THREADS, 4) k_sweep_mx0(BatchDev b) {
     extern __shared__ __align__(128) unsigned char swraw[];
     __shared__ __align__(8) uint64_t bar[2];
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(swraw) + 127) & ~uintptr_t(127));
-    if (*b.sweep_no == 0) sweep_tile<SW_MX0>(b, sm, bar);
-    else sweep_tile<SW_MX>(b, sm, bar);
+    sweep_tile<SW_MX0>(b, sm, bar);
+}
+
+// precision form, the later sweeps: FP32 throughout. Compiled apart from the FP64 first
+// sweep it needs 80 registers and no spills, so six CTAs (37 KB of shared memory each)
+// share an SM instead of four
+__global__ void __launch_bounds__(SW_THREADS, 6) k_sweep_mx1(BatchDev b) {
+    extern __shared__ __align__(128) unsigned char swraw[];
+    __shared__ __align__(8) uint64_t bar[2];
+    unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(swraw) + 127) & ~uintptr_t(127));
+    sweep_tile<SW_MX>(b, sm, bar);
 }
 
 // What the case's bookkeeping after a sweep reads, loaded by thread 0 of k_sweep_fin at its
@@ -491,7 +499,6 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
     const CaseDev& c = b.cases[cid];
     int* is = b.iscal + (long long)cid * NISCAL;
     const int word = is[I_MWORD];
-    if (cid == 0 && threadIdx.x == 0) atomicAdd(b.sweep_no, 1);  // read by the next sweep launch
     if (!(word & ((1 << NFIELD) - 1))) return;
     const int tid = threadIdx.x;
     FinIn in;
@@ -513,7 +520,8 @@ __global__ void __launch_bounds__(SWF_THREADS) k_sweep_fin(BatchDev b) {
 
 
 size_t sweep_smem_f64() { return (size_t)SwLayout<SW_F64>::TOTAL + 128; }
-size_t sweep_smem_mx() { return (size_t)max(SwLayout<SW_MX0>::TOTAL, SwLayout<SW_MX>::TOTAL) + 128; }
+size_t sweep_smem_mx0() { return (size_t)SwLayout<SW_MX0>::TOTAL + 128; }
+size_t sweep_smem_mx1() { return (size_t)SwLayout<SW_MX>::TOTAL + 128; }
 
 // x0 += d for every field of the precision form (after the last sweep, d_final in X_DA)
 // A solve whose result is in the scratch plane (FP64 form; it stopped after a sweep count of

@@ -11,10 +11,12 @@ constexpr int SWF_THREADS = 512;                  // per-case finalisation, most
                                                    // case of >= 1024 tiles; 128 otherwise)
 
 __global__ void k_sweep_f64(BatchDev b);
-__global__ void k_sweep_mx(BatchDev b);
+__global__ void k_sweep_mx0(BatchDev b);
+__global__ void k_sweep_mx1(BatchDev b);
 __global__ void k_sweep_fin(BatchDev b);
 __global__ void k_mom_update(BatchDev b);
 __global__ void k_mom_fix(BatchDev b);
 size_t sweep_smem_f64();
-size_t sweep_smem_mx();
+size_t sweep_smem_mx0();
+size_t sweep_smem_mx1();
 }  // namespace cfd
